@@ -1,0 +1,405 @@
+"""Python mirror of the sampler's C ABI (include/dualres_b200.h).
+
+The class names follow the reference's C++ API so that calling code reads
+like the reference (include/dualres/*.h):
+
+* ``MultiResData``        -> a device volume (images, masks, kriging matrix, spectrum)
+* ``HMCParameters``       -> the sampler options (burnin, nsave, thin, leapfrog, mhtarget, seed)
+* ``MultiResParameters``  -> a set of chains on one volume (state, energies, gradient, update)
+* ``fit_model``           -> the fit loop, returning an ``mcmc_summary``
+
+Errors raise ``DrError`` with the library's code and message, the way the
+reference throws std::domain_error / std::logic_error.  The library is CUDA
+only: loading works without a GPU (for the host-side kriging builder), but
+every device call needs one and fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import build as _build
+
+DR_OK = 0
+DR_ERR_INVALID = -1
+DR_ERR_CUDA = -2
+DR_ERR_NOMEM = -3
+DR_ERR_DOMAIN = -4
+DR_ERR_UNSUPPORTED = -5
+DR_ERR_STATE = -6
+DR_ERR_TIMEOUT = -7
+DR_COV_RBF = 0
+DR_COV_RQ = 1
+
+_ERR_NAMES = {DR_ERR_INVALID: "INVALID", DR_ERR_CUDA: "CUDA", DR_ERR_NOMEM: "NOMEM", DR_ERR_DOMAIN: "DOMAIN",
+              DR_ERR_UNSUPPORTED: "UNSUPPORTED", DR_ERR_STATE: "STATE", DR_ERR_TIMEOUT: "TIMEOUT"}
+
+
+class DrError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{_ERR_NAMES.get(code, code)}] {msg}")
+        self.code = code
+
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+
+class VolumeDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("highres", _fp), ("qform_hr", _fp),
+                ("hmask", _fp), ("omask", _fp), ("sx", C.c_int), ("sy", C.c_int), ("sz", C.c_int),
+                ("stdres", _fp), ("qform_sr", _fp), ("smask", _fp), ("covariance", C.c_float * 3),
+                ("covfun", C.c_int), ("neighborhood", C.c_float), ("device", C.c_int)]
+
+
+class VolumeInfo(C.Structure):
+    _fields_ = [("E", C.c_int * 3), ("N", C.c_int64), ("box", C.c_int * 3), ("n_highres", C.c_int),
+                ("n_stdres", C.c_int), ("n_output", C.c_int), ("kriging_nnz", C.c_int64),
+                ("n_nonpositive", C.c_int), ("max_eigenvalue", C.c_double), ("setup_seconds", C.c_double),
+                ("kriging_seconds", C.c_double), ("neighborhood", C.c_float), ("device_bytes", C.c_int64)]
+
+
+class HmcOpts(C.Structure):
+    _fields_ = [("burnin", C.c_int), ("nsave", C.c_int), ("thin", C.c_int), ("leapfrog", C.c_int),
+                ("mhtarget", C.c_float), ("starting_eps", C.c_float), ("seed", C.c_uint64),
+                ("store_samples", C.c_int)]
+
+
+class ChainStats(C.Structure):
+    _fields_ = [("iteration", C.c_int), ("saved", C.c_int), ("integrator_steps", C.c_int), ("eps", C.c_float),
+                ("mh_rate", C.c_float), ("sigma_hr", C.c_float), ("sigma_sr", C.c_float),
+                ("last_log_ratio", C.c_double), ("accepted", C.c_int64), ("grad_evals", C.c_int64),
+                ("done", C.c_int)]
+
+
+_lib = None
+
+
+def lib_path():
+    return _build.LIB
+
+
+def lib(build_if_missing=True):
+    """Load the in-tree shared library (building it if it is missing or stale)."""
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if build_if_missing:
+            _build.build()
+        if not os.path.exists(path):
+            raise DrError(DR_ERR_STATE, f"CUDA library not built: {path}")
+        L = C.CDLL(path)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L):
+    vp = C.c_void_p
+    L.dr_last_error.restype = C.c_char_p
+    L.dr_version.restype = C.c_char_p
+    L.dr_kernel_launches.argtypes = [C.c_int]
+    L.dr_kernel_launches.restype = C.c_int64
+    L.dr_volume_create.argtypes = [C.POINTER(VolumeDesc), C.POINTER(vp)]
+    L.dr_volume_info_get.argtypes = [vp, C.POINTER(VolumeInfo)]
+    L.dr_volume_kriging_get.argtypes = [vp, vp, vp, vp]
+    L.dr_volume_lambda_get.argtypes = [vp, vp]
+    L.dr_volume_indices_get.argtypes = [vp, vp, vp]
+    L.dr_volume_data_get.argtypes = [vp, vp, vp]
+    L.dr_volume_destroy.argtypes = [vp]
+    L.dr_volume_destroy.restype = None
+    L.dr_chainset_create.argtypes = [vp, C.c_int, C.POINTER(HmcOpts), C.POINTER(vp)]
+    L.dr_chainset_destroy.argtypes = [vp]
+    L.dr_chainset_destroy.restype = None
+    L.dr_step.argtypes = [vp, C.c_int]
+    L.dr_run.argtypes = [vp]
+    L.dr_chain_stats_get.argtypes = [vp, vp]
+    L.dr_summary_get.argtypes = [vp, C.c_int, vp, vp, vp]
+    L.dr_samples_get.argtypes = [vp, C.c_int, vp, C.c_int, _ip]
+    L.dr_set_state.argtypes = [vp, C.c_int, vp, C.c_float, C.c_float]
+    L.dr_get_state.argtypes = [vp, C.c_int, vp, vp]
+    L.dr_log_posterior.argtypes = [vp, C.c_int, vp, vp]
+    L.dr_gradient.argtypes = [vp, C.c_int, vp, vp]
+    L.dr_leapfrog_fixed.argtypes = [vp, C.c_int, vp, vp, C.c_float, C.c_int, vp, vp, vp]
+    L.dr_kriging_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int, vp, vp,
+                                    C.c_float, _ip, C.POINTER(C.c_int64), C.POINTER(_ip), C.POINTER(_ip),
+                                    C.POINTER(_fp)]
+    L.dr_free.argtypes = [vp]
+    L.dr_free.restype = None
+    L.dr_debug_dual_averaging.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, vp,
+                                          vp, vp, C.c_int]
+
+
+def check(rc):
+    if rc != DR_OK:
+        msg = lib().dr_last_error()
+        raise DrError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def kriging_matrix(highres, qform_hr, stdres, qform_sr, covariance, neighborhood):
+    """Host-side get_sparse_kriging_matrix_data (kriging_matrix.h:148-343); highres must be masked."""
+    L = lib()
+    hr, sr = _f32(highres), _f32(stdres)
+    nz, ny, nx = hr.shape
+    sz, sy, sx = sr.shape
+    qh, qs = _f32(qform_hr), _f32(qform_sr)
+    th = _f32(covariance)
+    nrows = C.c_int(0)
+    nnz = C.c_int64(0)
+    rp, cl, vl = _ip(), _ip(), _fp()
+    check(L.dr_kriging_matrix(_ptr(hr), nx, ny, nz, _ptr(qh), _ptr(sr), sx, sy, sz, _ptr(qs), _ptr(th),
+                              float(neighborhood), C.byref(nrows), C.byref(nnz), C.byref(rp), C.byref(cl),
+                              C.byref(vl)))
+    try:
+        n, z = nrows.value, nnz.value
+        rowptr = np.ctypeslib.as_array(rp, shape=(n + 1,)).copy()
+        col = np.ctypeslib.as_array(cl, shape=(max(z, 1),))[:z].copy()
+        val = np.ctypeslib.as_array(vl, shape=(max(z, 1),))[:z].copy()
+    finally:
+        L.dr_free(rp)
+        L.dr_free(cl)
+        L.dr_free(vl)
+    return rowptr, col, val
+
+
+class MultiResData:
+    """A volume on the GPU: the inputs of MultiResData<T> (MultiResData.h:96-127) plus
+    the one-time part of the MultiResParameters<T> constructor."""
+
+    def __init__(self, highres, qform_hr, stdres=None, qform_sr=None, covariance=(1.0, 0.6, 1.5),
+                 neighborhood=-1.0, hmask=None, omask=None, smask=None, covfun=DR_COV_RBF, device=0):
+        L = lib()
+        self._keep = []
+        hr = _f32(highres)
+        nz, ny, nx = hr.shape
+        d = VolumeDesc()
+        d.nx, d.ny, d.nz = nx, ny, nz
+
+        def fp(a):
+            if a is None:
+                return None
+            a = _f32(a)
+            self._keep.append(a)
+            return a.ctypes.data_as(_fp)
+
+        d.highres = fp(hr)
+        d.qform_hr = fp(qform_hr)
+        d.hmask = fp(hmask)
+        d.omask = fp(omask)
+        if stdres is not None:
+            sr = _f32(stdres)
+            d.sz, d.sy, d.sx = sr.shape
+            d.stdres = fp(sr)
+            d.qform_sr = fp(qform_sr)
+            d.smask = fp(smask)
+        for i in range(3):
+            d.covariance[i] = float(covariance[i])
+        d.covfun = covfun
+        d.neighborhood = float(neighborhood)
+        d.device = device
+        h = C.c_void_p()
+        check(L.dr_volume_create(C.byref(d), C.byref(h)))
+        self._keep = []
+        self.h = h
+        info = VolumeInfo()
+        check(L.dr_volume_info_get(self.h, C.byref(info)))
+        self.info = info
+        self.E = tuple(info.E)
+        self.N = int(info.N)
+        self.shape = (self.E[2], self.E[1], self.E[0])
+        self.n_highres = info.n_highres
+        self.n_stdres = info.n_stdres
+        self.n_output = info.n_output
+
+    @classmethod
+    def from_volume(cls, vol, device=0, **kw):
+        """Build from a ``dualres_b200.synth.Volume``."""
+        return cls(vol.highres, vol.qform_hr, vol.stdres, vol.qform_sr, vol.theta, vol.radius,
+                   hmask=vol.hmask, omask=vol.omask, device=device, **kw)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dr_volume_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def W(self):
+        """Kriging matrix as (rowptr, col, val)."""
+        rp = np.zeros(self.n_stdres + 1, np.int32)
+        z = int(self.info.kriging_nnz)
+        col = np.zeros(max(z, 1), np.int32)
+        val = np.zeros(max(z, 1), np.float32)
+        check(lib().dr_volume_kriging_get(self.h, _ptr(rp), _ptr(col), _ptr(val)))
+        return rp, col[:z], val[:z]
+
+    def lambda_re(self):
+        out = np.zeros(self.N, np.float64)
+        check(lib().dr_volume_lambda_get(self.h, _ptr(out)))
+        return out.reshape(self.shape)
+
+    def indices(self):
+        d = np.zeros(self.n_highres, np.int32)
+        o = np.zeros(max(self.n_output, 1), np.int32)
+        check(lib().dr_volume_indices_get(self.h, _ptr(d), _ptr(o)))
+        return d, o[: self.n_output]
+
+    def data(self):
+        yh = np.zeros(self.n_highres, np.float32)
+        ys = np.zeros(max(self.n_stdres, 1), np.float32)
+        check(lib().dr_volume_data_get(self.h, _ptr(yh), _ptr(ys)))
+        return yh, ys[: self.n_stdres]
+
+
+@dataclass
+class HMCParameters:
+    """HMCParameters<T>(burnin, n_save, thin, integrator_steps, starting_eps, mh_target)
+    (HMCParameters.h:97-149) plus --seed; defaults of GPMCommandParser.inl:210-226."""
+
+    burnin: int = 1000
+    nsave: int = 1000
+    thin: int = 3
+    leapfrog: int = 25
+    mhtarget: float = 0.65
+    starting_eps: float = -1.0
+    seed: int = 1
+    store_samples: bool = False
+
+    def c(self):
+        o = HmcOpts()
+        o.burnin, o.nsave, o.thin, o.leapfrog = self.burnin, self.nsave, self.thin, self.leapfrog
+        o.mhtarget, o.starting_eps, o.seed = self.mhtarget, self.starting_eps, self.seed
+        o.store_samples = 1 if self.store_samples else 0
+        return o
+
+
+class MultiResParameters:
+    """n independent chains on one volume (MultiResParameters<float> x n)."""
+
+    def __init__(self, data: MultiResData, hmc: HMCParameters, n_chains=1):
+        self.data = data
+        self.hmc = hmc
+        self.n_chains = n_chains
+        h = C.c_void_p()
+        o = hmc.c()
+        check(lib().dr_chainset_create(data.h, n_chains, C.byref(o), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dr_chainset_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _field(self, x):
+        a = np.ascontiguousarray(x, dtype=np.complex64).reshape(self.data.shape)
+        return a
+
+    def update(self, iterations=1):
+        check(lib().dr_step(self.h, iterations))
+
+    def run(self):
+        check(lib().dr_run(self.h))
+
+    def stats(self):
+        arr = (ChainStats * self.n_chains)()
+        check(lib().dr_chain_stats_get(self.h, arr))
+        return [{f: getattr(s, f) for f, _ in ChainStats._fields_} for s in arr]
+
+    def summary(self, chain=-1):
+        n = self.data.n_output
+        m = np.zeros(max(n, 1), np.float32)
+        v = np.zeros(max(n, 1), np.float32)
+        a = np.zeros(max(n, 1), np.float32)
+        check(lib().dr_summary_get(self.h, chain, _ptr(m), _ptr(v), _ptr(a)))
+        return dict(mean=m[:n], var=v[:n], activation=a[:n])
+
+    def samples(self, chain, max_saved=None):
+        max_saved = max_saved or self.hmc.nsave
+        out = np.zeros((max_saved, max(self.data.n_output, 1)), np.float32)
+        ns = C.c_int(0)
+        check(lib().dr_samples_get(self.h, chain, _ptr(out), max_saved, C.byref(ns)))
+        return out[: ns.value, : self.data.n_output]
+
+    def set_state(self, chain, mu, sigma_sq_inv):
+        a = self._field(mu)
+        check(lib().dr_set_state(self.h, chain, _ptr(a), float(sigma_sq_inv[0]), float(sigma_sq_inv[1])))
+
+    def get_state(self, chain):
+        mu = np.zeros(self.data.shape, np.complex64)
+        s = np.zeros(2, np.float32)
+        check(lib().dr_get_state(self.h, chain, _ptr(mu), _ptr(s)))
+        return mu, s
+
+    def log_prior_likelihood(self, chain, mu):
+        a = self._field(mu)
+        out = np.zeros(2, np.float64)
+        check(lib().dr_log_posterior(self.h, chain, _ptr(a), _ptr(out)))
+        return float(out[0]), float(out[1])
+
+    def log_posterior(self, chain, mu):
+        lp, ll = self.log_prior_likelihood(chain, mu)
+        return lp + ll
+
+    def gradient(self, chain, mu):
+        a = self._field(mu)
+        g = np.zeros(self.data.shape, np.complex64)
+        check(lib().dr_gradient(self.h, chain, _ptr(a), _ptr(g)))
+        return g
+
+    def leapfrog(self, chain, mu0, p0, eps, L):
+        a, b = self._field(mu0), self._field(p0)
+        mo = np.zeros(self.data.shape, np.complex64)
+        po = np.zeros(self.data.shape, np.complex64)
+        en = np.zeros(6, np.float64)
+        check(lib().dr_leapfrog_fixed(self.h, chain, _ptr(a), _ptr(b), float(eps), int(L), _ptr(mo), _ptr(po),
+                                      _ptr(en)))
+        return mo, po, en
+
+
+def fit_model(data: MultiResData, hmc: HMCParameters, n_chains=1):
+    """gpp_approx::fit_model (gaussian_process_model.h:88-177): run to nsave samples and summarise."""
+    p = MultiResParameters(data, hmc, n_chains)
+    p.run()
+    out = p.summary(-1)
+    st = p.stats()
+    out["mh_rate"] = float(np.mean([s["mh_rate"] for s in st]))
+    out["eps"] = float(np.mean([s["eps"] for s in st]))
+    out["stats"] = st
+    out["chains"] = p
+    return out
+
+
+def debug_dual_averaging(burnin, nsave, thin, L, starting_eps, mhtarget, rates, device=0):
+    r = np.ascontiguousarray(rates, np.float32)
+    e = np.zeros(len(r), np.float64)
+    s = np.zeros(len(r), np.int32)
+    check(lib().dr_debug_dual_averaging(burnin, nsave, thin, L, starting_eps, mhtarget, len(r), _ptr(r), _ptr(e),
+                                        _ptr(s), device))
+    return e, s
+
+
+def kernel_launches(reset=False):
+    return int(lib().dr_kernel_launches(1 if reset else 0))

@@ -1,0 +1,62 @@
+"""Build the sm_100a shared library dualres_b200/_lib/libdualres_b200.so.
+
+nvcc cross-compiles for sm_100a without a GPU.  The library is built in-tree
+so that it travels with the repository snapshot; nothing is installed.
+
+    python -m dualres_b200.build [--force] [--verbose]
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libdualres_b200.so")
+SOURCES = ["api.cu", "host_setup.cpp"]
+DEPS = ["api.cu", "kernels.cu", "common.cuh", "fft.cuh", "drb.h", "host_setup.cpp", "host_setup.h"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path():
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    inc = os.path.join(HERE, "..", "include", "dualres_b200.h")
+    deps = [os.path.join(CSRC, d) for d in DEPS] + [inc]
+    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+
+
+def build(force=False, verbose=False):
+    if not force and not _stale():
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    gxx = shutil.which("g++") or "g++"
+    cmd = [nvcc_path(), "-shared", "-std=c++17", "-O3", "-lineinfo", *ARCH,
+           "-ccbin", gxx, "-Xcompiler", "-fPIC,-fopenmp,-O3",
+           "--expt-relaxed-constexpr", "-Xptxas", "-O3",
+           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES], "-lgomp"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=not verbose, text=True)
+    if res.returncode != 0:
+        sys.stderr.write((res.stdout or "") + (res.stderr or ""))
+        raise RuntimeError("nvcc failed")
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    print(LIB)

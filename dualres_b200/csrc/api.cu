@@ -1,0 +1,1014 @@
+// Host driver and C ABI (include/dualres_b200.h) of the B200 sampler.
+//
+// One translation unit holds every kernel (kernels.cu) so that template
+// instantiation and the twiddle tables stay in one module.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dualres_b200.h"
+#include "host_setup.h"
+#include "kernels.cu"
+
+namespace drb {
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_err;
+static thread_local int64_t g_launches = 0;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                                     \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      throw Error(DR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+  } while (0)
+
+#define CK_LAUNCH()                                                                                  \
+  do {                                                                                               \
+    cudaError_t e_ = cudaGetLastError();                                                             \
+    if (e_ != cudaSuccess) throw Error(DR_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    g_launches++;                                                                                    \
+  } while (0)
+
+static int cdiv_i(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------- per-device set-up
+struct DeviceTables {
+  bool ready = false;
+  const float2* tw_f = nullptr;
+  const double2* tw_d = nullptr;
+};
+static std::mutex g_dev_mtx;
+static DeviceTables g_dev[64];
+
+template <int N, class C>
+static void set_pass_attrs() {
+  const int bytes = N * (TILE_LINES + 1) * (int)sizeof(C);
+  CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_STORE, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_LOAD, EPI_STORE, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  if constexpr (sizeof(C) == 8) {
+    CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_xline<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  }
+}
+
+template <class C>
+static void set_all_attrs() {
+  set_pass_attrs<2, C>(); set_pass_attrs<4, C>(); set_pass_attrs<8, C>(); set_pass_attrs<16, C>();
+  set_pass_attrs<32, C>(); set_pass_attrs<64, C>(); set_pass_attrs<128, C>(); set_pass_attrs<256, C>();
+  if constexpr (sizeof(C) == 8) set_pass_attrs<512, C>();
+}
+
+static DeviceTables& device_tables(int dev) {
+  std::lock_guard<std::mutex> lk(g_dev_mtx);
+  if (dev < 0 || dev >= 64) throw Error(DR_ERR_INVALID, "device ordinal out of range");
+  DeviceTables& t = g_dev[dev];
+  if (t.ready) return t;
+  CK(cudaSetDevice(dev));
+  std::vector<float2> hf(TW_TOTAL);
+  std::vector<double2> hd(TW_TOTAL);
+  for (int N = 2; N <= 512; N <<= 1)
+    for (int m = 0; m < N; m++) {
+      const double a = -2.0 * M_PI * (double)m / (double)N;
+      hd[tw_offset(N) + m] = make_double2(std::cos(a), std::sin(a));
+      hf[tw_offset(N) + m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+  CK(cudaMemcpyToSymbol(g_tw_f, hf.data(), sizeof(float2) * TW_TOTAL));
+  CK(cudaMemcpyToSymbol(g_tw_d, hd.data(), sizeof(double2) * TW_TOTAL));
+  void* p = nullptr;
+  CK(cudaGetSymbolAddress(&p, g_tw_f));
+  t.tw_f = (const float2*)p;
+  CK(cudaGetSymbolAddress(&p, g_tw_d));
+  t.tw_d = (const double2*)p;
+  set_all_attrs<float2>();
+  set_all_attrs<double2>();
+  t.ready = true;
+  return t;
+}
+
+// ---------------------------------------------------------------- pass launcher
+template <int N, class C>
+static void launch_pass_n(int dir, int pro, int epi, const PassArgs& a, const DevVolume& v, const DevChains& ch,
+                          const C* tw, int nch, cudaStream_t s) {
+  const dim3 grid(cdiv_i((long long)a.A * a.B, TILE_LINES), a.chain_only >= 0 ? 1 : nch);
+  const dim3 block(PassCfg<N>::NT);
+  const size_t smem = (size_t)N * (TILE_LINES + 1) * sizeof(C);
+  if (dir < 0 && pro == PRO_LOAD && epi == EPI_STORE)
+    k_pass<N, -1, PRO_LOAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+  else if (dir > 0 && pro == PRO_LOAD && epi == EPI_STORE)
+    k_pass<N, +1, PRO_LOAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+  else if constexpr (sizeof(C) == 8) {
+    if (dir > 0 && pro == PRO_DATAGRAD && epi == EPI_STORE)
+      k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+    else if (dir < 0 && pro == PRO_LOAD && epi == EPI_GATHER)
+      k_pass<N, -1, PRO_LOAD, EPI_GATHER, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+    else
+      throw Error(DR_ERR_INVALID, "unsupported pass combination");
+  } else {
+    throw Error(DR_ERR_INVALID, "unsupported pass combination");
+  }
+  CK_LAUNCH();
+}
+
+template <class C>
+static void launch_pass(int n, int dir, int pro, int epi, const PassArgs& a, const DevVolume& v, const DevChains& ch,
+                        const C* tw, int nch, cudaStream_t s) {
+  switch (n) {
+    case 2: launch_pass_n<2, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 4: launch_pass_n<4, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 8: launch_pass_n<8, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 16: launch_pass_n<16, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 32: launch_pass_n<32, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 64: launch_pass_n<64, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 128: launch_pass_n<128, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 256: launch_pass_n<256, C>(dir, pro, epi, a, v, ch, tw, nch, s); break;
+    case 512:
+      if constexpr (sizeof(C) == 8) {
+        launch_pass_n<512, C>(dir, pro, epi, a, v, ch, tw, nch, s);
+        break;
+      }
+      [[fallthrough]];
+    default: throw Error(DR_ERR_UNSUPPORTED, "FFT length not supported: " + std::to_string(n));
+  }
+}
+
+static PassArgs pass_args(const void* in, void* out, long long in_cs, long long out_cs, int A, int B, int n_in,
+                          int n_out, double scale = 1.0, int step = -1, int sel = 0, int write_o = 0,
+                          int chain_only = -1) {
+  PassArgs a;
+  a.in = in; a.out = out; a.in_cs = in_cs; a.out_cs = out_cs;
+  a.A = A; a.B = B; a.n_in = n_in; a.n_out = n_out; a.scale = scale;
+  a.step = step; a.sel = sel; a.write_o = write_o; a.chain_only = chain_only;
+  return a;
+}
+
+// Unpruned in-place 3D FFT of one (or nch chain-strided) field(s).
+template <class C>
+static void fft3d(C* f, const int* E, int dir, long long cs, int nch, const C* tw, cudaStream_t s,
+                  const DevVolume& v, const DevChains& ch, int chain_only = -1) {
+  const int E0 = E[0], E1 = E[1], E2 = E[2];
+  if (dir < 0) {
+    launch_pass<C>(E0, -1, PRO_LOAD, EPI_STORE, pass_args(f, f, cs, cs, E1 * E2, 1, E0, E0, 1.0, -1, 0, 0, chain_only), v, ch, tw, nch, s);
+    launch_pass<C>(E1, -1, PRO_LOAD, EPI_STORE, pass_args(f, f, cs, cs, E2, E0, E1, E1, 1.0, -1, 0, 0, chain_only), v, ch, tw, nch, s);
+    launch_pass<C>(E2, -1, PRO_LOAD, EPI_STORE, pass_args(f, f, cs, cs, 1, E0 * E1, E2, E2, 1.0, -1, 0, 0, chain_only), v, ch, tw, nch, s);
+  } else {
+    launch_pass<C>(E0, +1, PRO_LOAD, EPI_STORE, pass_args(f, f, cs, cs, E1 * E2, 1, E0, E0, 1.0, -1, 0, 0, chain_only), v, ch, tw, nch, s);
+    launch_pass<C>(E1, +1, PRO_LOAD, EPI_STORE, pass_args(f, f, cs, cs, E2, E0, E1, E1, 1.0, -1, 0, 0, chain_only), v, ch, tw, nch, s);
+    launch_pass<C>(E2, +1, PRO_LOAD, EPI_STORE, pass_args(f, f, cs, cs, 1, E0 * E1, E2, E2, 1.0, -1, 0, 0, chain_only), v, ch, tw, nch, s);
+  }
+}
+
+// ---------------------------------------------------------------- volume
+struct Volume {
+  int device = 0;
+  HostVolume hv;
+  DevVolume dv{};
+  std::vector<void*> allocs;
+  double* lam_re = nullptr;
+  int n_S = 0;
+  double max_eig = 0.0;
+  double setup_seconds = 0.0;
+  int64_t bytes = 0;
+  const float2* tw_f = nullptr;
+  const double2* tw_d = nullptr;
+
+  template <class T>
+  T* alloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(p);
+    bytes += (int64_t)(n * sizeof(T));
+    return (T*)p;
+  }
+  template <class T>
+  T* upload(const std::vector<T>& h) {
+    T* d = alloc<T>(h.size());
+    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+  }
+  ~Volume() {
+    if (!allocs.empty()) {
+      cudaSetDevice(device);
+      for (void* p : allocs) cudaFree(p);
+    }
+  }
+};
+
+static void volume_build(Volume* V, const dr_volume_desc* d) {
+  const auto t0 = std::chrono::steady_clock::now();
+  V->device = d->device;
+  DeviceTables& dt = device_tables(d->device);
+  CK(cudaSetDevice(d->device));
+  V->tw_f = dt.tw_f;
+  V->tw_d = dt.tw_d;
+  std::string err;
+  const int rc = host_prepare(d, &V->hv, &err);
+  if (rc != DR_OK) throw Error(rc, err);
+  HostVolume& hv = V->hv;
+  DevVolume& dv = V->dv;
+  dv.E0 = hv.E[0]; dv.E1 = hv.E[1]; dv.E2 = hv.E[2]; dv.N = hv.N;
+  dv.bx = hv.box[0]; dv.by = hv.box[1]; dv.bz = hv.box[2];
+  dv.n_h = (int)hv.Yh.size(); dv.n_s = (int)hv.Ys.size(); dv.n_o = (int)hv.o_flat.size();
+  dv.box_to_d = V->upload(hv.box_to_d);
+  dv.box_to_o = V->upload(hv.box_to_o);
+  dv.d_flat = V->upload(hv.d_flat);
+  dv.o_flat = V->upload(hv.o_flat);
+  dv.Yh = V->upload(hv.Yh);
+  dv.Ys = V->upload(hv.Ys);
+  dv.w_rowptr = V->upload(hv.w_rowptr.empty() ? std::vector<int>{0} : hv.w_rowptr);
+  dv.w_col = V->upload(hv.w_col);
+  dv.w_val = V->upload(hv.w_val);
+  dv.wt_rowptr = V->upload(hv.wt_rowptr);
+  dv.wt_col = V->upload(hv.wt_col);
+  dv.wt_val = V->upload(hv.wt_val);
+
+  // eigenvalues in FP64: base -> 3 forward passes -> S, 1/lambda
+  const long long N = hv.N;
+  float* sinv = V->alloc<float>(N);
+  V->lam_re = V->alloc<double>(N);
+  double2* base = nullptr;
+  CK(cudaMalloc(&base, sizeof(double2) * N));
+  int* nS = nullptr;
+  CK(cudaMalloc(&nS, sizeof(int)));
+  try {
+    CK(cudaMemset(nS, 0, sizeof(int)));
+    const float* Q = hv.Q;
+    k_base<<<cdiv_i(N, 256), 256>>>(base, hv.E[0], hv.E[1], hv.E[2], Q[0], Q[1], Q[2], Q[4], Q[5], Q[6], Q[8], Q[9],
+                                      Q[10], (double)d->covariance[0], (double)d->covariance[1],
+                                      (double)d->covariance[2], d->covfun);
+    CK_LAUNCH();
+    DevChains none{};
+    fft3d<double2>(base, hv.E, -1, 0, 1, V->tw_d, 0, dv, none);
+    k_spectrum<<<cdiv_i(N, 256), 256>>>(base, sinv, V->lam_re, N, nS);
+    CK_LAUNCH();
+    double2 l0;
+    CK(cudaMemcpy(&l0, base, sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&V->n_S, nS, sizeof(int), cudaMemcpyDeviceToHost));
+    V->max_eig = l0.x / (double)N;
+  } catch (...) {
+    cudaFree(base);
+    cudaFree(nS);
+    throw;
+  }
+  cudaFree(base);
+  cudaFree(nS);
+  dv.sinv = sinv;
+  if ((long long)V->n_S >= N / 2) throw Error(DR_ERR_DOMAIN, "Too many negative eigen values");
+  CK(cudaDeviceSynchronize());
+  V->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ---------------------------------------------------------------- chainset
+struct Chainset {
+  Volume* vol = nullptr;
+  int C = 0;
+  dr_hmc_opts opts{};
+  DevChains dc{};
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int64_t graph_nodes = 0;
+  std::vector<void*> allocs;
+  float2* tmp = nullptr;        // [N] scratch for evaluation calls
+  double* tmp_part = nullptr;   // spectral-energy partials
+  int tmp_blocks = 0;
+  int NR = 1;
+
+  template <class T>
+  T* alloc(size_t n, bool zero = true) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(p);
+    if (zero) CK(cudaMemset(p, 0, n * sizeof(T)));
+    return (T*)p;
+  }
+  ~Chainset() {
+    if (vol) cudaSetDevice(vol->device);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) cudaStreamDestroy(stream);
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+static void launch_spmv(Chainset* S, int step, int sel, int chain_only, bool w) {
+  const DevVolume& v = S->vol->dv;
+  const int rows = w ? v.n_s : v.n_h;
+  const int nb = std::max(1, std::min(cdiv_i(rows, 8), w ? S->dc.nb_w : S->dc.nb_wt));
+#define SPMV(NR_)                                                                                                     \
+  if (w) k_spmv_w<NR_><<<nb, 256, 0, S->stream>>>(v, S->dc, step, sel, chain_only);                                   \
+  else k_spmv_wt<NR_><<<nb, 256, 0, S->stream>>>(v, S->dc, step, sel, chain_only);
+  switch (S->NR) {
+    case 1: SPMV(1); break;
+    case 2: SPMV(2); break;
+    case 4: SPMV(4); break;
+    default: SPMV(8); break;
+  }
+#undef SPMV
+  CK_LAUNCH();
+}
+
+static void launch_xline(Chainset* S, int step, int flags) {
+  const DevVolume& v = S->vol->dv;
+  const dim3 grid(cdiv_i((long long)v.E1 * v.E2, TILE_LINES), S->C);
+  const size_t smem = (size_t)v.E0 * (TILE_LINES + 1) * sizeof(float2);
+  const float2* tw = S->vol->tw_f;
+  switch (v.E0) {
+    case 2: k_xline<2><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 4: k_xline<4><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 8: k_xline<8><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 16: k_xline<16><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 32: k_xline<32><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 64: k_xline<64><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 128: k_xline<128><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 256: k_xline<256><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 512: k_xline<512><<<grid, 512, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    default: throw Error(DR_ERR_UNSUPPORTED, "E0 not supported");
+  }
+  CK_LAUNCH();
+}
+
+// The gradient/leapfrog sequence for steps 0..L (see kernels.cu header).
+static void enqueue_steps(Chainset* S, int L, int flags) {
+  const DevVolume& v = S->vol->dv;
+  const DevChains& ch = S->dc;
+  const float2* tw = S->vol->tw_f;
+  const int C = S->C;
+  for (int s = 0; s <= L; s++) {
+    const int sel = s == 0 ? 0 : 1;
+    if (s > 0) {
+      // forward y then z (pruned to the box), gather mu at data / output voxels
+      launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE,
+                          pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by, 1.0, s), v, ch, tw,
+                          C, S->stream);
+      launch_pass<float2>(v.E2, -1, PRO_LOAD, EPI_GATHER,
+                          pass_args(ch.T2, nullptr, ch.t2_stride, 0, 1, v.by * v.bx, v.E2, v.bz,
+                                    1.0 / (double)v.N, s, 1, 2),
+                          v, ch, tw, C, S->stream);
+    }
+    if (v.n_s > 0) launch_spmv(S, s, sel, -1, true);
+    launch_spmv(S, s, sel, -1, false);
+    // inverse z then y from the box back to the spectral planes
+    launch_pass<float2>(v.E2, +1, PRO_DATAGRAD, EPI_STORE,
+                        pass_args(nullptr, ch.T2, 0, ch.t2_stride, 1, v.by * v.bx, v.bz, v.E2, 1.0, s), v, ch, tw, C,
+                        S->stream);
+    launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE,
+                        pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1, 1.0, s), v, ch, tw,
+                        C, S->stream);
+    launch_xline(S, s, flags);
+  }
+}
+
+static void enqueue_iteration(Chainset* S) {
+  const DevVolume& v = S->vol->dv;
+  k_iter_begin<<<cdiv_i(S->C, 128), 128, 0, S->stream>>>(S->dc);
+  CK_LAUNCH();
+  enqueue_steps(S, S->opts.leapfrog, 0);
+  k_accept<<<S->C, 256, 0, S->stream>>>(v, S->dc);
+  CK_LAUNCH();
+  k_summary_max<<<S->C, 256, 0, S->stream>>>(v, S->dc);
+  CK_LAUNCH();
+  k_summary_acc<<<std::max(1, cdiv_i((long long)v.n_o * S->dc.Cp, 256)), 256, 0, S->stream>>>(v, S->dc);
+  CK_LAUNCH();
+}
+
+static void init_chain_states(Chainset* S) {
+  std::vector<ChainState> st(S->C);
+  const dr_hmc_opts& o = S->opts;
+  for (int c = 0; c < S->C; c++) {
+    ChainState h;
+    std::memset(&h, 0, sizeof(h));
+    // HMCParameters<float> constructor (HMCParameters.h:97-149)
+    h.warmup = o.burnin > 0;
+    h.eps_start_found = !h.warmup;
+    h.burnin = o.burnin;
+    h.integrator_steps = o.leapfrog;
+    h.iteration = 0;
+    h.n_save = o.nsave;
+    h.thin = o.thin == 0 ? 1 : o.thin;
+    h.A = 1;
+    h.eps0 = 1e-5;
+    const float e0 = o.starting_eps > 0 ? o.starting_eps : (float)(1.0 / o.leapfrog);
+    h.eps = std::max((double)e0, h.eps0);
+    h.eps_bar = 1;
+    h.gamma = (double)0.05f;
+    h.h_bar = 0;
+    h.mh_running_sum = 0;
+    h.mh_target = (double)o.mhtarget;
+    h.t0 = 10;
+    h.kappa = (double)0.75f;
+    h.acc = 0;
+    h.L_cur = -1;
+    h.done = o.nsave <= 0 ? 1 : 0;
+    st[c] = h;
+  }
+  CK(cudaMemcpy(S->dc.st, st.data(), sizeof(ChainState) * S->C, cudaMemcpyHostToDevice));
+}
+
+static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) {
+  if (C <= 0 || C > 256) throw Error(DR_ERR_UNSUPPORTED, "n_chains must be in [1, 256]");
+  if (!o) throw Error(DR_ERR_INVALID, "opts is NULL");
+  if (o->burnin < 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: burnin must be >= 0");
+  if (o->nsave < 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: n_save must be >= 0");
+  if (o->thin < 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: thin must be >= 0");
+  if (o->leapfrog <= 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: integrator_steps must be > 0");
+  if (!(o->mhtarget > 0 && o->mhtarget < 1)) throw Error(DR_ERR_DOMAIN, "HMCParameters: mh_target should be within (0, 1)");
+  S->vol = V;
+  S->C = C;
+  S->opts = *o;
+  CK(cudaSetDevice(V->device));
+  CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  const DevVolume& v = V->dv;
+  DevChains& ch = S->dc;
+  ch.C = C;
+  ch.Cp = C;
+  int cg = 1;
+  while (cg < C && cg < 32) cg <<= 1;
+  ch.CG = cg;
+  S->NR = cdiv_i(C, cg);
+  if (S->NR > 8) throw Error(DR_ERR_UNSUPPORTED, "too many chains");
+  if (S->NR == 3) S->NR = 4;
+  if (S->NR > 4 && S->NR < 8) S->NR = 8;
+  const long long N = v.N;
+  ch.U = S->alloc<float2>((size_t)C * 2 * N);
+  ch.Q = S->alloc<float2>((size_t)C * N);
+  ch.t1_stride = (long long)v.E2 * v.E1 * v.bx;
+  ch.t2_stride = (long long)v.E2 * v.by * v.bx;
+  ch.T1 = S->alloc<float2>((size_t)C * ch.t1_stride);
+  ch.T2 = S->alloc<float2>((size_t)C * ch.t2_stride);
+  ch.muD = S->alloc<float>((size_t)2 * v.n_h * C);
+  ch.muO = S->alloc<float>((size_t)2 * std::max(v.n_o, 1) * C);
+  ch.gD = S->alloc<float>((size_t)v.n_h * C);
+  ch.rs = S->alloc<float>((size_t)std::max(v.n_s, 1) * C);
+  ch.nb_x = cdiv_i((long long)v.E1 * v.E2, TILE_LINES);
+  ch.nb_w = std::max(1, std::min(cdiv_i(v.n_s, 8), 148 * 8));
+  ch.nb_wt = std::max(1, std::min(cdiv_i(v.n_h, 8), 148 * 8));
+  ch.maxblk = std::max(ch.nb_x, std::max(ch.nb_w, ch.nb_wt));
+  ch.part = S->alloc<double>((size_t)C * NSLOT * ch.maxblk);
+  ch.st = S->alloc<ChainState>(C);
+  ch.s1 = S->alloc<double>((size_t)std::max(v.n_o, 1) * C);
+  ch.s2 = S->alloc<double>((size_t)std::max(v.n_o, 1) * C);
+  ch.sa = S->alloc<double>((size_t)std::max(v.n_o, 1) * C);
+  ch.samples = o->store_samples ? S->alloc<float>((size_t)std::max(o->nsave, 1) * std::max(v.n_o, 1) * C, false) : nullptr;
+  ch.seed = o->seed;
+  ch.chain0 = 0;
+  S->tmp = S->alloc<float2>(N);
+  S->tmp_blocks = 296;
+  S->tmp_part = S->alloc<double>(S->tmp_blocks);
+  init_chain_states(S);
+
+  // initial state: sigma, then u0 = IFFT(scatter(Yh)) + sqrt(N lambda) w / 10, then mu at data/output voxels
+  const float2* tw = V->tw_f;
+  cudaStream_t s = S->stream;
+  k_init_sigma<<<cdiv_i(C, 128), 128, 0, s>>>(ch, V->hv.theta[0] > 0 ? (float)V->hv.theta[0] : 1.0f, v.n_s > 0 ? 2 : 1);
+  CK_LAUNCH();
+  k_fill_gD<<<std::max(1, cdiv_i((long long)v.n_h * C, 256)), 256, 0, s>>>(v, ch);
+  CK_LAUNCH();
+  launch_pass<float2>(v.E2, +1, PRO_DATAGRAD, EPI_STORE, pass_args(nullptr, ch.T2, 0, ch.t2_stride, 1, v.by * v.bx, v.bz, v.E2), v, ch, tw, C, s);
+  launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE, pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1), v, ch, tw, C, s);
+  launch_pass<float2>(v.E0, +1, PRO_LOAD, EPI_STORE, pass_args(ch.T1, ch.U, ch.t1_stride, 2 * N, v.E2 * v.E1, 1, v.bx, v.E0), v, ch, tw, C, s);
+  k_init_prior<<<dim3(std::max(1, cdiv_i(N / 2, 256)), C), 256, 0, s>>>(v, ch);
+  CK_LAUNCH();
+  launch_pass<float2>(v.E0, -1, PRO_LOAD, EPI_STORE, pass_args(ch.U, ch.T1, 2 * N, ch.t1_stride, v.E2 * v.E1, 1, v.E0, v.bx), v, ch, tw, C, s);
+  launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE, pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by), v, ch, tw, C, s);
+  launch_pass<float2>(v.E2, -1, PRO_LOAD, EPI_GATHER, pass_args(ch.T2, nullptr, ch.t2_stride, 0, 1, v.by * v.bx, v.E2, v.bz, 1.0 / (double)N, -1, 0, 1), v, ch, tw, C, s);
+  CK(cudaStreamSynchronize(s));
+}
+
+static void read_states(Chainset* S, std::vector<ChainState>* st) {
+  st->resize(S->C);
+  CK(cudaMemcpyAsync(st->data(), S->dc.st, sizeof(ChainState) * S->C, cudaMemcpyDeviceToHost, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
+}
+static void write_states(Chainset* S, const std::vector<ChainState>& st) {
+  CK(cudaMemcpyAsync(S->dc.st, st.data(), sizeof(ChainState) * S->C, cudaMemcpyHostToDevice, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
+}
+
+static void step(Chainset* S, int iters) {
+  CK(cudaSetDevice(S->vol->device));
+  if (!S->graph) {
+    cudaGraph_t g = nullptr;
+    const int64_t before = g_launches;
+    CK(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_iteration(S);
+    } catch (...) {
+      cudaStreamEndCapture(S->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(S->stream, &g));
+    S->graph_nodes = g_launches - before;
+    g_launches = before;
+    const cudaError_t e = cudaGraphInstantiate(&S->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw Error(DR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  }
+  for (int i = 0; i < iters; i++) {
+    CK(cudaGraphLaunch(S->graph, S->stream));
+    g_launches += S->graph_nodes;
+  }
+  CK(cudaStreamSynchronize(S->stream));
+}
+
+// Spectral state of chain c from a real-space field (host, 2N floats).
+static void upload_field(Chainset* S, const float* mu) {
+  CK(cudaMemcpyAsync(S->tmp, mu, sizeof(float2) * S->vol->dv.N, cudaMemcpyHostToDevice, S->stream));
+}
+
+static void gather_data(Chainset* S, const float2* field, int c, int half, bool with_output) {
+  const DevVolume& v = S->vol->dv;
+  k_gather_re<<<cdiv_i(v.n_h, 256), 256, 0, S->stream>>>(field, v.d_flat, v.n_h, S->dc.muD + (long long)half * v.n_h * S->C, S->C, c);
+  CK_LAUNCH();
+  if (with_output && v.n_o > 0) {
+    k_gather_re<<<cdiv_i(v.n_o, 256), 256, 0, S->stream>>>(field, v.o_flat, v.n_o, S->dc.muO + (long long)half * v.n_o * S->C, S->C, c);
+    CK_LAUNCH();
+  }
+}
+
+static double spectral_energy(Chainset* S, const float2* u, float sh, int mode) {
+  const DevVolume& v = S->vol->dv;
+  k_spectral_energy<<<S->tmp_blocks, 256, 0, S->stream>>>(u, v.sinv, v.N, sh, mode, S->tmp_part);
+  CK_LAUNCH();
+  std::vector<double> h(S->tmp_blocks);
+  CK(cudaMemcpyAsync(h.data(), S->tmp_part, sizeof(double) * S->tmp_blocks, cudaMemcpyDeviceToHost, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
+  double s = 0.0;
+  for (double x : h) s += x;
+  return s;
+}
+
+static double part_sum(Chainset* S, int c, int slot, int nb) {
+  std::vector<double> h(nb);
+  CK(cudaMemcpyAsync(h.data(), S->dc.part + ((long long)c * NSLOT + slot) * S->dc.maxblk, sizeof(double) * nb,
+                     cudaMemcpyDeviceToHost, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
+  double s = 0.0;
+  for (double x : h) s += x;
+  return s;
+}
+
+// data-term residual norms and gD for chain c from muD half `half` (sel relative to acc)
+static void data_term(Chainset* S, int c, int sel) {
+  if (S->vol->dv.n_s > 0) launch_spmv(S, -1, sel, c, true);
+  launch_spmv(S, -1, sel, c, false);
+}
+
+}  // namespace drb
+
+// ==================================================================== C ABI
+using namespace drb;
+
+struct dr_volume : Volume {};
+struct dr_chainset : Chainset {};
+
+#define API_BEGIN try {
+#define API_END                                                     \
+  }                                                                 \
+  catch (const Error& e) {                                          \
+    g_err = e.what();                                               \
+    return e.code;                                                  \
+  }                                                                 \
+  catch (const std::bad_alloc&) {                                   \
+    g_err = "host allocation failed";                               \
+    return DR_ERR_NOMEM;                                            \
+  }                                                                 \
+  catch (const std::exception& e) {                                 \
+    g_err = e.what();                                               \
+    return DR_ERR_INVALID;                                          \
+  }                                                                 \
+  return DR_OK;
+
+extern "C" {
+
+const char* dr_last_error(void) { return g_err.c_str(); }
+const char* dr_version(void) { return "dualres_b200 0.1 (sm_100a)"; }
+int64_t dr_kernel_launches(int reset) {
+  const int64_t n = g_launches;
+  if (reset) g_launches = 0;
+  return n;
+}
+
+int dr_volume_create(const dr_volume_desc* desc, dr_volume** out) {
+  API_BEGIN
+  if (!desc || !out) throw Error(DR_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  dr_volume* v = new dr_volume();
+  try {
+    volume_build(v, desc);
+  } catch (...) {
+    delete v;
+    throw;
+  }
+  *out = v;
+  API_END
+}
+
+int dr_volume_info_get(const dr_volume* v, dr_volume_info* info) {
+  API_BEGIN
+  if (!v || !info) throw Error(DR_ERR_INVALID, "NULL argument");
+  std::memset(info, 0, sizeof(*info));
+  for (int k = 0; k < 3; k++) { info->E[k] = v->hv.E[k]; info->box[k] = v->hv.box[k]; }
+  info->N = v->hv.N;
+  info->n_highres = v->dv.n_h;
+  info->n_stdres = v->dv.n_s;
+  info->n_output = v->dv.n_o;
+  info->kriging_nnz = (int64_t)v->hv.w_col.size();
+  info->n_nonpositive = v->n_S;
+  info->max_eigenvalue = v->max_eig;
+  info->setup_seconds = v->setup_seconds;
+  info->kriging_seconds = v->hv.kriging_seconds;
+  info->neighborhood = v->hv.radius;
+  info->device_bytes = v->bytes;
+  API_END
+}
+
+int dr_volume_kriging_get(const dr_volume* v, int* rowptr, int* col, float* val) {
+  API_BEGIN
+  if (!v) throw Error(DR_ERR_INVALID, "NULL volume");
+  if (rowptr && !v->hv.w_rowptr.empty()) std::memcpy(rowptr, v->hv.w_rowptr.data(), sizeof(int) * v->hv.w_rowptr.size());
+  if (col && !v->hv.w_col.empty()) std::memcpy(col, v->hv.w_col.data(), sizeof(int) * v->hv.w_col.size());
+  if (val && !v->hv.w_val.empty()) std::memcpy(val, v->hv.w_val.data(), sizeof(float) * v->hv.w_val.size());
+  API_END
+}
+
+int dr_volume_lambda_get(const dr_volume* v, double* lam) {
+  API_BEGIN
+  if (!v || !lam) throw Error(DR_ERR_INVALID, "NULL argument");
+  CK(cudaSetDevice(v->device));
+  CK(cudaMemcpy(lam, v->lam_re, sizeof(double) * v->hv.N, cudaMemcpyDeviceToHost));
+  API_END
+}
+
+int dr_volume_indices_get(const dr_volume* v, int* data_idx, int* out_idx) {
+  API_BEGIN
+  if (!v) throw Error(DR_ERR_INVALID, "NULL volume");
+  if (data_idx) std::memcpy(data_idx, v->hv.d_flat.data(), sizeof(int) * v->hv.d_flat.size());
+  if (out_idx && !v->hv.o_flat.empty()) std::memcpy(out_idx, v->hv.o_flat.data(), sizeof(int) * v->hv.o_flat.size());
+  API_END
+}
+
+int dr_volume_data_get(const dr_volume* v, float* Yh, float* Ys) {
+  API_BEGIN
+  if (!v) throw Error(DR_ERR_INVALID, "NULL volume");
+  if (Yh) std::memcpy(Yh, v->hv.Yh.data(), sizeof(float) * v->hv.Yh.size());
+  if (Ys && !v->hv.Ys.empty()) std::memcpy(Ys, v->hv.Ys.data(), sizeof(float) * v->hv.Ys.size());
+  API_END
+}
+
+void dr_volume_destroy(dr_volume* v) { delete v; }
+
+int dr_chainset_create(dr_volume* v, int n_chains, const dr_hmc_opts* opts, dr_chainset** out) {
+  API_BEGIN
+  if (!v || !out) throw Error(DR_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  dr_chainset* s = new dr_chainset();
+  try {
+    chainset_build(s, v, n_chains, opts);
+  } catch (...) {
+    delete s;
+    throw;
+  }
+  *out = s;
+  API_END
+}
+
+void dr_chainset_destroy(dr_chainset* s) { delete s; }
+
+int dr_step(dr_chainset* s, int iterations) {
+  API_BEGIN
+  if (!s || iterations < 0) throw Error(DR_ERR_INVALID, "bad argument");
+  step(s, iterations);
+  API_END
+}
+
+int dr_run(dr_chainset* s) {
+  API_BEGIN
+  if (!s) throw Error(DR_ERR_INVALID, "NULL chainset");
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const int total = s->opts.burnin + (s->opts.thin == 0 ? 1 : s->opts.thin) * s->opts.nsave;
+  int it = 0;
+  for (const auto& h : st) it = std::max(it, h.iteration);
+  if (total > it) step(s, total - it);
+  API_END
+}
+
+int dr_chain_stats_get(dr_chainset* s, dr_chain_stats* out) {
+  API_BEGIN
+  if (!s || !out) throw Error(DR_ERR_INVALID, "NULL argument");
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  for (int c = 0; c < s->C; c++) {
+    const ChainState& h = st[c];
+    dr_chain_stats& o = out[c];
+    o.iteration = h.iteration;
+    o.saved = h.saved;
+    o.integrator_steps = h.eps_start_found ? h.integrator_steps : 1;
+    o.eps = (float)h.eps;
+    const int d = h.iteration - h.burnin;
+    o.mh_rate = (float)(h.mh_running_sum / std::max(d, 1));
+    o.sigma_hr = std::sqrt(1.0f / h.sh);
+    o.sigma_sr = std::sqrt(1.0f / h.ss);
+    o.last_log_ratio = h.last_log_ratio;
+    o.accepted = h.accepted;
+    o.grad_evals = h.grad_evals;
+    o.done = h.done;
+  }
+  API_END
+}
+
+int dr_summary_get(dr_chainset* s, int chain, float* mean, float* var, float* activation) {
+  API_BEGIN
+  if (!s || chain < -1 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad chain");
+  const DevVolume& v = s->vol->dv;
+  const size_t n = (size_t)v.n_o * s->C;
+  std::vector<double> s1(n), s2(n), sa(n);
+  CK(cudaSetDevice(s->vol->device));
+  CK(cudaMemcpy(s1.data(), s->dc.s1, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(s2.data(), s->dc.s2, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sa.data(), s->dc.sa, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const int c0 = chain < 0 ? 0 : chain, c1 = chain < 0 ? s->C : chain + 1;
+  double ns = 0.0;
+  for (int c = c0; c < c1; c++) ns += st[c].saved;
+  if (ns <= 0) ns = 1;  // mcmc_summary::samples() (gaussian_process_model.h:255-258)
+  std::vector<double> act(v.n_o);
+  double amax = -1e300;
+  for (int o = 0; o < v.n_o; o++) {
+    double a1 = 0, a2 = 0, aa = 0;
+    for (int c = c0; c < c1; c++) {
+      a1 += s1[(size_t)o * s->C + c];
+      a2 += s2[(size_t)o * s->C + c];
+      aa += sa[(size_t)o * s->C + c];
+    }
+    const double m = a1 / ns, vr = (a2 - a1 * a1 / ns) / ns;
+    if (mean) mean[o] = (float)m;
+    if (var) var[o] = (float)vr;
+    act[o] = aa / (ns * std::sqrt(vr));
+    amax = std::max(amax, act[o]);
+  }
+  if (activation)
+    for (int o = 0; o < v.n_o; o++) activation[o] = (float)(act[o] / amax);
+  API_END
+}
+
+int dr_samples_get(dr_chainset* s, int chain, float* samples, int max_saved, int* n_saved) {
+  API_BEGIN
+  if (!s || chain < 0 || chain >= s->C || !n_saved) throw Error(DR_ERR_INVALID, "bad argument");
+  if (!s->dc.samples) throw Error(DR_ERR_STATE, "samples were not stored (store_samples = 0)");
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const int ns = std::min(st[chain].saved, max_saved);
+  *n_saved = ns;
+  const DevVolume& v = s->vol->dv;
+  const size_t per = (size_t)v.n_o * s->C;
+  std::vector<float> buf(per);
+  for (int i = 0; i < ns; i++) {
+    CK(cudaMemcpy(buf.data(), s->dc.samples + i * per, sizeof(float) * per, cudaMemcpyDeviceToHost));
+    for (int o = 0; o < v.n_o; o++) samples[(size_t)i * v.n_o + o] = buf[(size_t)o * s->C + chain];
+  }
+  API_END
+}
+
+int dr_set_state(dr_chainset* s, int chain, const float* mu, float s_hr, float s_sr) {
+  API_BEGIN
+  if (!s || !mu || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(s->vol->device));
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const DevVolume& v = s->vol->dv;
+  const int acc = st[chain].acc;
+  upload_field(s, mu);
+  gather_data(s, s->tmp, chain, acc, true);
+  DevChains none{};
+  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
+  CK(cudaMemcpyAsync(s->dc.U + ((long long)chain * 2 + acc) * v.N, s->tmp, sizeof(float2) * v.N,
+                     cudaMemcpyDeviceToDevice, s->stream));
+  st[chain].sh = s_hr;
+  st[chain].ss = s_sr;
+  write_states(s, st);
+  API_END
+}
+
+int dr_get_state(dr_chainset* s, int chain, float* mu, float* s2inv) {
+  API_BEGIN
+  if (!s || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(s->vol->device));
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const DevVolume& v = s->vol->dv;
+  if (mu) {
+    CK(cudaMemcpyAsync(s->tmp, s->dc.U + ((long long)chain * 2 + st[chain].acc) * v.N, sizeof(float2) * v.N,
+                       cudaMemcpyDeviceToDevice, s->stream));
+    DevChains none{};
+    fft3d<float2>(s->tmp, s->vol->hv.E, -1, 0, 1, s->vol->tw_f, s->stream, v, none);
+    k_scale<<<cdiv_i(v.N, 256), 256, 0, s->stream>>>(s->tmp, v.N, 1.0f / (float)v.N);
+    CK_LAUNCH();
+    CK(cudaMemcpyAsync(mu, s->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  if (s2inv) { s2inv[0] = st[chain].sh; s2inv[1] = st[chain].ss; }
+  API_END
+}
+
+int dr_log_posterior(dr_chainset* s, int chain, const float* mu, double* out) {
+  API_BEGIN
+  if (!s || !mu || !out || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(s->vol->device));
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const DevVolume& v = s->vol->dv;
+  const ChainState& h = st[chain];
+  upload_field(s, mu);
+  gather_data(s, s->tmp, chain, h.acc ^ 1, false);
+  data_term(s, chain, 1);
+  const double Rh = part_sum(s, chain, SL_RH0, s->dc.nb_wt);
+  const double Rs = v.n_s > 0 ? part_sum(s, chain, SL_RS0, s->dc.nb_w) : 0.0;
+  DevChains none{};
+  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
+  const double e = spectral_energy(s, s->tmp, h.sh, 0);
+  out[0] = -0.5 * e / (double)v.N;
+  out[1] = -0.5 * ((double)h.sh * Rh + (v.n_s > 0 ? (double)h.ss * Rs : 0.0));
+  API_END
+}
+
+int dr_gradient(dr_chainset* s, int chain, const float* mu, float* grad) {
+  API_BEGIN
+  if (!s || !mu || !grad || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(s->vol->device));
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const DevVolume& v = s->vol->dv;
+  upload_field(s, mu);
+  gather_data(s, s->tmp, chain, st[chain].acc ^ 1, false);
+  data_term(s, chain, 1);
+  DevChains none{};
+  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
+  k_prior_grad_spectral<<<cdiv_i(v.N, 256), 256, 0, s->stream>>>(s->tmp, v.sinv, v.N);
+  CK_LAUNCH();
+  fft3d<float2>(s->tmp, s->vol->hv.E, -1, 0, 1, s->vol->tw_f, s->stream, v, none);
+  k_scatter_add_re<<<cdiv_i(v.n_h, 256), 256, 0, s->stream>>>(s->tmp, v.d_flat, v.n_h, s->dc.gD, s->C, chain);
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(grad, s->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  API_END
+}
+
+int dr_leapfrog_fixed(dr_chainset* s, int chain, const float* mu0, const float* p0, float eps, int L, float* mu_out,
+                      float* p_out, double* energies) {
+  API_BEGIN
+  if (!s || !mu0 || !p0 || chain < 0 || chain >= s->C || L <= 0) throw Error(DR_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(s->vol->device));
+  std::vector<ChainState> st, saved;
+  read_states(s, &st);
+  saved = st;
+  const DevVolume& v = s->vol->dv;
+  const int acc = st[chain].acc;
+  DevChains none{};
+  // u0 and the data values of mu0
+  upload_field(s, mu0);
+  gather_data(s, s->tmp, chain, acc, false);
+  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
+  CK(cudaMemcpyAsync(s->dc.U + ((long long)chain * 2 + acc) * v.N, s->tmp, sizeof(float2) * v.N,
+                     cudaMemcpyDeviceToDevice, s->stream));
+  // q0 = IFFT(p0)
+  upload_field(s, p0);
+  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
+  CK(cudaMemcpyAsync(s->dc.Q + (long long)chain * v.N, s->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToDevice,
+                     s->stream));
+  for (int c = 0; c < s->C; c++) st[c].L_cur = -1;
+  st[chain].L_cur = L;
+  st[chain].eps_cur = eps;
+  write_states(s, st);
+  enqueue_steps(s, L, XF_FIXED_MOMENTUM | XF_WRITE_Q_LAST);
+  CK(cudaStreamSynchronize(s->stream));
+  const double N = (double)v.N;
+  const double sh = st[chain].sh, ss = st[chain].ss;
+  if (energies) {
+    const double K0 = part_sum(s, chain, SL_E0, s->dc.nb_x), lp0 = part_sum(s, chain, SL_LP0, s->dc.nb_x);
+    const double Rh0 = part_sum(s, chain, SL_RH0, s->dc.nb_wt), RhL = part_sum(s, chain, SL_RHL, s->dc.nb_wt);
+    const double Rs0 = v.n_s > 0 ? part_sum(s, chain, SL_RS0, s->dc.nb_w) : 0.0;
+    const double RsL = v.n_s > 0 ? part_sum(s, chain, SL_RSL, s->dc.nb_w) : 0.0;
+    const double lpL = part_sum(s, chain, SL_LPL, s->dc.nb_x), KL = part_sum(s, chain, SL_KL, s->dc.nb_x);
+    energies[0] = -0.5 * lp0 / N;
+    energies[1] = -0.5 * (sh * Rh0 + ss * Rs0);
+    energies[2] = -0.5 * K0 / N;
+    energies[3] = -0.5 * lpL / N;
+    energies[4] = -0.5 * (sh * RhL + ss * RsL);
+    energies[5] = -0.5 * KL / N;
+  }
+  if (mu_out) {
+    CK(cudaMemcpyAsync(s->tmp, s->dc.U + ((long long)chain * 2 + (acc ^ 1)) * v.N, sizeof(float2) * v.N,
+                       cudaMemcpyDeviceToDevice, s->stream));
+    fft3d<float2>(s->tmp, s->vol->hv.E, -1, 0, 1, s->vol->tw_f, s->stream, v, none);
+    k_scale<<<cdiv_i(v.N, 256), 256, 0, s->stream>>>(s->tmp, v.N, 1.0f / (float)v.N);
+    CK_LAUNCH();
+    CK(cudaMemcpyAsync(mu_out, s->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToHost, s->stream));
+  }
+  if (p_out) {
+    CK(cudaMemcpyAsync(s->tmp, s->dc.Q + (long long)chain * v.N, sizeof(float2) * v.N, cudaMemcpyDeviceToDevice,
+                       s->stream));
+    fft3d<float2>(s->tmp, s->vol->hv.E, -1, 0, 1, s->vol->tw_f, s->stream, v, none);
+    k_scale<<<cdiv_i(v.N, 256), 256, 0, s->stream>>>(s->tmp, v.N, 1.0f / (float)v.N);
+    CK_LAUNCH();
+    CK(cudaMemcpyAsync(p_out, s->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToHost, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  // the chain keeps mu0 as its state; the other chains are untouched
+  for (int c = 0; c < s->C; c++) saved[c].L_cur = -1;
+  write_states(s, saved);
+  API_END
+}
+
+int dr_kriging_matrix(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy,
+                      int sz, const float* Qsr, const float* theta, float radius, int* n_rows, int64_t* nnz,
+                      int** rowptr, int** col, float** val) {
+  API_BEGIN
+  if (!hr || !Qhr || !sr || !Qsr || !theta || !n_rows || !nnz || !rowptr || !col || !val)
+    throw Error(DR_ERR_INVALID, "NULL argument");
+  if (nx <= 0 || ny <= 0 || nz <= 0 || sx <= 0 || sy <= 0 || sz <= 0) throw Error(DR_ERR_INVALID, "bad grid");
+  std::vector<int> rp, cl;
+  std::vector<float> vl;
+  std::string err;
+  int nofs = 0;
+  const int rc = kriging_build(hr, nx, ny, nz, Qhr, sr, sx, sy, sz, Qsr, theta, radius, &rp, &cl, &vl, &nofs, &err);
+  if (rc != DR_OK) throw Error(rc, err);
+  *n_rows = (int)rp.size() - 1;
+  *nnz = (int64_t)cl.size();
+  *rowptr = (int*)std::malloc(sizeof(int) * rp.size());
+  *col = (int*)std::malloc(sizeof(int) * std::max<size_t>(cl.size(), 1));
+  *val = (float*)std::malloc(sizeof(float) * std::max<size_t>(vl.size(), 1));
+  if (!*rowptr || !*col || !*val) {
+    std::free(*rowptr); std::free(*col); std::free(*val);
+    throw Error(DR_ERR_NOMEM, "host allocation failed");
+  }
+  std::memcpy(*rowptr, rp.data(), sizeof(int) * rp.size());
+  if (!cl.empty()) std::memcpy(*col, cl.data(), sizeof(int) * cl.size());
+  if (!vl.empty()) std::memcpy(*val, vl.data(), sizeof(float) * vl.size());
+  API_END
+}
+
+void dr_free(void* p) { std::free(p); }
+
+int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starting_eps, float mhtarget, int n,
+                            const float* rates, double* eps_out, int* steps_out, int device) {
+  API_BEGIN
+  if (n < 0 || !rates || !eps_out || !steps_out) throw Error(DR_ERR_INVALID, "bad argument");
+  device_tables(device);
+  CK(cudaSetDevice(device));
+  ChainState h;
+  std::memset(&h, 0, sizeof(h));
+  h.warmup = burnin > 0;
+  h.eps_start_found = !h.warmup;
+  h.burnin = burnin;
+  h.integrator_steps = L;
+  h.n_save = nsave;
+  h.thin = thin == 0 ? 1 : thin;
+  h.A = 1;
+  h.eps0 = 1e-5;
+  h.eps = std::max((double)starting_eps, h.eps0);
+  h.eps_bar = 1;
+  h.gamma = (double)0.05f;
+  h.mh_target = (double)mhtarget;
+  h.t0 = 10;
+  h.kappa = (double)0.75f;
+  float* dr = nullptr;
+  double* de = nullptr;
+  int* ds = nullptr;
+  CK(cudaMalloc(&dr, sizeof(float) * std::max(n, 1)));
+  CK(cudaMalloc(&de, sizeof(double) * std::max(n, 1)));
+  CK(cudaMalloc(&ds, sizeof(int) * std::max(n, 1)));
+  cudaError_t e = cudaMemcpy(dr, rates, sizeof(float) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_debug_dual_averaging<<<1, 32>>>(h, n, dr, de, ds);
+    e = cudaGetLastError();
+    g_launches++;
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(eps_out, de, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(steps_out, ds, sizeof(int) * n, cudaMemcpyDeviceToHost);
+  cudaFree(dr);
+  cudaFree(de);
+  cudaFree(ds);
+  if (e != cudaSuccess) throw Error(DR_ERR_CUDA, cudaGetErrorString(e));
+  API_END
+}
+
+}  // extern "C"

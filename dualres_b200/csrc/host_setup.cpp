@@ -1,0 +1,483 @@
+// One-time host set-up of a volume (images -> indices -> kriging CSR).
+//
+// Restates src/dualgpm.cpp:125-245, 288 (masking, covariance checks, default
+// neighbourhood), gaussian_process_model.h:104-117 (input bounding box, data
+// and output indices), MultiResParameters.h:191-206, 287-289, 647-667 (grid,
+// embedding, flat indices) and kriging_matrix.h:41-343 (the kriging matrix).
+// The sparsity pattern follows the reference step by step (offset order,
+// truncation, flat-offset bounds check, ordinal map), so it is bit-exact for
+// inputs without borderline truncations.  The weights are solved in FP64
+// (blocked Cholesky, column-pivoted Householder QR when the sub-matrix is not
+// numerically positive definite) where the reference uses FP32
+// colPivHouseholderQr.
+#include "host_setup.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace drb {
+
+static inline bool has_data(float v) { return !(std::isnan(v) || v == 0.0f); }
+
+// ---------------------------------------------------------------- dense solves
+// In-place lower Cholesky of the m x m row-major SPD matrix A (blocked,
+// right-looking).  Returns false when a pivot is not positive.
+static bool cholesky(double* A, int m) {
+  const int NB = 64;
+  for (int kb = 0; kb < m; kb += NB) {
+    const int ke = std::min(m, kb + NB);
+    for (int j = kb; j < ke; j++) {
+      double* Aj = A + (size_t)j * m;
+      double d = Aj[j];
+      for (int p = kb; p < j; p++) d -= Aj[p] * Aj[p];
+      if (!(d > 0.0)) return false;
+      const double ljj = std::sqrt(d);
+      Aj[j] = ljj;
+      const double inv = 1.0 / ljj;
+      for (int i = j + 1; i < m; i++) {
+        double* Ai = A + (size_t)i * m;
+        double s = Ai[j];
+        for (int p = kb; p < j; p++) s -= Ai[p] * Aj[p];
+        Ai[j] = s * inv;
+      }
+    }
+    // trailing update A22 -= L21 L21^T (lower triangle), rows in groups of 4
+    const int w = ke - kb;
+    for (int i = ke; i < m; i += 4) {
+      const int ni = std::min(4, m - i);
+      const double* r[4];
+      for (int t = 0; t < 4; t++) r[t] = A + (size_t)(i + std::min(t, ni - 1)) * m + kb;
+      const int jmax = i + ni - 1;
+      for (int j = ke; j <= jmax; j++) {
+        const double* rj = A + (size_t)j * m + kb;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int p = 0; p < w; p++) {
+          const double x = rj[p];
+          s0 += r[0][p] * x;
+          s1 += r[1][p] * x;
+          s2 += r[2][p] * x;
+          s3 += r[3][p] * x;
+        }
+        const double s[4] = {s0, s1, s2, s3};
+        for (int t = 0; t < ni; t++)
+          if (j <= i + t) A[(size_t)(i + t) * m + j] -= s[t];
+      }
+    }
+  }
+  return true;
+}
+
+static void cholesky_solve(const double* L, int m, double* b) {
+  for (int i = 0; i < m; i++) {
+    const double* Li = L + (size_t)i * m;
+    double s = b[i];
+    for (int p = 0; p < i; p++) s -= Li[p] * b[p];
+    b[i] = s / Li[i];
+  }
+  for (int i = m - 1; i >= 0; i--) {
+    double s = b[i];
+    for (int p = i + 1; p < m; p++) s -= L[(size_t)p * m + i] * b[p];
+    b[i] = s / L[(size_t)i * m + i];
+  }
+}
+
+// Column-pivoted Householder QR solve (A destroyed); components beyond the
+// numerical rank are zero (basic solution).
+static void qr_solve(double* A, int m, double* b, double* x) {
+  std::vector<int> perm(m);
+  std::vector<double> v(m), y(m, 0.0);
+  for (int j = 0; j < m; j++) perm[j] = j;
+  int rank = m;
+  double r00 = 0.0;
+  for (int k = 0; k < m; k++) {
+    int best = k;
+    double bn = -1.0;
+    for (int j = k; j < m; j++) {
+      double s = 0.0;
+      for (int i = k; i < m; i++) s += A[(size_t)i * m + j] * A[(size_t)i * m + j];
+      if (s > bn) { bn = s; best = j; }
+    }
+    if (best != k) {
+      for (int i = 0; i < m; i++) std::swap(A[(size_t)i * m + k], A[(size_t)i * m + best]);
+      std::swap(perm[k], perm[best]);
+    }
+    double alpha = std::sqrt(bn);
+    if (k == 0) r00 = alpha;
+    if (alpha <= (double)m * 2.220446049250313e-16 * r00) { rank = k; break; }
+    if (A[(size_t)k * m + k] > 0) alpha = -alpha;
+    double vn = 0.0;
+    for (int i = k; i < m; i++) v[i] = A[(size_t)i * m + k];
+    v[k] -= alpha;
+    for (int i = k; i < m; i++) vn += v[i] * v[i];
+    if (vn > 0.0) {
+      for (int j = k; j < m; j++) {
+        double s = 0.0;
+        for (int i = k; i < m; i++) s += v[i] * A[(size_t)i * m + j];
+        s = 2.0 * s / vn;
+        for (int i = k; i < m; i++) A[(size_t)i * m + j] -= s * v[i];
+      }
+      double s = 0.0;
+      for (int i = k; i < m; i++) s += v[i] * b[i];
+      s = 2.0 * s / vn;
+      for (int i = k; i < m; i++) b[i] -= s * v[i];
+    }
+  }
+  for (int i = rank - 1; i >= 0; i--) {
+    double s = b[i];
+    for (int j = i + 1; j < rank; j++) s -= A[(size_t)i * m + j] * y[j];
+    y[i] = s / A[(size_t)i * m + i];
+  }
+  for (int j = 0; j < m; j++) x[perm[j]] = y[j];
+}
+
+static double rbf(double d, const double* th) { return th[0] * std::exp(-th[1] * std::pow(std::fabs(d), th[2])); }
+
+// ---------------------------------------------------------------- neighbourhood
+// kriging_matrix.h:63-106 in float arithmetic (voxel dims = column norms of Q,
+// nifti_manipulation.inl:600-605), offsets i fastest (kriging_matrix.h:41-56).
+static int neighbourhood(const float* Q, float radius, std::vector<int>* P) {
+  float vd[3];
+  int nr[3];
+  for (int c = 0; c < 3; c++) {
+    float s = 0.0f;
+    for (int r = 0; r < 4; r++) s += Q[4 * r + c] * Q[4 * r + c];
+    vd[c] = std::sqrt(s);
+    nr[c] = (int)(radius / vd[c]);
+  }
+  P->clear();
+  long total = 0, inside = 0;
+  for (int k = -nr[2]; k <= nr[2]; k++)
+    for (int j = -nr[1]; j <= nr[1]; j++)
+      for (int i = -nr[0]; i <= nr[0]; i++) {
+        total++;
+        float q2 = 0.0f;
+        for (int r = 0; r < 3; r++) {
+          const float q = Q[4 * r + 0] * (float)i + Q[4 * r + 1] * (float)j + Q[4 * r + 2] * (float)k;
+          q2 += q * q;
+        }
+        if (std::sqrt(q2) <= radius) {
+          P->push_back(i); P->push_back(j); P->push_back(k);
+          inside++;
+        }
+      }
+  return (int)inside;
+}
+
+static void mat4_inverse(const double* a, double* inv) {
+  double m[4][8];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) { m[i][j] = a[4 * i + j]; m[i][j + 4] = i == j ? 1.0 : 0.0; }
+  for (int c = 0; c < 4; c++) {
+    int p = c;
+    for (int r = c + 1; r < 4; r++) if (std::fabs(m[r][c]) > std::fabs(m[p][c])) p = r;
+    if (p != c) for (int j = 0; j < 8; j++) std::swap(m[c][j], m[p][j]);
+    const double d = m[c][c];
+    for (int j = 0; j < 8; j++) m[c][j] /= d;
+    for (int r = 0; r < 4; r++) {
+      if (r == c) continue;
+      const double f = m[r][c];
+      for (int j = 0; j < 8; j++) m[r][j] -= f * m[c][j];
+    }
+  }
+  for (int i = 0; i < 4; i++) for (int j = 0; j < 4; j++) inv[4 * i + j] = m[i][j + 4];
+}
+
+int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
+                  const float* Qsr, const float* theta, float radius, std::vector<int>* rowptr, std::vector<int>* col,
+                  std::vector<float>* val, int* n_offsets, std::string* err) {
+  if (radius < 0) { *err = "neighborhood_perturbation: radius cannot be negative"; return DR_ERR_INVALID; }
+  std::vector<int> P;
+  const int m = neighbourhood(Qhr, radius, &P);
+  *n_offsets = m;
+  if (m == 0) { *err = "neighborhood_perturbation: no perturbations within radius"; return DR_ERR_DOMAIN; }
+  if (m > 5000) { *err = "get_sparse_kriging_array_data: neighborhood >5e3 voxels"; return DR_ERR_DOMAIN; }
+  const double th[3] = {theta[0], theta[1], theta[2]};
+  // K over the offsets (kriging_matrix.h:111-138): unit diagonal.
+  std::vector<double> Pm(3 * (size_t)m), K((size_t)m * m);
+  for (int i = 0; i < m; i++)
+    for (int r = 0; r < 3; r++)
+      Pm[3 * i + r] = (double)Qhr[4 * r] * P[3 * i] + (double)Qhr[4 * r + 1] * P[3 * i + 1] +
+                      (double)Qhr[4 * r + 2] * P[3 * i + 2];
+  for (int i = 0; i < m; i++) {
+    K[(size_t)i * m + i] = 1.0;
+    for (int j = 0; j < i; j++) {
+      const double dx = Pm[3 * i] - Pm[3 * j], dy = Pm[3 * i + 1] - Pm[3 * j + 1], dz = Pm[3 * i + 2] - Pm[3 * j + 2];
+      const double v = rbf(std::sqrt(dx * dx + dy * dy + dz * dz), th);
+      K[(size_t)i * m + j] = v;
+      K[(size_t)j * m + i] = v;
+    }
+  }
+  // bounded nonzero ordinal map of the high-res image (nifti_manipulation.inl:244-275)
+  int bbmin[3] = {nx, ny, nz}, bbmax[3] = {-1, -1, -1};
+  const long nvox = (long)nx * ny * nz;
+  for (long idx = 0; idx < nvox; idx++) {
+    if (!has_data(hr[idx])) continue;
+    const int ii[3] = {(int)(idx % nx), (int)((idx / nx) % ny), (int)(idx / ((long)nx * ny))};
+    for (int d = 0; d < 3; d++) { bbmin[d] = std::min(bbmin[d], ii[d]); bbmax[d] = std::max(bbmax[d], ii[d]); }
+  }
+  if (bbmax[0] < 0) { *err = "kriging: high-res image has no data"; return DR_ERR_INVALID; }
+  const int bd[3] = {bbmax[0] - bbmin[0] + 1, bbmax[1] - bbmin[1] + 1, bbmax[2] - bbmin[2] + 1};
+  const long bprod = (long)bd[0] * bd[1] * bd[2];
+  std::vector<int> bmap(bprod);
+  {
+    int count = 0;
+    for (int k = 0; k < bd[2]; k++)
+      for (int j = 0; j < bd[1]; j++)
+        for (int i = 0; i < bd[0]; i++) {
+          const long ni = (long)(k + bbmin[2]) * nx * ny + (long)(j + bbmin[1]) * nx + (i + bbmin[0]);
+          bmap[(long)k * bd[0] * bd[1] + (long)j * bd[0] + i] = has_data(hr[ni]) ? count++ : -1;
+        }
+  }
+  double Qh[16], Qs[16], Qhi[16], mp[16];
+  for (int i = 0; i < 16; i++) { Qh[i] = Qhr[i]; Qs[i] = Qsr[i]; }
+  mat4_inverse(Qh, Qhi);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0.0;
+      for (int k = 0; k < 4; k++) s += Qhi[4 * i + k] * Qs[4 * k + j];
+      mp[4 * i + j] = s;
+    }
+  // std-res rows in column-major nonzero order (nifti_manipulation.inl:335-360)
+  std::vector<long> rows;
+  const long nvs = (long)sx * sy * sz;
+  for (long s = 0; s < nvs; s++)
+    if (has_data(sr[s])) rows.push_back(s);
+  const int nrows = (int)rows.size();
+  std::vector<std::vector<int>> rcol(nrows), rpid(nrows);
+  std::vector<std::vector<double>> rkp(nrows);
+  int bad = 0;
+  // candidates per row (kriging_matrix.h:242-299)
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int ri = 0; ri < nrows; ri++) {
+    const long sidx = rows[ri];
+    const double s[4] = {(double)(sidx % sx), (double)((sidx / sx) % sy), (double)(sidx / ((long)sx * sy)), 1.0};
+    int base[3];
+    double sm[3];
+    for (int r = 0; r < 3; r++) {
+      double a = 0.0, b = 0.0;
+      for (int k = 0; k < 4; k++) { a += mp[4 * r + k] * s[k]; b += Qs[4 * r + k] * s[k]; }
+      base[r] = (int)a;  // truncation toward zero (kriging_matrix.h:255)
+      sm[r] = b;
+    }
+    for (int j = 0; j < m; j++) {
+      const int h0 = base[0] + P[3 * j], h1 = base[1] + P[3 * j + 1], h2 = base[2] + P[3 * j + 2];
+      const long flat = (long)h2 * ny * nx + (long)h1 * nx + h0;  // flat-offset-only check (:263-266)
+      if (flat < 0 || flat >= nvox || !has_data(hr[flat])) continue;
+      const long b = (long)(h2 - bbmin[2]) * bd[0] * bd[1] + (long)(h1 - bbmin[1]) * bd[0] + (h0 - bbmin[0]);
+      if (b < 0 || b >= bprod) {
+#pragma omp atomic
+        bad++;
+        continue;
+      }
+      if (bmap[b] < 0) continue;
+      rcol[ri].push_back(bmap[b]);
+      rpid[ri].push_back(j);
+      double hm[3];
+      for (int r = 0; r < 3; r++) hm[r] = Qh[4 * r] * h0 + Qh[4 * r + 1] * h1 + Qh[4 * r + 2] * h2 + Qh[4 * r + 3];
+      const double dx = sm[0] - hm[0], dy = sm[1] - hm[1], dz = sm[2] - hm[2];
+      rkp[ri].push_back(rbf(std::sqrt(dx * dx + dy * dy + dz * dz) + 1e-5, th));
+    }
+  }
+  if (bad) {
+    *err = "kriging: a neighbourhood index falls outside the bounded high-res index map (undefined in the reference)";
+    return DR_ERR_DOMAIN;
+  }
+  // Rows whose neighbourhood is complete share K; identical k' then share w.
+  std::map<std::vector<double>, std::vector<double>> full_cache;
+  std::mutex cache_mtx;
+  std::vector<std::vector<double>> rw(nrows);
+  std::vector<char> keep(nrows, 1);
+#pragma omp parallel
+  {
+    std::vector<double> A, b, x;
+#pragma omp for schedule(dynamic, 1)
+    for (int ri = 0; ri < nrows; ri++) {
+      const int cnt = (int)rcol[ri].size();
+      if (cnt == 0) continue;
+      if (cnt == m) {
+        std::lock_guard<std::mutex> lk(cache_mtx);
+        auto it = full_cache.find(rkp[ri]);
+        if (it != full_cache.end()) { rw[ri] = it->second; continue; }
+      }
+      A.resize((size_t)cnt * cnt);
+      for (int a = 0; a < cnt; a++)
+        for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)rpid[ri][a] * m + rpid[ri][c]];
+      b = rkp[ri];
+      x.assign(cnt, 0.0);
+      if (cholesky(A.data(), cnt)) {
+        cholesky_solve(A.data(), cnt, b.data());
+        x = b;
+      } else {
+        for (int a = 0; a < cnt; a++)
+          for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)rpid[ri][a] * m + rpid[ri][c]];
+        b = rkp[ri];
+        qr_solve(A.data(), cnt, b.data(), x.data());
+      }
+      double wsum = 0.0;
+      for (int a = 0; a < cnt; a++) wsum += x[a];
+      if (wsum == 0.0) wsum = 1.0;       // kriging_matrix.h:318-319
+      if (std::isnan(wsum)) { keep[ri] = 0; continue; }
+      for (int a = 0; a < cnt; a++) x[a] /= wsum;
+      rw[ri] = x;
+      if (cnt == m) {
+        std::lock_guard<std::mutex> lk(cache_mtx);
+        full_cache.emplace(rkp[ri], x);
+      }
+    }
+  }
+  rowptr->assign(nrows + 1, 0);
+  col->clear();
+  val->clear();
+  for (int ri = 0; ri < nrows; ri++) {
+    if (keep[ri] && !rcol[ri].empty()) {
+      col->insert(col->end(), rcol[ri].begin(), rcol[ri].end());
+      for (double w : rw[ri]) val->push_back((float)w);
+    }
+    (*rowptr)[ri + 1] = (int)col->size();
+  }
+  return DR_OK;
+}
+
+// ---------------------------------------------------------------- preparation
+int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err) {
+  if (!d || !d->highres || !d->qform_hr || d->nx <= 0 || d->ny <= 0 || d->nz <= 0) {
+    *err = "dr_volume_create: highres image and qform are required";
+    return DR_ERR_INVALID;
+  }
+  const int nx = d->nx, ny = d->ny, nz_ = d->nz;
+  const long nvox = (long)nx * ny * nz_;
+  // covariance checks (dualgpm.cpp:447-464)
+  const float* th = d->covariance;
+  if (!(th[0] > 0)) { *err = "First covariance parameter (marginal variance) must be > 0"; return DR_ERR_DOMAIN; }
+  if (!(th[1] > 0)) { *err = "Second covariance parameter (bandwidth) must be > 0"; return DR_ERR_DOMAIN; }
+  if (!(th[2] > 0 && th[2] <= 2)) { *err = "Third covariance parameter (exponent) must be in (0, 2]"; return DR_ERR_DOMAIN; }
+  if (d->covfun != DR_COV_RBF && d->covfun != DR_COV_RQ) { *err = "Unknown covariance function"; return DR_ERR_DOMAIN; }
+  for (int i = 0; i < 3; i++) hv->theta[i] = th[i];
+  hv->covfun = d->covfun;
+  std::memcpy(hv->Q, d->qform_hr, sizeof(float) * 16);
+
+  // masks (dualgpm.cpp:126-155, 288; both default to the high-res image)
+  std::vector<float> hr(d->highres, d->highres + nvox);
+  std::vector<float> hm(d->hmask ? d->hmask : d->highres, (d->hmask ? d->hmask : d->highres) + nvox);
+  const float* om = d->omask ? d->omask : d->highres;
+  for (long i = 0; i < nvox; i++)
+    if (hm[i] == 0.0f || std::isnan(hr[i])) hr[i] = 0.0f;
+  for (long i = 0; i < nvox; i++) hm[i] += om[i];
+  int bbmin[3] = {nx, ny, nz_}, bbmax[3] = {-1, -1, -1};
+  for (long idx = 0; idx < nvox; idx++) {
+    if (!has_data(hm[idx])) continue;
+    const int ii[3] = {(int)(idx % nx), (int)((idx / nx) % ny), (int)(idx / ((long)nx * ny))};
+    for (int k = 0; k < 3; k++) { bbmin[k] = std::min(bbmin[k], ii[k]); bbmax[k] = std::max(bbmax[k], ii[k]); }
+  }
+  if (bbmax[0] < 0) { *err = "dr_volume_create: the masks select no voxel"; return DR_ERR_INVALID; }
+  std::vector<int> D, O;
+  for (long idx = 0; idx < nvox; idx++) {
+    const int ii[3] = {(int)(idx % nx), (int)((idx / nx) % ny), (int)(idx / ((long)nx * ny))};
+    const bool inbox = ii[0] >= bbmin[0] && ii[0] <= bbmax[0] && ii[1] >= bbmin[1] && ii[1] <= bbmax[1] &&
+                       ii[2] >= bbmin[2] && ii[2] <= bbmax[2];
+    if (has_data(hr[idx])) {
+      hv->Yh.push_back(hr[idx]);
+      if (inbox) for (int k = 0; k < 3; k++) D.push_back(ii[k] - bbmin[k]);
+    }
+    if (has_data(om[idx]) && inbox) for (int k = 0; k < 3; k++) O.push_back(ii[k] - bbmin[k]);
+  }
+  const int n_h = (int)D.size() / 3, n_o = (int)O.size() / 3;
+  if (n_h == 0) { *err = "dr_volume_create: no high-res data"; return DR_ERR_INVALID; }
+  if ((int)hv->Yh.size() != n_h) { *err = "dr_volume_create: data voxels outside the mask bounding box"; return DR_ERR_INVALID; }
+  for (int k = 0; k < 3; k++) hv->g[k] = 0;
+  for (int i = 0; i < n_h; i++) for (int k = 0; k < 3; k++) hv->g[k] = std::max(hv->g[k], D[3 * i + k] + 1);
+  for (int k = 0; k < 3; k++) {
+    if (hv->g[k] <= 1) { *err = "circulant_base_3d: Cannot have dimensions <= 1"; return DR_ERR_DOMAIN; }
+    int p = 1;
+    while (p < 2 * (hv->g[k] - 1)) p <<= 1;
+    hv->E[k] = p;
+    if (p > 256) { *err = "dr_volume_create: embedding dimension above 256 is not supported"; return DR_ERR_UNSUPPORTED; }
+  }
+  hv->N = (long long)hv->E[0] * hv->E[1] * hv->E[2];
+  if (hv->N > (1LL << 30)) { *err = "dr_volume_create: embedding too large"; return DR_ERR_UNSUPPORTED; }
+  // output indices must lie on the embedding (MultiResParameters.h:647-667)
+  for (int i = 0; i < n_o; i++)
+    for (int k = 0; k < 3; k++)
+      if (O[3 * i + k] >= hv->E[k]) { *err = "MultiResParameters:set_output_indices MAX"; return DR_ERR_DOMAIN; }
+  for (int k = 0; k < 3; k++) {
+    int b = hv->g[k];
+    for (int i = 0; i < n_o; i++) b = std::max(b, O[3 * i + k] + 1);
+    hv->box[k] = b;
+  }
+  const int bx = hv->box[0], by = hv->box[1], bz = hv->box[2];
+  hv->box_to_d.assign((size_t)bx * by * bz, -1);
+  hv->box_to_o.assign((size_t)bx * by * bz, -1);
+  hv->d_flat.resize(n_h);
+  hv->o_flat.resize(n_o);
+  for (int i = 0; i < n_h; i++) {
+    const int x = D[3 * i], y = D[3 * i + 1], z = D[3 * i + 2];
+    hv->d_flat[i] = (z * hv->E[1] + y) * hv->E[0] + x;
+    hv->box_to_d[((size_t)z * by + y) * bx + x] = i;
+  }
+  for (int i = 0; i < n_o; i++) {
+    const int x = O[3 * i], y = O[3 * i + 1], z = O[3 * i + 2];
+    hv->o_flat[i] = (z * hv->E[1] + y) * hv->E[0] + x;
+    hv->box_to_o[((size_t)z * by + y) * bx + x] = i;
+  }
+
+  // std-res data and kriging matrix (dualgpm.cpp:166-227, MultiResData.h:96-127)
+  if (d->stdres) {
+    if (!d->qform_sr || d->sx <= 0 || d->sy <= 0 || d->sz <= 0) {
+      *err = "dr_volume_create: stdres requires its grid and qform";
+      return DR_ERR_INVALID;
+    }
+    const long nvs = (long)d->sx * d->sy * d->sz;
+    std::vector<float> sr(d->stdres, d->stdres + nvs);
+    if (d->smask)
+      for (long i = 0; i < nvs; i++)
+        if (d->smask[i] == 0.0f || std::isnan(sr[i])) sr[i] = 0.0f;
+    for (long i = 0; i < nvs; i++)
+      if (has_data(sr[i])) hv->Ys.push_back(sr[i]);
+    float radius = d->neighborhood;
+    if (radius <= 0) {
+      float vmax = 0.f;
+      for (int c = 0; c < 3; c++) {
+        float s = 0.f;
+        for (int r = 0; r < 4; r++) s += d->qform_hr[4 * r + c] * d->qform_hr[4 * r + c];
+        vmax = std::max(vmax, std::sqrt(s));
+      }
+      radius = 3.0f * vmax;
+    }
+    hv->radius = radius;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = kriging_build(hr.data(), nx, ny, nz_, d->qform_hr, sr.data(), d->sx, d->sy, d->sz, d->qform_sr,
+                                 d->covariance, radius, &hv->w_rowptr, &hv->w_col, &hv->w_val, &hv->n_offsets, err);
+    hv->kriging_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc != DR_OK) return rc;
+    for (int c : hv->w_col)
+      if (c < 0 || c >= n_h) { *err = "kriging: column outside the data range"; return DR_ERR_DOMAIN; }
+    // transpose (rows ordered by data voxel, columns ascending)
+    const int n_s = (int)hv->Ys.size();
+    hv->wt_rowptr.assign(n_h + 1, 0);
+    for (int c : hv->w_col) hv->wt_rowptr[c + 1]++;
+    for (int i = 0; i < n_h; i++) hv->wt_rowptr[i + 1] += hv->wt_rowptr[i];
+    hv->wt_col.resize(hv->w_col.size());
+    hv->wt_val.resize(hv->w_col.size());
+    std::vector<int> fill(hv->wt_rowptr.begin(), hv->wt_rowptr.end() - 1);
+    for (int r = 0; r < n_s; r++)
+      for (int k = hv->w_rowptr[r]; k < hv->w_rowptr[r + 1]; k++) {
+        const int c = hv->w_col[k];
+        hv->wt_col[fill[c]] = r;
+        hv->wt_val[fill[c]] = hv->w_val[k];
+        fill[c]++;
+      }
+  } else {
+    hv->wt_rowptr.assign(n_h + 1, 0);
+  }
+  return DR_OK;
+}
+
+}  // namespace drb

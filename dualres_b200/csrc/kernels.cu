@@ -1,0 +1,703 @@
+// Device kernels of the dual-resolution GP-HMC sampler.
+//
+// The sampler keeps every chain's state in the spectral domain of the
+// circulant embedding: u = IFFT(mu) and q = IFFT(p) (unnormalised).  In that
+// basis the reference's operators (include/dualres/MultiResParameters.h) become:
+//   position update  mu* += FFT(IFFT(p) eps/(N lambda_m))  ->  u* += eps q / lambda_m
+//   prior gradient   FFT(IFFT(mu)/(-N lambda))             ->  -u / lambda
+//   log prior        -(1/2N) sum |IFFT(mu)|^2 / lambda       ->  -(1/2N) sum |u|^2 / lambda
+//   kinetic energy   -(1/2N) sum |IFFT(p)|^2 / lambda_m      ->  -(1/2N) sum |q|^2 / lambda_m
+// all element-wise, zeroed on S = {Re lambda <= 0} exactly as _low_rank_adjust
+// does.  Only the data term needs real space: Re mu at the data voxels, and the
+// scatter of the data gradient.  One gradient therefore costs one pruned
+// forward transform (spectral -> real box) and one pruned inverse transform
+// (real box -> spectral) instead of the reference's four full 3D FFTs.
+#include "common.cuh"
+#include "drb.h"
+#include "fft.cuh"
+
+namespace drb {
+
+// ----------------------------------------------------------------- twiddles
+__device__ float2 g_tw_f[TW_TOTAL];
+__device__ double2 g_tw_d[TW_TOTAL];
+
+// ----------------------------------------------------------------- HMC parameters
+// Device restatement of HMCParameters<float> (include/dualres/HMCParameters.h).
+__device__ __forceinline__ float hmc_eps(const ChainState& h, double u01) {
+  // :212-221  eps() = eps (warm-up) or max(eps * U(0.9, 1.1), eps0)
+  if (h.warmup) return (float)h.eps;
+  return (float)fmax(h.eps * (0.9 + 0.2 * u01), h.eps0);
+}
+__device__ __forceinline__ int hmc_steps(const ChainState& h) {  // :172-179
+  return h.eps_start_found ? h.integrator_steps : 1;
+}
+__device__ __forceinline__ int hmc_save_iteration(const ChainState& h) {  // :158-161
+  return (h.iteration > h.burnin) && ((h.iteration - h.burnin) % h.thin == 0);
+}
+__device__ void hmc_update(ChainState& h, float mh_rate_f) {  // :259-297
+  const double mh_rate = (double)mh_rate_f;
+  if (h.iteration == h.burnin) {
+    h.warmup = 0;
+    h.eps_start_found = 1;
+    if (h.eps_bar > h.eps0) h.eps = h.eps_bar;
+  }
+  if (h.warmup) {
+    if (!h.eps_start_found) {
+      if (h.iteration == 0) h.A = 2 * (int)(mh_rate > 0.5) - 1;
+      if (pow(mh_rate, h.A) > pow(2.0, -h.A)) {
+        h.eps *= pow(2.0, h.A);
+      } else {
+        h.eps_start_found = 1;
+        h.eps_target = log(10.0 * h.eps);
+      }
+    } else {
+      const double it = (double)h.iteration;
+      h.h_bar = (1 - 1 / (it + h.t0)) * h.h_bar + (h.mh_target - mh_rate) / (it + h.t0);
+      h.eps = exp(h.eps_target - (double)sqrtf((float)h.iteration) * h.h_bar / h.gamma);
+      h.eps = fmax(h.eps, h.eps0);
+      const double pk = pow((double)(float)h.iteration, -h.kappa);
+      h.eps_bar = exp(pk * log(h.eps) + (1 - pk) * log(h.eps_bar));
+    }
+  } else {
+    h.mh_running_sum += mh_rate;
+  }
+  h.iteration++;
+}
+
+// Marsaglia & Tsang (2000), "A simple method for generating gamma variables",
+// ACM TOMS 26(3); shape < 1 by Gamma(a) = Gamma(a + 1) U^(1/a).  Draws come
+// from the counter stream (stream, chain, iteration, base + attempt).  The
+// loop is bounded; a failure sets *err and returns the mean.
+__device__ double gamma_draw(double shape, double scale, uint64_t seed, uint32_t stream, uint32_t chain,
+                             uint32_t iter, uint32_t base, int* err) {
+  double boost = 1.0;
+  if (shape < 1.0) {
+    const u32x4 r = philox(u32x4{base + 1000u, iter, chain, stream}, seed);
+    boost = pow(u01d(r.x, r.y), 1.0 / shape);
+    shape += 1.0;
+  }
+  const double d = shape - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
+  for (uint32_t a = 0; a < 64; a++) {
+    const u32x4 r1 = philox(u32x4{base + 2 * a, iter, chain, stream}, seed);
+    const u32x4 r2 = philox(u32x4{base + 2 * a + 1, iter, chain, stream}, seed);
+    const double x = box_muller_d(u01d(r1.x, r1.y), u01d(r1.z, r1.w)).x;
+    double v = 1.0 + c * x;
+    if (v <= 0.0) continue;
+    v = v * v * v;
+    const double u = u01d(r2.x, r2.y);
+    if (log(u) < 0.5 * x * x + d - d * v + d * log(v)) return d * v * boost * scale;
+  }
+  *err += 1;
+  return shape * scale;
+}
+
+// ----------------------------------------------------------------- pass kernel
+// Batched 1D FFT along the middle axis of [A][n][B] arrays, one tile of 32
+// lines (line = a * B + b) per block, chains on blockIdx.y.
+template <int N> struct PassCfg {
+  static constexpr int NT = N >= 512 ? 512 : 256;
+};
+
+template <int N, int DIR, int PRO, int EPI, class C>
+__global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v, DevChains ch, const C* __restrict__ tw) {
+  constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = PassCfg<N>::NT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int c = (a.chain_only >= 0) ? a.chain_only : (int)blockIdx.y;
+  if (a.step >= 0 && ch.st != nullptr) {
+    if (a.step > ch.st[c].L_cur) return;
+  }
+  const long long lines = (long long)a.A * a.B;
+  const long long l0 = (long long)blockIdx.x * TL;
+  const int nl = (int)min((long long)TL, lines - l0);
+  const C* in = reinterpret_cast<const C*>(a.in) + (long long)c * a.in_cs;
+  C* out = reinterpret_cast<C*>(a.out) + (long long)c * a.out_cs;
+  const int B = a.B, n_in = a.n_in, n_out = a.n_out;
+  int hsel = 0;
+  if (EPI == EPI_GATHER) hsel = (ch.st != nullptr ? ch.st[c].acc : 0) ^ a.sel;
+
+  auto in_index = [&](int l, int i) -> long long {
+    const long long lam = l0 + l;
+    const long long aa = lam / B, bb = lam - aa * B;
+    return (aa * n_in + i) * B + bb;
+  };
+  auto load = [&](int l, int i) -> C {
+    C val = mk((decltype(C().x))0, (decltype(C().x))0);
+    if (l < nl && i < n_in) {
+      const long long idx = in_index(l, i);
+      if (PRO == PRO_LOAD) {
+        val = in[idx];
+      } else {
+        const int j = v.box_to_d[idx];
+        if (j >= 0) val.x = ch.gD[(long long)j * ch.Cp + c];
+      }
+    }
+    return val;
+  };
+  if (B == 1) {
+    for (int e = threadIdx.x; e < TL * N; e += NT) {
+      const int l = e / N, i = e % N;
+      sm[i * P + l] = load(l, i);
+    }
+  } else {
+    for (int e = threadIdx.x; e < TL * N; e += NT) {
+      const int i = e / TL, l = e % TL;
+      sm[i * P + l] = load(l, i);
+    }
+  }
+  __syncthreads();
+  fft_smem<N, DIR, TL, NT>(sm, 1, P, TL, tw + tw_offset(N));
+
+  const auto scale = (decltype(C().x))a.scale;
+  int wo = 0;
+  if (EPI == EPI_GATHER) {
+    wo = a.write_o == 1 || (a.write_o == 2 && ch.st != nullptr && a.step == ch.st[c].L_cur);
+  }
+  auto store = [&](int l, int k) {
+    if (l >= nl || k >= n_out) return;
+    const long long lam = l0 + l;
+    const long long aa = lam / B, bb = lam - aa * B;
+    const long long idx = (aa * n_out + k) * B + bb;
+    const C val = sm[k * P + l];
+    if (EPI == EPI_STORE) {
+      out[idx] = mk(val.x * scale, val.y * scale);
+    } else {
+      const int j = v.box_to_d[idx];
+      if (j >= 0) ch.muD[((long long)hsel * v.n_h + j) * ch.Cp + c] = (float)(val.x * scale);
+      if (wo) {
+        const int o = v.box_to_o[idx];
+        if (o >= 0) ch.muO[((long long)hsel * v.n_o + o) * ch.Cp + c] = (float)(val.x * scale);
+      }
+    }
+  };
+  if (B == 1) {
+    for (int e = threadIdx.x; e < TL * N; e += NT) store(e / N, e % N);
+  } else {
+    for (int e = threadIdx.x; e < TL * N; e += NT) store(e % TL, e / TL);
+  }
+}
+
+// ----------------------------------------------------------------- x-line kernel
+// The hot kernel of one leapfrog step, for 32 x-lines of one chain:
+//   inverse x-FFT of the data gradient (spectral except along x),
+//   kick  q += k eps (IFFT(data grad) - u / lambda)          (MultiResParameters.h:690, 699)
+//   drift u* += eps q / lambda_m                              (:693-698)
+//   forward x-FFT of u* for the next gradient.
+// Step 0 also draws the momentum (:784-815) and the initial energies; the
+// last step only kicks and accumulates the final energies (:702-705).
+template <int E0> struct XCfg {
+  static constexpr int NT = E0 >= 512 ? 512 : 256;
+};
+
+template <int E0>
+__global__ void __launch_bounds__(XCfg<E0>::NT) k_xline(DevVolume v, DevChains ch, int step, int flags,
+                                                        const float2* __restrict__ tw) {
+  constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = XCfg<E0>::NT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2* sm = reinterpret_cast<float2*>(smraw);
+  __shared__ double red[NT / 32];
+  const int c = blockIdx.y;
+  const ChainState& st = ch.st[c];
+  const int Lc = st.L_cur;
+  if (step > Lc) return;
+  const bool first = step == 0, last = step == Lc;
+  const float eps = st.eps_cur, sh = st.sh;
+  const int acc = st.acc;
+  const long long N = v.N;
+  const long long lines = (long long)v.E1 * v.E2;
+  const long long lam0 = (long long)blockIdx.x * TL;
+  const int nl = (int)min((long long)TL, lines - lam0);
+  float2* Ub = ch.U + (long long)c * 2 * N;
+  const float2* Usrc = Ub + (long long)(first ? acc : (acc ^ 1)) * N;
+  float2* Udst = Ub + (long long)(acc ^ 1) * N;
+  float2* Qc = ch.Q + (long long)c * N;
+  float2* T1 = ch.T1 + (long long)c * ch.t1_stride;
+  const int bx = v.bx;
+
+  for (int e = threadIdx.x; e < TL * E0; e += NT) {
+    const int l = e / E0, x = e % E0;
+    float2 val = make_float2(0.f, 0.f);
+    if (l < nl && x < bx) val = T1[(lam0 + l) * bx + x];
+    sm[x * P + l] = val;
+  }
+  __syncthreads();
+  fft_smem<E0, +1, TL, NT>(sm, 1, P, TL, tw + tw_offset(E0));
+
+  const bool fixed = (flags & XF_FIXED_MOMENTUM) != 0;
+  const bool write_q = !last || (flags & XF_WRITE_Q_LAST);
+  const float keps = ((first || last) ? 0.5f : 1.0f) * eps;
+  const float Nf = (float)N;
+  double pa = 0.0, pb = 0.0;
+  for (int e = threadIdx.x; e < TL * (E0 / 2); e += NT) {
+    const int l = e / (E0 / 2), x = 2 * (e % (E0 / 2));
+    if (l >= nl) continue;
+    const long long gi = (lam0 + l) * E0 + x;
+    const float4 u4 = *reinterpret_cast<const float4*>(Usrc + gi);
+    const float2 s2 = *reinterpret_cast<const float2*>(v.sinv + gi);
+    float4 q4;
+    float2 w0 = make_float2(0.f, 0.f), w1 = w0;
+    if (first && !fixed) {
+      const u32x4 r = philox(u32x4{(uint32_t)(gi >> 1), (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c),
+                                   RNG_MOMENTUM}, ch.seed);
+      w0 = box_muller(u01f(r.x), u01f(r.y));
+      w1 = box_muller(u01f(r.z), u01f(r.w));
+      pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
+    } else {
+      q4 = *reinterpret_cast<const float4*>(Qc + gi);
+    }
+    float2 uo[2], qo[2];
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const float2 u = m == 0 ? make_float2(u4.x, u4.y) : make_float2(u4.z, u4.w);
+      const float s = m == 0 ? s2.x : s2.y;
+      const bool live = s > 0.0f;
+      const float lm = s + sh;  // lambda_m = 1/lambda + sigma_h^-2 (MultiResParameters.h:735-738)
+      float2 q;
+      if (first && !fixed) {
+        const float2 w = m == 0 ? w0 : w1;
+        const float a = live ? sqrtf(Nf * lm) : 0.0f;
+        q = make_float2(a * w.x, a * w.y);
+      } else {
+        q = m == 0 ? make_float2(q4.x, q4.y) : make_float2(q4.z, q4.w);
+        if (first && live) pa += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+      }
+      if (first && live) pb += (double)(u.x * u.x + u.y * u.y) * (double)s;
+      const float2 g = sm[(x + m) * P + l];
+      float2 gt = g;
+      if (live) {
+        gt.x = fmaf(-u.x, s, g.x);
+        gt.y = fmaf(-u.y, s, g.y);
+      }
+      q.x = fmaf(keps, gt.x, q.x);
+      q.y = fmaf(keps, gt.y, q.y);
+      float2 un = u;
+      if (last) {
+        if (live) {
+          pa += (double)(u.x * u.x + u.y * u.y) * (double)s;
+          pb += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+        }
+      } else if (live) {
+        const float f = eps / lm;
+        un.x = fmaf(f, q.x, u.x);
+        un.y = fmaf(f, q.y, u.y);
+      }
+      uo[m] = un;
+      qo[m] = q;
+      sm[(x + m) * P + l] = un;
+    }
+    if (write_q) *reinterpret_cast<float4*>(Qc + gi) = make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y);
+    if (!last) *reinterpret_cast<float4*>(Udst + gi) = make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y);
+  }
+  // per-block partial sums -> accept step
+  if (first || last) {
+    const double ta = block_sum(pa, red);
+    if (threadIdx.x == 0) ch.part[((long long)c * NSLOT + (first ? SL_E0 : SL_LPL)) * ch.maxblk + blockIdx.x] = ta;
+    const double tb = block_sum(pb, red);
+    if (threadIdx.x == 0) ch.part[((long long)c * NSLOT + (first ? SL_LP0 : SL_KL)) * ch.maxblk + blockIdx.x] = tb;
+  }
+  if (last) return;
+  __syncthreads();
+  fft_smem<E0, -1, TL, NT>(sm, 1, P, TL, tw + tw_offset(E0));
+  for (int e = threadIdx.x; e < TL * bx; e += NT) {
+    const int l = e / bx, x = e % bx;
+    if (l < nl) T1[(lam0 + l) * bx + x] = sm[x * P + l];
+  }
+}
+
+// ----------------------------------------------------------------- kriging products
+// Chain-activity helpers shared by the kriging kernels.
+struct ChainLanes {
+  int cc, grp, G;
+};
+
+// rs = Ys - W mu_D for every chain (MultiResParameters.h:361-363, 505-507):
+// warp per row of W (grid-stride), chains across lanes.  The chain-minor
+// layout makes each nonzero read one contiguous vector of chain values.
+// NR = chain rounds per lane (C <= CG * NR).
+template <int NR>
+__global__ void __launch_bounds__(256) k_spmv_w(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int C = ch.C, Cp = ch.Cp, CG = ch.CG, G = 32 / CG;
+  const int cc = lane % CG, grp = lane / CG;
+  __shared__ double red[8][32 * NR];
+  const float* mrow[NR];
+  bool act[NR];
+  double sq[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int c = cc + CG * r;
+    act[r] = false;
+    mrow[r] = ch.muD;
+    sq[r] = 0.0;
+    if (c < C && (chain_only < 0 || c == chain_only)) {
+      const ChainState& st = ch.st[c];
+      act[r] = step < 0 || step <= st.L_cur;
+      mrow[r] = ch.muD + (long long)(st.acc ^ sel) * v.n_h * Cp + c;
+    }
+  }
+  for (int row = blockIdx.x * 8 + warp; row < v.n_s; row += gridDim.x * 8) {
+    float acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = 0.f;
+    const int k0 = v.w_rowptr[row], k1 = v.w_rowptr[row + 1];
+    for (int k = k0 + grp; k < k1; k += G) {
+      const float w = __ldg(v.w_val + k);
+      const long long col = (long long)__ldg(v.w_col + k) * Cp;
+#pragma unroll
+      for (int r = 0; r < NR; r++)
+        if (act[r]) acc[r] = fmaf(w, mrow[r][col], acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+      for (int off = CG; off < 32; off <<= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
+    if (grp == 0) {
+      const float ys = v.Ys[row];
+#pragma unroll
+      for (int r = 0; r < NR; r++) {
+        if (!act[r]) continue;
+        const float rsv = ys - acc[r];
+        ch.rs[(long long)row * Cp + cc + CG * r] = rsv;
+        sq[r] += (double)rsv * rsv;
+      }
+    }
+  }
+  if (grp == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) red[warp][cc + CG * r] = sq[r];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    if (chain_only >= 0 && c != chain_only) continue;
+    const ChainState& st = ch.st[c];
+    if (step >= 0 && step > st.L_cur) continue;
+    double s = 0.0;
+    for (int w = 0; w < 8; w++) s += red[w][c];
+    const int slot = step <= 0 ? SL_RS0 : (step == st.L_cur ? SL_RSL : SL_SCRATCH);
+    ch.part[((long long)c * NSLOT + slot) * ch.maxblk + blockIdx.x] = s;
+  }
+}
+
+// gD = sigma_h^-2 (Yh - mu_D) + sigma_s^-2 W^T rs (MultiResParameters.h:357-364):
+// warp per data voxel over the transposed CSR (grid-stride), plus
+// ||Yh - mu_D||^2 partials.
+template <int NR>
+__global__ void __launch_bounds__(256) k_spmv_wt(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int C = ch.C, Cp = ch.Cp, CG = ch.CG, G = 32 / CG;
+  const int cc = lane % CG, grp = lane / CG;
+  __shared__ double red[8][32 * NR];
+  bool act[NR];
+  double sq[NR];
+  int half[NR];
+  float shv[NR], ssv[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int c = cc + CG * r;
+    act[r] = false;
+    sq[r] = 0.0;
+    half[r] = 0;
+    shv[r] = ssv[r] = 0.f;
+    if (c < C && (chain_only < 0 || c == chain_only)) {
+      const ChainState& st = ch.st[c];
+      act[r] = step < 0 || step <= st.L_cur;
+      half[r] = st.acc ^ sel;
+      shv[r] = st.sh;
+      ssv[r] = st.ss;
+    }
+  }
+  for (int row = blockIdx.x * 8 + warp; row < v.n_h; row += gridDim.x * 8) {
+    float acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = 0.f;
+    if (v.n_s > 0) {
+      const int k0 = v.wt_rowptr[row], k1 = v.wt_rowptr[row + 1];
+      for (int k = k0 + grp; k < k1; k += G) {
+        const float w = __ldg(v.wt_val + k);
+        const long long col = (long long)__ldg(v.wt_col + k) * Cp;
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+          if (act[r]) acc[r] = fmaf(w, ch.rs[col + cc + CG * r], acc[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < NR; r++)
+        for (int off = CG; off < 32; off <<= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
+    }
+    if (grp == 0) {
+      const float yh = v.Yh[row];
+#pragma unroll
+      for (int r = 0; r < NR; r++) {
+        if (!act[r]) continue;
+        const int c = cc + CG * r;
+        const float m = ch.muD[((long long)half[r] * v.n_h + row) * Cp + c];
+        const float rh = yh - m;
+        ch.gD[(long long)row * Cp + c] = shv[r] * rh + ssv[r] * acc[r];
+        sq[r] += (double)rh * rh;
+      }
+    }
+  }
+  if (grp == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) red[warp][cc + CG * r] = sq[r];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    if (chain_only >= 0 && c != chain_only) continue;
+    const ChainState& st = ch.st[c];
+    if (step >= 0 && step > st.L_cur) continue;
+    double s = 0.0;
+    for (int w = 0; w < 8; w++) s += red[w][c];
+    const int slot = step <= 0 ? SL_RH0 : (step == st.L_cur ? SL_RHL : SL_SCRATCH);
+    ch.part[((long long)c * NSLOT + slot) * ch.maxblk + blockIdx.x] = s;
+  }
+}
+
+// ----------------------------------------------------------------- per-iteration scalars
+// The arguments of MultiResParameters::update: eps() and integrator_steps()
+// (gaussian_process_model.h:135).
+__global__ void k_iter_begin(DevChains ch) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ch.C) return;
+  ChainState& st = ch.st[c];
+  if (st.done) {
+    st.L_cur = -1;
+    return;
+  }
+  const u32x4 r = philox(u32x4{0u, (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c), RNG_SCALAR}, ch.seed);
+  st.eps_cur = hmc_eps(st, u01d(r.x, r.y));
+  st.L_cur = hmc_steps(st);
+}
+
+__device__ double slot_sum(const DevChains& ch, int c, int slot, int nb, double* red) {
+  double s = 0.0;
+  const double* p = ch.part + ((long long)c * NSLOT + slot) * ch.maxblk;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) s += p[i];
+  return block_sum(s, red);
+}
+
+// Metropolis accept (MultiResParameters.h:702-726), Gibbs sigma draws
+// (:821-838) and HMCParameters::update (HMCParameters.h:259-297).  The
+// Hamiltonian difference is formed in FP64.
+__global__ void __launch_bounds__(256) k_accept(DevVolume v, DevChains ch) {
+  __shared__ double red[8];
+  __shared__ double sums[8];
+  const int c = blockIdx.x;
+  ChainState& st = ch.st[c];
+  if (st.L_cur < 0) return;
+  const int nbs[8] = {ch.nb_x, ch.nb_x, ch.nb_wt, ch.nb_w, ch.nb_x, ch.nb_x, ch.nb_wt, ch.nb_w};
+  for (int s = 0; s < 8; s++) {
+    double t = 0.0;
+    if (!((s == SL_RS0 || s == SL_RSL) && v.n_s == 0)) t = slot_sum(ch, c, s, nbs[s], red);
+    if (threadIdx.x == 0) sums[s] = t;
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double N = (double)v.N;
+  const double sh = st.sh, ss = st.ss;
+  const double lp0 = -0.5 * sums[SL_LP0] / N;
+  const double ll0 = -0.5 * (sh * sums[SL_RH0] + (v.n_s > 0 ? ss * sums[SL_RS0] : 0.0));
+  const double E0 = -0.5 * sums[SL_E0] + lp0 + ll0;
+  const double lpL = -0.5 * sums[SL_LPL] / N;
+  const double llL = -0.5 * (sh * sums[SL_RHL] + (v.n_s > 0 ? ss * sums[SL_RSL] : 0.0));
+  const double KL = -0.5 * sums[SL_KL] / N;
+  const double logR = (lpL + llL + KL) - E0;
+  double R = exp(logR);
+  if (isnan(R)) R = 0.0;
+  const u32x4 r = philox(u32x4{0u, (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c), RNG_SCALAR}, ch.seed);
+  const double u = u01d(r.z, r.w);
+  double Rh = sums[SL_RH0], Rs = sums[SL_RS0];
+  if (u < R) {
+    st.acc ^= 1;
+    st.accepted += 1;
+    Rh = sums[SL_RHL];
+    Rs = sums[SL_RSL];
+  }
+  st.Rh_acc = Rh;
+  st.Rs_acc = Rs;
+  // Gibbs: shape n/2 + 1, rate ||residual||^2 / 2 (float arithmetic as in the reference)
+  const float shape_h = 0.5f * (float)v.n_h + 1.0f, rate_h = 0.5f * (float)Rh;
+  st.sh = (float)gamma_draw(shape_h, 1.0 / (double)rate_h, ch.seed, RNG_SCALAR, ch.chain0 + c, st.iteration, 16u, &st.err);
+  if (v.n_s > 0) {
+    const float shape_s = 0.5f * (float)v.n_s + 1.0f, rate_s = 0.5f * (float)Rs;
+    st.ss = (float)gamma_draw(shape_s, 1.0 / (double)rate_s, ch.seed, RNG_SCALAR, ch.chain0 + c, st.iteration, 4096u,
+                              &st.err);
+  }
+  st.grad_evals += st.L_cur + 1;
+  st.last_log_ratio = logR;
+  hmc_update(st, (float)fmin(1.0, R));
+  st.save_now = 0;
+  if (hmc_save_iteration(st)) {
+    st.save_now = 1;
+    st.saved += 1;
+    st.ll_sum += -0.5 * ((double)st.sh * Rh + (v.n_s > 0 ? (double)st.ss * Rs : 0.0));
+    st.sigh_sum += sqrt(1.0 / (double)st.sh);
+    st.sigs_sum += v.n_s > 0 ? sqrt(1.0 / (double)st.ss) : 0.0;
+    if (st.saved >= st.n_save) st.done = 1;
+  }
+}
+
+// mcmc_summary::update (gaussian_process_model.h:209-229): max |mu| per chain, then moments.
+__global__ void __launch_bounds__(256) k_summary_max(DevVolume v, DevChains ch) {
+  __shared__ float red[8];
+  const int c = blockIdx.x;
+  ChainState& st = ch.st[c];
+  if (!st.save_now || st.L_cur < 0) return;
+  const float* mo = ch.muO + (long long)st.acc * v.n_o * ch.Cp + c;
+  float m = 0.f;
+  for (int o = threadIdx.x; o < v.n_o; o += blockDim.x) m = fmaxf(m, fabsf(mo[(long long)o * ch.Cp]));
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) m = fmaxf(m, red[i]);
+    m = fmaxf(m, red[0]);
+    st.maxabs = m;
+  }
+}
+
+__global__ void k_summary_acc(DevVolume v, DevChains ch) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)v.n_o * ch.Cp;
+  if (e >= total) return;
+  const int c = (int)(e % ch.Cp);
+  if (c >= ch.C) return;
+  const ChainState& st = ch.st[c];
+  if (!st.save_now || st.L_cur < 0) return;
+  const float val = ch.muO[(long long)st.acc * v.n_o * ch.Cp + e];
+  ch.s1[e] += val;
+  ch.s2[e] += (double)val * val;
+  ch.sa[e] += fabs((double)val) / fmax((double)st.maxabs, 1e-6);
+  if (ch.samples != nullptr) ch.samples[(long long)(st.saved - 1) * total + e] = val;
+}
+
+// ----------------------------------------------------------------- initialisation
+// _initialize_sigma (MultiResParameters.h:764-778): sigma_h^-2 ~ Gamma(v, 1),
+// sigma_s^-2 = sigma_h^-2 / U(0, 1).
+__global__ void k_init_sigma(DevChains ch, float shape, int n_datasets) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ch.C) return;
+  ChainState& st = ch.st[c];
+  st.sh = (float)gamma_draw((double)shape, 1.0, ch.seed, RNG_INIT_SIGMA, ch.chain0 + c, 0u, 16u, &st.err);
+  const u32x4 r = philox(u32x4{0u, 0u, (uint32_t)(ch.chain0 + c), RNG_INIT_SIGMA}, ch.seed);
+  st.ss = n_datasets == 2 ? st.sh / u01f(r.x) : 1.0f;
+}
+
+// gD <- Yh for all chains (the data part of the initial state, add_data_to_mu).
+__global__ void k_fill_gD(DevVolume v, DevChains ch) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)v.n_h * ch.Cp) return;
+  ch.gD[e] = v.Yh[e / ch.Cp];
+}
+
+// _initialize_mu (MultiResParameters.h:744-759) in the spectral basis:
+// u0 += sqrt(N lambda) w / 10 on live modes, w ~ CN(0, 2).
+__global__ void k_init_prior(DevVolume v, DevChains ch) {
+  const long long pair = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (2 * pair >= v.N) return;
+  const long long gi = 2 * pair;
+  float2* U = ch.U + (long long)c * 2 * v.N + (long long)ch.st[c].acc * v.N;
+  const u32x4 r = philox(u32x4{(uint32_t)pair, 0u, (uint32_t)(ch.chain0 + c), RNG_INIT_MU}, ch.seed);
+  const float2 w0 = box_muller(u01f(r.x), u01f(r.y)), w1 = box_muller(u01f(r.z), u01f(r.w));
+  const float Nf = (float)v.N;
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const float s = v.sinv[gi + m];
+    if (s > 0.0f) {
+      const float a = sqrtf(Nf / s) * 0.1f;
+      const float2 w = m == 0 ? w0 : w1;
+      U[gi + m].x += a * w.x;
+      U[gi + m].y += a * w.y;
+    }
+  }
+}
+
+// ----------------------------------------------------------------- spectrum (FP64, one-time)
+// circulant_base_3d (circulant_base.inl:30-89): wrapped offsets, float norm of
+// Q (o, 0), covariance evaluated in FP64.
+__global__ void k_base(double2* base, int E0, int E1, int E2, float q00, float q01, float q02, float q10, float q11,
+                       float q12, float q20, float q21, float q22, double th0, double th1, double th2, int covfun) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long N = (long long)E0 * E1 * E2;
+  if (i >= N) return;
+  const int l = (int)(i % E0), m = (int)((i / E0) % E1), n = (int)(i / ((long long)E0 * E1));
+  const float o0 = (float)(l <= E0 / 2 ? l : E0 - l), o1 = (float)(m <= E1 / 2 ? m : E1 - m),
+              o2 = (float)(n <= E2 / 2 ? n : E2 - n);
+  const float a = q00 * o0 + q01 * o1 + q02 * o2;
+  const float b = q10 * o0 + q11 * o1 + q12 * o2;
+  const float cc = q20 * o0 + q21 * o1 + q22 * o2;
+  const double d = (double)sqrtf(a * a + b * b + cc * cc);
+  double val;
+  if (covfun == 0)
+    val = th0 * exp(-th1 * pow(fabs(d), th2));
+  else
+    val = th0 * pow(1.0 + th1 / th2 * d * d, -th2);
+  base[i] = make_double2(val, 0.0);
+}
+
+// S = {Re lambda <= 0} (MultiResParameters.h:258-262); sinv = 1/Re lambda on live modes.
+__global__ void k_spectrum(const double2* lam, float* sinv, double* lam_re, long long N, int* n_S) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double re = lam[i].x;
+  lam_re[i] = re;
+  if (re > 0.0) {
+    sinv[i] = (float)(1.0 / re);
+  } else {
+    sinv[i] = -1.0f;
+    atomicAdd(n_S, 1);
+  }
+}
+
+// ----------------------------------------------------------------- evaluation helpers
+__global__ void k_gather_re(const float2* field, const int* idx, int n, float* out, int pitch, int col) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) out[(long long)j * pitch + col] = field[idx[j]].x;
+}
+
+// u <- -u sinv / N on live modes, 0 on S (prior part of the gradient before the forward FFT).
+__global__ void k_prior_grad_spectral(float2* u, const float* sinv, long long N) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float s = sinv[i];
+  const float f = s > 0.f ? -s / (float)N : 0.f;
+  u[i] = make_float2(u[i].x * f, u[i].y * f);
+}
+
+__global__ void k_scatter_add_re(float2* field, const int* idx, int n, const float* vals, int pitch, int col) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) field[idx[j]].x += vals[(long long)j * pitch + col];
+}
+
+// Block partials of sum_live |u|^2 * sinv  (mode 0) or sum_live |u|^2 / (sinv + sh)  (mode 1).
+__global__ void __launch_bounds__(256) k_spectral_energy(const float2* u, const float* sinv, long long N, float sh,
+                                                         int mode, double* part) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const float s = sinv[i];
+    if (s > 0.f) {
+      const double m2 = (double)u[i].x * u[i].x + (double)u[i].y * u[i].y;
+      acc += mode == 0 ? m2 * s : m2 / (double)(s + sh);
+    }
+  }
+  const double t = block_sum(acc, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_scale(float2* u, long long N, float f) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) u[i] = make_float2(u[i].x * f, u[i].y * f);
+}
+
+// Device restatement of HMCParameters::update over a given MH-rate sequence (diagnostics).
+__global__ void k_debug_dual_averaging(ChainState st, int n, const float* rates, double* eps_out, int* steps_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = 0; i < n; i++) {
+    hmc_update(st, rates[i]);
+    eps_out[i] = st.eps;
+    steps_out[i] = hmc_steps(st);
+  }
+}
+
+}  // namespace drb

@@ -1,0 +1,189 @@
+/*
+ * dualres_b200.h -- C ABI of the B200-native dual-resolution GP-HMC sampler.
+ *
+ * This is the drop-in boundary for the `dualgpmf` path of asw221/dualres.  The
+ * reference has no C ABI of its own; its boundary is the C++ template API
+ * (MultiResData<T>, MultiResParameters<T>, HMCParameters<T>, fit_model) plus
+ * the `dualgpmf` command line.  Each entry point below names the reference
+ * interface it replaces (paths relative to the reference project root).
+ *
+ * Conventions
+ *  - Every function returns DR_OK (0) or a negative DR_ERR_* code;
+ *    dr_last_error() returns a message for the calling thread.  No C++
+ *    exception crosses this boundary (the reference throws std::domain_error /
+ *    std::logic_error, which dualgpm.cpp:382-405 turns into exit code 1).
+ *  - Images are float32, x fastest (NIfTI column-major), 0 or NaN = no data.
+ *  - Qforms are 4x4 float32 row-major (nifti_manipulation.h:34).
+ *  - Complex fields are interleaved float32 (re, im), x fastest, on the
+ *    embedding grid E0 x E1 x E2.
+ *  - Unless a parameter says "device", pointers are host pointers.
+ *  - Handles are not thread-safe; use one handle per thread.
+ *  - The library runs only on a CUDA GPU (sm_100a).  There is no CPU path.
+ */
+#ifndef DUALRES_B200_H
+#define DUALRES_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DR_OK 0
+#define DR_ERR_INVALID (-1)     /* bad argument: NULL, size, range */
+#define DR_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define DR_ERR_NOMEM (-3)       /* device memory exhausted or budget exceeded */
+#define DR_ERR_DOMAIN (-4)      /* model domain error (std::domain_error in the reference) */
+#define DR_ERR_UNSUPPORTED (-5) /* a size outside the supported range */
+#define DR_ERR_STATE (-6)       /* call not valid in the current state */
+#define DR_ERR_TIMEOUT (-7)     /* a bounded device wait gave up */
+
+#define DR_COV_RBF 0 /* v exp(-b |d|^e)            (include/dualres/impl/kernels.inl:8-15)  */
+#define DR_COV_RQ 1  /* v (1 + psi/nu d^2)^(-nu)   (include/dualres/impl/kernels.inl:59-74) */
+
+typedef struct dr_volume dr_volume;
+typedef struct dr_chainset dr_chainset;
+
+/* One dual-resolution problem: the inputs `dualgpmf` reads
+ * (src/dualgpm.cpp:84-245, GPMCommandParser.inl:196-545). */
+typedef struct {
+  int nx, ny, nz;          /* high-res image grid (voxels) */
+  const float* highres;    /* nx*ny*nz, required (--highres) */
+  const float* qform_hr;   /* 16 floats */
+  const float* hmask;      /* optional (--hmask); NULL = the high-res image itself */
+  const float* omask;      /* optional (--omask); NULL = the high-res image itself */
+  int sx, sy, sz;          /* std-res grid; ignored when stdres == NULL */
+  const float* stdres;     /* optional (--stdres); NULL = single resolution */
+  const float* qform_sr;   /* 16 floats, required with stdres */
+  const float* smask;      /* optional (--smask) */
+  float covariance[3];     /* --covariance: variance, bandwidth, exponent */
+  int covfun;              /* DR_COV_RBF (default) or DR_COV_RQ (--rational-quadratic) */
+  float neighborhood;      /* --neighborhood mm; <= 0 = 3 x largest voxel dimension */
+  int device;              /* CUDA device ordinal */
+} dr_volume_desc;
+
+typedef struct {
+  int E[3];                   /* embedding grid */
+  int64_t N;                  /* E0*E1*E2 */
+  int box[3];                 /* real-space region covering data and output voxels */
+  int n_highres;              /* data voxels (rows of Yh) */
+  int n_stdres;               /* std-res voxels (rows of W) */
+  int n_output;               /* output voxels */
+  int64_t kriging_nnz;        /* nnz(W) */
+  int n_nonpositive;          /* |S|, eigenvalues with Re <= 0 */
+  double max_eigenvalue;      /* lambda[0] / N */
+  double setup_seconds;       /* host + device set-up time */
+  double kriging_seconds;     /* of which the kriging build */
+  float neighborhood;         /* radius used (mm) */
+  int64_t device_bytes;       /* device memory held by the volume */
+} dr_volume_info;
+
+/* Replaces MultiResData<T>(h_res, s_res, theta, r) (MultiResData.h:96-127), the
+ * kriging build (kriging_matrix.h:148-343) and the one-time part of the
+ * MultiResParameters<T> constructor (MultiResParameters.h:173-300): masks,
+ * bounding box, data/output indices, circulant eigenvalues (FP64) and S.
+ * Errors: DR_ERR_DOMAIN for |S| >= N/2 (MultiResParameters.h:283-284), invalid
+ * covariance (dualgpm.cpp:447-464) or > 5000 neighbourhood offsets
+ * (kriging_matrix.h:172-174). */
+int dr_volume_create(const dr_volume_desc* desc, dr_volume** out);
+int dr_volume_info_get(const dr_volume* v, dr_volume_info* info);
+/* W as CSR (host buffers of n_stdres+1, kriging_nnz, kriging_nnz entries). */
+int dr_volume_kriging_get(const dr_volume* v, int* rowptr, int* col, float* val);
+/* Re lambda in FP64 (N entries); MultiResParameters::lambda() (:411-415). */
+int dr_volume_lambda_get(const dr_volume* v, double* lambda_re);
+/* Flat embedding-grid indices of the data (n_highres) and output (n_output)
+ * voxels; MultiResParameters::data_indices() (:419-422). Either may be NULL. */
+int dr_volume_indices_get(const dr_volume* v, int* data_idx, int* out_idx);
+/* Observed data vectors; MultiResData::Yh()/Ys() (MultiResData.h:139-150). */
+int dr_volume_data_get(const dr_volume* v, float* Yh, float* Ys);
+void dr_volume_destroy(dr_volume* v);
+
+/* HMC settings: HMCParameters<T>(burnin, nsave, thin, L, eps0, mhtarget)
+ * (HMCParameters.h:97-149) plus the --seed option. */
+typedef struct {
+  int burnin;              /* --burnin (default 1000) */
+  int nsave;               /* --nsave (default 1000) */
+  int thin;                /* --thin (default 3) */
+  int leapfrog;            /* --leapfrog (default 25) */
+  float mhtarget;          /* --mhtarget (default 0.65) */
+  float starting_eps;      /* <= 0: 1 / leapfrog (dualgpm.cpp:253-258) */
+  uint64_t seed;           /* --seed */
+  int store_samples;       /* keep every saved output-voxel sample on the device (--samples) */
+} dr_hmc_opts;
+
+typedef struct {
+  int iteration;           /* HMCParameters::iteration() */
+  int saved;               /* samples accumulated in the summary */
+  int integrator_steps;    /* HMCParameters::integrator_steps() for the next iteration */
+  float eps;               /* HMCParameters::eps_value() */
+  float mh_rate;           /* HMCParameters::metropolis_hastings_rate() */
+  float sigma_hr;          /* MultiResParameters::sigma(0) */
+  float sigma_sr;          /* MultiResParameters::sigma(1) */
+  double last_log_ratio;   /* log R of the last transition (proposed - initial energy) */
+  int64_t accepted;        /* accepted transitions */
+  int64_t grad_evals;      /* gradient evaluations so far (sum of L + 1) */
+  int done;                /* nsave samples saved */
+} dr_chain_stats;
+
+/* n_chains independent chains on one volume, advanced together.  Each chain
+ * is initialised as MultiResParameters<T> does (_initialize_mu / _initialize_sigma,
+ * MultiResParameters.h:744-778) followed by add_data_to_mu (:632-641). */
+int dr_chainset_create(dr_volume* v, int n_chains, const dr_hmc_opts* opts, dr_chainset** out);
+/* One MultiResParameters::update + HMCParameters::update per chain and per
+ * iteration (the loop body of gaussian_process_model.h:134-171), `iterations`
+ * times.  Chains that have saved nsave samples stop changing. */
+int dr_step(dr_chainset* cs, int iterations);
+/* Runs until every chain has saved nsave samples (fit_model's loop). */
+int dr_run(dr_chainset* cs);
+int dr_chain_stats_get(dr_chainset* cs, dr_chain_stats* stats /* n_chains entries */);
+/* Posterior summary of mcmc_summary<T> (gaussian_process_model.h:191-316):
+ * mean, variance and activation over the output voxels (n_output each, any
+ * may be NULL).  chain = -1 pools every chain. */
+int dr_summary_get(dr_chainset* cs, int chain, float* mean, float* var, float* activation);
+/* Saved samples of one chain at the output voxels: n_saved x n_output floats
+ * (requires store_samples). */
+int dr_samples_get(dr_chainset* cs, int chain, float* samples, int max_saved, int* n_saved);
+void dr_chainset_destroy(dr_chainset* cs);
+
+/* ---- fixed-input evaluation (MultiResParameters public API) ------------- */
+/* Sets chain `chain` to mu (2N floats) and sigma^-2 = (s_hr, s_sr). */
+int dr_set_state(dr_chainset* cs, int chain, const float* mu, float s_hr, float s_sr);
+/* mu (2N floats) and sigma^-2 of a chain (MultiResParameters::mu_ / sigma). */
+int dr_get_state(dr_chainset* cs, int chain, float* mu, float* s2inv);
+/* log prior (MultiResParameters.h:429-476) and log likelihood (:488-514) at mu
+ * with the chain's sigma: out[0] = prior, out[1] = likelihood. */
+int dr_log_posterior(dr_chainset* cs, int chain, const float* mu, double* out);
+/* Gradient of the log posterior at mu (MultiResParameters.h:337-376), 2N floats. */
+int dr_gradient(dr_chainset* cs, int chain, const float* mu, float* grad);
+/* The leapfrog integrator of MultiResParameters::update (:689-700) from
+ * (mu0, p0) with a fixed momentum, through the same device kernels that run
+ * the sampler.  energies[0..5] = {log prior(mu0), log lik(mu0), kinetic(p0),
+ * log prior(muL), log lik(muL), kinetic(pL)} with kinetic as in :551-603. */
+int dr_leapfrog_fixed(dr_chainset* cs, int chain, const float* mu0, const float* p0, float eps,
+                      int L, float* mu_out, float* p_out, double* energies);
+
+/* ---- host-side set-up --------------------------------------------------- */
+/* The kriging matrix of get_sparse_kriging_matrix_data (kriging_matrix.h:
+ * 148-343), built on the host (no GPU needed).  `highres` must already be
+ * masked (the reference masks it first, dualgpm.cpp:126-137).  The CSR arrays
+ * are allocated by the library; release them with dr_free. */
+int dr_kriging_matrix(const float* highres, int nx, int ny, int nz, const float* qform_hr, const float* stdres, int sx,
+                      int sy, int sz, const float* qform_sr, const float* covariance, float neighborhood, int* n_rows,
+                      int64_t* nnz, int** rowptr, int** col, float** val);
+void dr_free(void* p);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* Runs the device implementation of HMCParameters::update (HMCParameters.h:
+ * 259-297) over n given MH rates and returns eps_value() and integrator_steps()
+ * after each update; for parity checks of the step-size adaptation. */
+int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starting_eps, float mhtarget,
+                            int n, const float* mh_rates, double* eps_out, int* steps_out, int device);
+/* Device kernel launches made by this thread since the last call (for launch accounting). */
+int64_t dr_kernel_launches(int reset);
+const char* dr_last_error(void);
+const char* dr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
