@@ -1,0 +1,446 @@
+"""Benchmark of the B200 dual-resolution GP-HMC sampler.
+
+Workload (default, "batched64"): 64 independent HMC chains on the seeded
+synthetic 32^3 @ 1 mm volume (RBF 0.806/0.132/1, 64^3 embedding, ellipsoid mask
+~60 %, noise 0.5 / 0.3, kriging radius 6.9 mm), leapfrog 25, burnin 500,
+nsave 500, thin 3.  A step is one HMC iteration of every chain (one
+MultiResParameters::update + HMCParameters::update per chain).  Metric: HMC
+gradient evaluations per second (sum over chains of L + 1 per iteration).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload batched64|single_c1|single_c2] [--no-ess]
+
+Under torchrun each rank runs its own 64-chain set on its GPU (chains are
+independent: no collective on the data path, weak scaling); the timed region
+is bracketed by barriers and the max over ranks is reported.
+
+--impl reference times the reference algorithm on the host CPU: the oracle's
+FP32 restatement of MultiResParameters<float>::update (the `dualgpmf`
+build: four FFTs per leapfrog step, OpenMP), all host threads, one chain and
+one iteration per step (a bounded sample of the same workload).  The
+reference itself cannot be built in this image (Eigen, FFTW3, Boost and NLopt
+are absent), so the restatement stands in for it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HMC gradient evals/sec"
+UNIT = "grad_evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched64", choices=["batched64", "single_c1", "single_c2"])
+    ap.add_argument("--no-ess", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--profile-kernel", type=int, default=-1,
+                    help="set up, run --warmup iterations, then launch kernel K of the leapfrog step 4 times "
+                         "(for ncu: its launches are the last ones of that kernel name)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+class Dist:
+    def __init__(self, backend):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            if backend == "nccl":
+                import torch
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+        self.backend = backend
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if not self.pg:
+            return x
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ workloads
+WORKLOADS = {
+    "batched64": dict(chains=64, vol="c1", burnin=500, nsave=500, thin=3, leapfrog=25),
+    "single_c1": dict(chains=1, vol="c1", burnin=200, nsave=200, thin=1, leapfrog=25),
+    "single_c2": dict(chains=1, vol="c2", burnin=200, nsave=200, thin=1, leapfrog=25),
+}
+
+
+def make_volume(name):
+    from dualres_b200 import synth
+    return synth.config_c1() if name == "c1" else synth.config_c2()
+
+
+def config_of(w, extra=None):
+    cfg = {"workload": w, **{k: v for k, v in WORKLOADS[w].items()},
+           "latent_grid": "32x32x32 @ 1mm" if WORKLOADS[w]["vol"] == "c1" else "64x64x48 @ 1.5mm",
+           "embedding": "64^3" if WORKLOADS[w]["vol"] == "c1" else "128^3",
+           "covariance": [0.806, 0.132, 1.0] if WORKLOADS[w]["vol"] == "c1" else [1.0, 0.4, 1.5],
+           "neighborhood_mm": 6.9, "parallelism": "independent chains per GPU (no collective)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ ESS
+def ess_geyer(x):
+    """ESS of one chain (Geyer initial monotone sequence over the FFT autocorrelation); x: (n, V)."""
+    n = x.shape[0]
+    x = x - x.mean(axis=0)
+    f = np.fft.rfft(x, n=2 * n, axis=0)
+    ac = np.fft.irfft(f * np.conj(f), axis=0)[:n] / n
+    var = ac[0]
+    ok = var > 0
+    rho = np.where(ok, ac / np.where(ok, var, 1.0), 0.0)
+    m = (n - 1) // 2
+    pairs = rho[0:2 * m:2] + rho[1:2 * m:2]           # Gamma_k = rho_2k + rho_2k+1
+    pos = pairs > 0
+    first_neg = np.where(pos.all(axis=0), m, np.argmin(pos, axis=0))
+    idx = np.arange(m)[:, None]
+    pairs = np.where(idx < first_neg[None, :], pairs, 0.0)
+    pairs = np.minimum.accumulate(np.where(pairs > 0, pairs, np.inf), axis=0)
+    pairs = np.where(np.isfinite(pairs), pairs, 0.0)
+    tau = -1.0 + 2.0 * pairs.sum(axis=0)
+    tau = np.maximum(tau, 1.0 / np.log10(max(n, 10)))
+    return np.where(ok, n / tau, 0.0)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, dist):
+    import dualres_b200 as d
+    wl = WORKLOADS[args.workload]
+    C = wl["chains"]
+    hmc = d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"], leapfrog=wl["leapfrog"],
+                          seed=args.seed + 7919 * dist.rank)
+    vol = make_volume(wl["vol"])
+    d.lib()
+    import ctypes
+    dev = 0
+
+    # ---- end to end through the C ABI with host buffers: volume + chains + K iterations,
+    # each followed by a device->host read of every chain's statistics; then the summary.
+    dist.barrier()
+    t0 = time.perf_counter()
+    data = d.MultiResData.from_volume(vol, device=dev)
+    chains = d.MultiResParameters(data, hmc, C)
+    stats = None
+    for _ in range(args.warmup + args.steps):
+        chains.update(1)
+        stats = chains.stats()
+    summ = chains.summary(-1)
+    t_e2e = time.perf_counter() - t0
+    grads_e2e = sum(s["grad_evals"] for s in stats)
+    img_bytes = sum(a.nbytes for a in (vol.highres, vol.stdres))
+    stat_bytes = C * ctypes.sizeof(d.api.ChainStats)
+    t_e2e = dist.max(t_e2e)
+    grads_e2e = dist.sum(grads_e2e)
+
+    # ---- device-timed steps on the warm chain set
+    chains.update(args.warmup)
+    st0 = chains.stats()
+    launches0 = d.kernel_launches()
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    dist.barrier()
+    clk.start()
+    ms = chains.update_timed(args.steps)
+    clocks = clk.stop()
+    launches = d.kernel_launches() - launches0
+    st1 = chains.stats()
+    grads = sum(b["grad_evals"] - a["grad_evals"] for a, b in zip(st0, st1))
+    t_max = dist.max(ms / 1e3)
+    grads_all = dist.sum(grads)
+    value = grads_all / t_max
+
+    extra = {}
+    # ---- ESS/s of voxelwise posterior means on the full configured job (fresh chain set)
+    if not args.no_ess and dist.rank == 0:
+        hmc2 = d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"], leapfrog=wl["leapfrog"],
+                               seed=args.seed + 1, store_samples=True)
+        job = d.MultiResParameters(data, hmc2, C)
+        total_iters = wl["burnin"] + wl["thin"] * wl["nsave"]
+        job_ms = job.update_timed(total_iters)
+        st = job.stats()
+        rng = np.random.default_rng(0)
+        vox = np.sort(rng.choice(data.n_output, size=min(2000, data.n_output), replace=False))
+        ess = np.zeros(len(vox))
+        for c in range(C):
+            s = job.samples(c)[:, vox].astype(np.float64)
+            ess += ess_geyer(s)
+        extra["ess"] = {"median": float(np.median(ess)), "min": float(np.min(ess)), "voxels": int(len(vox)),
+                        "job_seconds": job_ms / 1e3, "iterations": total_iters,
+                        "mh_rate": float(np.mean([x["mh_rate"] for x in st])),
+                        "eps": float(np.mean([x["eps"] for x in st]))}
+        extra["ess_per_sec"] = {"median": float(np.median(ess)) / (job_ms / 1e3),
+                                "min": float(np.min(ess)) / (job_ms / 1e3)}
+        extra["job_grad_evals_per_sec"] = sum(x["grad_evals"] for x in st) / (job_ms / 1e3)
+        job.close()
+
+    # ---- roofline of the dominant kernel (timed live with CUDA events on the library stream)
+    per_iter = {}
+    L = wl["leapfrog"]
+    launches_per_iter = [L + 1, L, L, L + 1, L + 1, L + 1, L + 1]
+    peak = peaks()
+    for k in range(7):
+        kms, kbytes = d.api.time_kernel(chains, k, step=1, reps=20)
+        per_iter[k] = (kms * launches_per_iter[k], kms, kbytes)
+    dom = max(per_iter, key=lambda k: per_iter[k][0])
+    _, kms, kbytes = per_iter[dom]
+    achieved = kbytes / (kms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": d.api.KERNEL_NAMES[dom], "achieved": achieved, "peak": peak[0],
+                "unit": "GB/s", "frac": achieved / peak[0], "peak_source": peak[1],
+                "algorithmic_bytes_per_launch": kbytes, "launch_ms": kms,
+                "traffic": traffic_from_profile(), "kernels": {
+                    d.api.KERNEL_NAMES[k]: {"ms_per_launch": v[1], "ms_per_iteration": v[0],
+                                            "GBps_algorithmic": v[2] / (v[1] / 1e3) / 1e9}
+                    for k, v in per_iter.items()}}
+    info = data.info
+    cfg = config_of(args.workload, {
+        "global_batch": C * dist.world, "l2": "working set larger than L2 (state 0.5 GB per GPU)",
+        "n_highres": info.n_highres, "n_stdres": info.n_stdres, "kriging_nnz": int(info.kriging_nnz),
+        "setup_seconds": info.setup_seconds, "kriging_seconds": info.kriging_seconds})
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded GP draw)",
+        "config": cfg,
+        "e2e": {"value": grads_e2e / t_e2e, "unit": UNIT, "seconds": t_e2e,
+                "h2d_bytes_per_step": int(img_bytes / (args.warmup + args.steps)),
+                "d2h_bytes_per_step": int(stat_bytes),
+                "includes": "volume upload + host kriging + FP64 spectrum + chain init + every iteration "
+                            "(dr_step + d2h chain statistics) + summary d2h"},
+        "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
+        "grad_evals_per_step": grads_all / args.steps, **extra,
+    }
+    chains.close()
+    data.close()
+    return line
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("bytes_per_launch")
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ CPU (oracle restatement)
+def oracle_model(vol, W=None, precision="f"):
+    from oracle import oracle as o
+    prep = o.prepare(vol.highres)
+    if W is None:
+        W = o.kriging(prep["masked"], vol.qform_hr, vol.stdres, vol.qform_sr, vol.theta, vol.radius)
+    ys = vol.stdres.ravel()[~(np.isnan(vol.stdres.ravel()) | (vol.stdres.ravel() == 0))]
+    m = o.Model(prep["D"], prep["Yh"], vol.qform_hr, vol.theta, ys, W, prep["O"], precision=precision)
+    return m, prep
+
+
+def cpu_rate(m, iters, L, threads, seed=5):
+    from oracle import oracle as o
+    o.set_threads(threads)
+    rng = np.random.default_rng(seed)
+    mu = (rng.standard_normal(m.shape) * 0.1).astype(np.complex64)
+    m.set_mu(mu)
+    m.set_sigma(2.0, 5.0)
+    t0 = time.perf_counter()
+    g = m.run_iterations(iters, L, 0.02, seed)
+    dt = time.perf_counter() - t0
+    return g / dt, dt, g
+
+
+def cpu_baseline_line(vol, W, L, target_s=12.0):
+    threads = os.cpu_count() or 1
+    m, _ = oracle_model(vol, W)
+    r1, dt1, _ = cpu_rate(m, 1, L, threads)
+    iters = max(1, int(target_s / max(dt1, 1e-3)))
+    r, dt, g = cpu_rate(m, iters, L, threads)
+    return {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{iters} HMC iterations (L={L}, {g} gradient evals) of one chain on the same volume, "
+                      f"FP32 restatement of MultiResParameters<float>::update (4 FFTs per leapfrog step), "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args, dist):
+    wl = WORKLOADS[args.workload]
+    if dist.rank != 0:
+        return None
+    vol = make_volume(wl["vol"])
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    m, _ = oracle_model(vol, None)
+    setup = time.perf_counter() - t0
+    from oracle import oracle as o
+    o.set_threads(threads)
+    L = wl["leapfrog"]
+    rng = np.random.default_rng(1)
+    m.set_mu((rng.standard_normal(m.shape) * 0.1).astype(np.complex64))
+    m.set_sigma(2.0, 5.0)
+    for _ in range(args.warmup):
+        m.run_iterations(1, L, 0.02, 3)
+    t0 = time.perf_counter()
+    g = 0
+    for i in range(args.steps):
+        g += m.run_iterations(1, L, 0.02, 100 + i)
+    dt = time.perf_counter() - t0
+    value = g / dt
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded GP draw)",
+            "impl": "reference",
+            "config": config_of(args.workload, {"setup_seconds": setup,
+                                                "sample": "one chain, one HMC iteration per step"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} HMC iterations (L={L}) of one chain on the same volume, "
+                                       f"FP32 restatement of MultiResParameters<float>::update, {threads} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def profile_kernel(args):
+    import dualres_b200 as d
+    wl = WORKLOADS[args.workload]
+    hmc = d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"], leapfrog=wl["leapfrog"],
+                          seed=args.seed)
+    data = d.MultiResData.from_volume(make_volume(wl["vol"]))
+    chains = d.MultiResParameters(data, hmc, wl["chains"])
+    chains.update(args.warmup)
+    ms, b = d.api.time_kernel(chains, args.profile_kernel, step=1, reps=3)
+    print(json.dumps({"kernel": d.api.KERNEL_NAMES[args.profile_kernel], "ms": ms, "algorithmic_bytes": b,
+                      "steps": [s["integrator_steps"] for s in chains.stats()][:4]}))
+
+
+def main():
+    args = parse()
+    if args.profile_kernel >= 0:
+        profile_kernel(args)
+        return
+    if args.impl == "reference":
+        dist = Dist("gloo")
+        line = run_reference(args, dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        dist.close()
+        return
+    dist = Dist("nccl")
+    line = run_ours(args, dist)
+    if dist.rank == 0:
+        if dist.world == 1 and not args.no_cpu:
+            vol = make_volume(WORKLOADS[args.workload]["vol"])
+            import dualres_b200 as d
+            dv = d.MultiResData.from_volume(vol)
+            rp, col, val = dv.W()
+            dv.close()
+            line["cpu_baseline"] = cpu_baseline_line(vol, (rp, col, val.astype(np.float32)),
+                                                     WORKLOADS[args.workload]["leapfrog"])
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -116,6 +116,7 @@ def _declare(L):
     L.dr_chainset_destroy.argtypes = [vp]
     L.dr_chainset_destroy.restype = None
     L.dr_step.argtypes = [vp, C.c_int]
+    L.dr_step_timed.argtypes = [vp, C.c_int, vp]
     L.dr_run.argtypes = [vp]
     L.dr_chain_stats_get.argtypes = [vp, vp]
     L.dr_summary_get.argtypes = [vp, C.c_int, vp, vp, vp]
@@ -128,6 +129,7 @@ def _declare(L):
     L.dr_kriging_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int, vp, vp,
                                     C.c_float, _ip, C.POINTER(C.c_int64), C.POINTER(_ip), C.POINTER(_ip),
                                     C.POINTER(_fp)]
+    L.dr_debug_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
     L.dr_debug_dual_averaging.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, vp,
@@ -320,6 +322,12 @@ class MultiResParameters:
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))
 
+    def update_timed(self, iterations=1):
+        """Advance and return the device time (ms, CUDA events on the library's stream)."""
+        ms = np.zeros(1, np.float64)
+        check(lib().dr_step_timed(self.h, iterations, _ptr(ms)))
+        return float(ms[0])
+
     def run(self):
         check(lib().dr_run(self.h))
 
@@ -399,6 +407,19 @@ def debug_dual_averaging(burnin, nsave, thin, L, starting_eps, mhtarget, rates, 
     check(lib().dr_debug_dual_averaging(burnin, nsave, thin, L, starting_eps, mhtarget, len(r), _ptr(r), _ptr(e),
                                         _ptr(s), device))
     return e, s
+
+
+KERNEL_NAMES = ["x-line update (k_xline)", "forward y pass (k_pass)", "forward z pass + gather (k_pass)",
+                "W product (k_spmv_w)", "W^T product (k_spmv_wt)", "inverse z pass (k_pass)",
+                "inverse y pass (k_pass)"]
+
+
+def time_kernel(chains, which, step=1, reps=20):
+    """Mean CUDA-event duration (ms) and algorithmic bytes of one kernel of the leapfrog step."""
+    ms = np.zeros(1, np.float64)
+    b = np.zeros(1, np.float64)
+    check(lib().dr_debug_time_kernel(chains.h, which, step, reps, _ptr(ms), _ptr(b)))
+    return float(ms[0]), float(b[0])
 
 
 def kernel_launches(reset=False):

@@ -500,7 +500,7 @@ static void write_states(Chainset* S, const std::vector<ChainState>& st) {
   CK(cudaStreamSynchronize(S->stream));
 }
 
-static void step(Chainset* S, int iters) {
+static void step(Chainset* S, int iters, double* device_ms = nullptr) {
   CK(cudaSetDevice(S->vol->device));
   if (!S->graph) {
     cudaGraph_t g = nullptr;
@@ -520,11 +520,25 @@ static void step(Chainset* S, int iters) {
     cudaGraphDestroy(g);
     if (e != cudaSuccess) throw Error(DR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
   }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (device_ms) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, S->stream));
+  }
   for (int i = 0; i < iters; i++) {
     CK(cudaGraphLaunch(S->graph, S->stream));
     g_launches += S->graph_nodes;
   }
+  if (device_ms) CK(cudaEventRecord(e1, S->stream));
   CK(cudaStreamSynchronize(S->stream));
+  if (device_ms) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *device_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
 }
 
 // Spectral state of chain c from a real-space field (host, 2N floats).
@@ -695,6 +709,13 @@ int dr_step(dr_chainset* s, int iterations) {
   API_BEGIN
   if (!s || iterations < 0) throw Error(DR_ERR_INVALID, "bad argument");
   step(s, iterations);
+  API_END
+}
+
+int dr_step_timed(dr_chainset* s, int iterations, double* device_ms) {
+  API_BEGIN
+  if (!s || iterations < 0 || !device_ms) throw Error(DR_ERR_INVALID, "bad argument");
+  step(s, iterations, device_ms);
   API_END
 }
 
@@ -967,6 +988,59 @@ int dr_kriging_matrix(const float* hr, int nx, int ny, int nz, const float* Qhr,
 }
 
 void dr_free(void* p) { std::free(p); }
+
+int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* avg_ms, double* algo_bytes) {
+  API_BEGIN
+  if (!s || !avg_ms || reps <= 0 || stp < 1 || which < 0 || which > 6) throw Error(DR_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(s->vol->device));
+  const DevVolume& v = s->vol->dv;
+  const DevChains& ch = s->dc;
+  const float2* tw = s->vol->tw_f;
+  const int C = s->C;
+  const double N = (double)v.N, t1 = (double)ch.t1_stride, t2 = (double)ch.t2_stride, z = (double)s->vol->hv.w_col.size();
+  auto launch = [&]() {
+    switch (which) {
+      case 0: launch_xline(s, stp, 0); break;
+      case 1: launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE, pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by, 1.0, stp), v, ch, tw, C, s->stream); break;
+      case 2: launch_pass<float2>(v.E2, -1, PRO_LOAD, EPI_GATHER, pass_args(ch.T2, nullptr, ch.t2_stride, 0, 1, v.by * v.bx, v.E2, v.bz, 1.0 / N, stp, 1, 2), v, ch, tw, C, s->stream); break;
+      case 3: if (v.n_s > 0) launch_spmv(s, stp, 1, -1, true); break;
+      case 4: launch_spmv(s, stp, 1, -1, false); break;
+      case 5: launch_pass<float2>(v.E2, +1, PRO_DATAGRAD, EPI_STORE, pass_args(nullptr, ch.T2, 0, ch.t2_stride, 1, v.by * v.bx, v.bz, v.E2, 1.0, stp), v, ch, tw, C, s->stream); break;
+      default: launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE, pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1, 1.0, stp), v, ch, tw, C, s->stream); break;
+    }
+  };
+  launch();  // warm-up
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaEventRecord(e0, s->stream));
+  for (int i = 0; i < reps; i++) launch();
+  CK(cudaEventRecord(e1, s->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *avg_ms = (double)ms / reps;
+  if (algo_bytes) {
+    // bytes a launch must move (each array read or written once; shared arrays once per launch)
+    const double box = (double)v.bx * v.by * v.bz;
+    double b = 0.0;
+    switch (which) {
+      case 0: b = C * (2.0 * t1 * 8 + 4.0 * N * 8) + N * 4; break;                  // T1 in/out, U and q in/out, 1/lambda
+      case 1: b = C * (t1 + t2) * 8; break;
+      case 2: b = C * (t2 * 8 + (v.n_h + v.n_o) * 4.0) + box * 8; break;            // box maps (2 x int32)
+      case 3: b = z * 8 + C * ((double)v.n_h * 4 + (double)v.n_s * 4) + v.n_s * 8.0; // W values + columns, mu_D, rs
+        break;
+      case 4: b = z * 8 + C * ((double)v.n_s * 4 + 2.0 * v.n_h * 4) + v.n_h * 12.0; break;
+      case 5: b = C * ((double)v.n_h * 4 + t2 * 8) + box * 4; break;
+      default: b = C * (t2 + t1) * 8; break;
+    }
+    *algo_bytes = b;
+  }
+  API_END
+}
 
 int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starting_eps, float mhtarget, int n,
                             const float* rates, double* eps_out, int* steps_out, int device) {

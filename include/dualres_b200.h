@@ -133,6 +133,9 @@ int dr_chainset_create(dr_volume* v, int n_chains, const dr_hmc_opts* opts, dr_c
  * iteration (the loop body of gaussian_process_model.h:134-171), `iterations`
  * times.  Chains that have saved nsave samples stop changing. */
 int dr_step(dr_chainset* cs, int iterations);
+/* dr_step, also returning the device time of the iterations in ms, measured
+ * with CUDA events on the chainset's stream around the launches. */
+int dr_step_timed(dr_chainset* cs, int iterations, double* device_ms);
 /* Runs until every chain has saved nsave samples (fit_model's loop). */
 int dr_run(dr_chainset* cs);
 int dr_chain_stats_get(dr_chainset* cs, dr_chain_stats* stats /* n_chains entries */);
@@ -178,6 +181,14 @@ void dr_free(void* p);
  * after each update; for parity checks of the step-size adaptation. */
 int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starting_eps, float mhtarget,
                             int n, const float* mh_rates, double* eps_out, int* steps_out, int device);
+/* Times `reps` back-to-back launches of one kernel of the leapfrog step at
+ * step index `step` (>= 1) on the chainset's stream with CUDA events and
+ * returns the mean duration in ms.  which: 0 x-line update, 1 forward y pass,
+ * 2 forward z pass + gather, 3 W product, 4 W^T product, 5 inverse z pass,
+ * 6 inverse y pass.  The kernels run on the live chain state, which they
+ * change: call it only when the chains are no longer needed.  algo_bytes
+ * receives the kernel's algorithmic bytes per launch (may be NULL). */
+int dr_debug_time_kernel(dr_chainset* cs, int which, int step, int reps, double* avg_ms, double* algo_bytes);
 /* Device kernel launches made by this thread since the last call (for launch accounting). */
 int64_t dr_kernel_launches(int reset);
 const char* dr_last_error(void);

@@ -147,6 +147,39 @@ double orc_cov(int covfun, double d, const double* theta) {
 
 static double rbf_d(double d, const double* th) { return th[0] * exp(-th[1] * pow(fabs(d), th[2])); }
 
+/* Lower Cholesky of the m x m row-major SPD matrix A (unblocked, dot-product
+ * form).  Returns 0 if a pivot is not positive. */
+static int cholesky_inplace(double* A, int m) {
+  for (int j = 0; j < m; j++) {
+    double* Aj = A + (long)j * m;
+    double d = Aj[j];
+    for (int p = 0; p < j; p++) d -= Aj[p] * Aj[p];
+    if (!(d > 0.0)) return 0;
+    const double l = sqrt(d);
+    Aj[j] = l;
+    for (int i = j + 1; i < m; i++) {
+      double* Ai = A + (long)i * m;
+      double s = Ai[j];
+      for (int p = 0; p < j; p++) s -= Ai[p] * Aj[p];
+      Ai[j] = s / l;
+    }
+  }
+  return 1;
+}
+
+static void cholesky_solve_inplace(const double* L, int m, double* b) {
+  for (int i = 0; i < m; i++) {
+    double s = b[i];
+    for (int p = 0; p < i; p++) s -= L[(long)i * m + p] * b[p];
+    b[i] = s / L[(long)i * m + i];
+  }
+  for (int i = m - 1; i >= 0; i--) {
+    double s = b[i];
+    for (int p = i + 1; p < m; p++) s -= L[(long)p * m + i] * b[p];
+    b[i] = s / L[(long)i * m + i];
+  }
+}
+
 /* Column-pivoted Householder QR solve of the m x m system A x = b (A row-major,
  * destroyed).  Components beyond the numerical rank are set to zero, as in a
  * rank-revealing basic solution. */
@@ -297,31 +330,32 @@ int64_t orc_kriging_build(const float* hr, int nx, int ny, int nz, const float* 
     }
 
   const long nvox_s = (long)sx * sy * sz;
-  int* cols = (int*)malloc(sizeof(int) * m);
-  int* pidx = (int*)malloc(sizeof(int) * m);
-  double* kp = (double*)malloc(sizeof(double) * m);
-  double* Ks = solve ? (double*)malloc(sizeof(double) * (size_t)m * m) : NULL;
-  double* w = (double*)malloc(sizeof(double) * m);
-  int64_t nnz = 0;
-  int row = 0;
+  /* phase 1: candidate columns, offsets and k' of every std-res row */
+  long nrows_all = 0;
+  for (long sidx = 0; sidx < nvox_s; sidx++) nrows_all += is_nz(sr[sidx]);
+  if (nrows_all > max_rows) { free(P); free(Pmm); free(K); free(bmap); return -1; }
+  int** rcols = (int**)calloc(nrows_all, sizeof(int*));
+  int** rpid = (int**)calloc(nrows_all, sizeof(int*));
+  double** rkp = (double**)calloc(nrows_all, sizeof(double*));
+  double** rw = (double**)calloc(nrows_all, sizeof(double*));
+  int* rcnt = (int*)calloc(nrows_all, sizeof(int));
+  int* rkeep = (int*)malloc(sizeof(int) * nrows_all);
   int64_t status = 0;
-  rowptr[0] = 0;
+  int row = 0;
   for (long sidx = 0; sidx < nvox_s && status == 0; sidx++) {
     if (!is_nz(sr[sidx])) continue;
-    if (row >= max_rows) { status = -1; break; }
     const double s[4] = {(double)(sidx % sx), (double)((sidx / sx) % sy), (double)(sidx / ((long)sx * sy)), 1.0};
     int base[3];
-    for (int r = 0; r < 3; r++) {
-      double a = 0.0;
-      for (int k = 0; k < 4; k++) a += map[4 * r + k] * s[k];
-      base[r] = (int)a; /* truncation toward zero, kriging_matrix.h:255 */
-    }
     double sm[3];
     for (int r = 0; r < 3; r++) {
-      double a = 0.0;
-      for (int k = 0; k < 4; k++) a += Qs[4 * r + k] * s[k];
-      sm[r] = a;
+      double a = 0.0, b = 0.0;
+      for (int k = 0; k < 4; k++) { a += map[4 * r + k] * s[k]; b += Qs[4 * r + k] * s[k]; }
+      base[r] = (int)a; /* truncation toward zero, kriging_matrix.h:255 */
+      sm[r] = b;
     }
+    rcols[row] = (int*)malloc(sizeof(int) * m);
+    rpid[row] = (int*)malloc(sizeof(int) * m);
+    rkp[row] = (double*)malloc(sizeof(double) * m);
     int cnt = 0;
     for (int j = 0; j < m; j++) {
       const int h0 = base[0] + P[3 * j], h1 = base[1] + P[3 * j + 1], h2 = base[2] + P[3 * j + 2];
@@ -331,38 +365,88 @@ int64_t orc_kriging_build(const float* hr, int nx, int ny, int nz, const float* 
       const long bhr = (long)(h2 - bbmin[2]) * bd[0] * bd[1] + (long)(h1 - bbmin[1]) * bd[0] + (h0 - bbmin[0]);
       if (bhr < 0 || bhr >= bprod) { status = -3; break; }
       if (bmap[bhr] < 0) continue;
-      cols[cnt] = bmap[bhr];
-      pidx[cnt] = j;
+      rcols[row][cnt] = bmap[bhr];
+      rpid[row][cnt] = j;
       double hm[3];
       for (int r = 0; r < 3; r++)
         hm[r] = Qh[4 * r + 0] * h0 + Qh[4 * r + 1] * h1 + Qh[4 * r + 2] * h2 + Qh[4 * r + 3];
       const double dx = sm[0] - hm[0], dy = sm[1] - hm[1], dz = sm[2] - hm[2];
-      kp[cnt] = rbf_d(sqrt(dx * dx + dy * dy + dz * dz) + 1e-5, th);
+      rkp[row][cnt] = rbf_d(sqrt(dx * dx + dy * dy + dz * dz) + 1e-5, th);
       cnt++;
     }
-    if (status) break;
-    int keep = cnt;
-    if (cnt > 0 && solve) {
-      for (int a = 0; a < cnt; a++)
-        for (int b = 0; b < cnt; b++) Ks[(long)a * cnt + b] = K[(long)pidx[a] * m + pidx[b]];
-      colpiv_qr_solve(Ks, cnt, kp, w);
-      double wsum = 0.0;
-      for (int a = 0; a < cnt; a++) wsum += w[a];
-      if (wsum == 0.0) wsum = 1.0;
-      if (isnan(wsum)) keep = 0;
-      else for (int a = 0; a < cnt; a++) w[a] /= wsum;
+    rcnt[row] = cnt;
+    rkeep[row] = 1;
+    row++;
+  }
+  /* phase 2: K_sub w = k' per row (Cholesky; column-pivoted QR if K_sub is not
+   * numerically positive definite).  Rows whose neighbourhood is complete share
+   * K, so a row with the same k' as an earlier complete row reuses its w. */
+  if (solve && status == 0) {
+    int full_ref = -1;
+    for (int r = 0; r < row; r++)
+      if (rcnt[r] == m) { full_ref = r; break; }
+#pragma omp parallel
+    {
+      double* A = (double*)malloc(sizeof(double) * (size_t)m * m);
+      double* b = (double*)malloc(sizeof(double) * m);
+#pragma omp for schedule(dynamic, 1)
+      for (int r = -1; r < row; r++) {
+        const int rr = r < 0 ? full_ref : r;
+        if (rr < 0) continue;
+        if (r >= 0 && rcnt[r] == m && full_ref >= 0 && r != full_ref &&
+            memcmp(rkp[r], rkp[full_ref], sizeof(double) * m) == 0)
+          continue; /* filled from the shared solution below */
+        if (r >= 0 && r == full_ref) continue; /* solved by the r = -1 pass */
+        const int cnt = rcnt[rr];
+        if (cnt == 0) continue;
+        for (int a = 0; a < cnt; a++)
+          for (int c = 0; c < cnt; c++) A[(long)a * cnt + c] = K[(long)rpid[rr][a] * m + rpid[rr][c]];
+        double* w = (double*)malloc(sizeof(double) * cnt);
+        memcpy(b, rkp[rr], sizeof(double) * cnt);
+        if (cholesky_inplace(A, cnt)) {
+          cholesky_solve_inplace(A, cnt, b);
+          memcpy(w, b, sizeof(double) * cnt);
+        } else {
+          for (int a = 0; a < cnt; a++)
+            for (int c = 0; c < cnt; c++) A[(long)a * cnt + c] = K[(long)rpid[rr][a] * m + rpid[rr][c]];
+          memcpy(b, rkp[rr], sizeof(double) * cnt);
+          colpiv_qr_solve(A, cnt, b, w);
+        }
+        rw[rr] = w;
+      }
+      free(A); free(b);
     }
+    for (int r = 0; r < row; r++) {
+      if (rcnt[r] == 0) continue;
+      if (!rw[r]) {
+        if (full_ref < 0 || !rw[full_ref]) { rkeep[r] = 0; continue; }
+        rw[r] = (double*)malloc(sizeof(double) * m);
+        memcpy(rw[r], rw[full_ref], sizeof(double) * m);
+      }
+      double wsum = 0.0;
+      for (int a = 0; a < rcnt[r]; a++) wsum += rw[r][a];
+      if (wsum == 0.0) wsum = 1.0;
+      if (isnan(wsum)) rkeep[r] = 0;
+      else for (int a = 0; a < rcnt[r]; a++) rw[r][a] /= wsum;
+    }
+  }
+  /* phase 3: CSR */
+  int64_t nnz = 0;
+  rowptr[0] = 0;
+  for (int r = 0; r < row && status == 0; r++) {
+    const int keep = rkeep[r] ? rcnt[r] : 0;
     if (nnz + keep > max_nnz) { status = -1; break; }
     for (int a = 0; a < keep; a++) {
-      col[nnz + a] = cols[a];
-      if (solve) val[nnz + a] = w[a];
+      col[nnz + a] = rcols[r][a];
+      if (solve) val[nnz + a] = rw[r][a];
     }
     nnz += keep;
-    row++;
-    rowptr[row] = (int)nnz;
+    rowptr[r + 1] = (int)nnz;
   }
   *n_rows_out = row;
-  free(P); free(Pmm); free(K); free(bmap); free(cols); free(pidx); free(kp); free(Ks); free(w);
+  for (int r = 0; r < row; r++) { free(rcols[r]); free(rpid[r]); free(rkp[r]); free(rw[r]); }
+  free(rcols); free(rpid); free(rkp); free(rw); free(rcnt); free(rkeep);
+  free(P); free(Pmm); free(K); free(bmap);
   return status ? status : nnz;
 }
 
