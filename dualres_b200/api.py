@@ -130,6 +130,7 @@ def _declare(L):
                                     C.c_float, _ip, C.POINTER(C.c_int64), C.POINTER(_ip), C.POINTER(_ip),
                                     C.POINTER(_fp)]
     L.dr_debug_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
+    L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
     L.dr_debug_dual_averaging.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, vp,
@@ -420,6 +421,20 @@ def time_kernel(chains, which, step=1, reps=20):
     b = np.zeros(1, np.float64)
     check(lib().dr_debug_time_kernel(chains.h, which, step, reps, _ptr(ms), _ptr(b)))
     return float(ms[0]), float(b[0])
+
+
+def log_posterior_noalloc(data: MultiResData, mu_device_ptr: int, s_hr: float, s_sr: float):
+    """(log prior, log likelihood) of a device-resident field without any device allocation.
+
+    For callers that cannot call cudaMalloc/cudaFree (their device memory is owned by
+    another allocator, or their loop has stopped allocating).  mu_device_ptr points to
+    2N float32 values (re, im) on the volume's device.  Calls share one library-owned
+    scratch array: do not overlap them on the GPU.
+    """
+    out = np.zeros(2, np.float64)
+    check(lib().dr_log_posterior_noalloc(data.h, C.c_void_p(int(mu_device_ptr)), float(s_hr), float(s_sr),
+                                         _ptr(out)))
+    return float(out[0]), float(out[1])
 
 
 def kernel_launches(reset=False):

@@ -1085,4 +1085,129 @@ int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starti
   API_END
 }
 
+
 }  // extern "C"
+
+// ==================================================================== allocation-free evaluation
+namespace drb {
+
+// Scratch of dr_log_posterior_noalloc: one array in the library's device
+// image, so that the call itself never allocates.  Layout (bytes):
+//   [0, 16 MiB)      complex field, N <= 2^21
+//   [16, 24 MiB)     Re mu at data voxels, two halves of n_h <= 2^20
+//   [24, 28 MiB)     Ys - W mu_D, n_s <= 2^20
+//   [28, 32 MiB)     data gradient (written by the W^T kernel, not used)
+//   [32 MiB, +256 KiB) partial sums, chain state, result
+constexpr long long NA_MAX_N = 1LL << 21;
+constexpr long long NA_MAX_ROWS = 1LL << 20;
+constexpr size_t NA_FIELD = 0;
+constexpr size_t NA_MUD = NA_FIELD + sizeof(float2) * NA_MAX_N;
+constexpr size_t NA_RS = NA_MUD + 2 * sizeof(float) * NA_MAX_ROWS;
+constexpr size_t NA_GD = NA_RS + sizeof(float) * NA_MAX_ROWS;
+constexpr size_t NA_PART = NA_GD + sizeof(float) * NA_MAX_ROWS;
+constexpr int NA_MAXBLK = 148 * 8;
+constexpr int NA_EBLK = 296;
+constexpr size_t NA_EPART = NA_PART + ((sizeof(double) * NSLOT * NA_MAXBLK + 255) / 256) * 256;
+constexpr size_t NA_ST = NA_EPART + ((sizeof(double) * NA_EBLK + 255) / 256) * 256;
+constexpr size_t NA_OUT = NA_ST + ((sizeof(ChainState) + 255) / 256) * 256;
+constexpr size_t NA_BYTES = NA_OUT + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+static std::mutex g_na_mtx;
+static unsigned char* g_na_ptr[64] = {nullptr};
+
+// Device address of the scratch array on device `dev` (looked up once per
+// device with that device current; the host-side symbol is not a device address).
+static unsigned char* noalloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lk(g_na_mtx);
+  if (dev < 0 || dev >= 64) throw Error(DR_ERR_INVALID, "device ordinal out of range");
+  if (!g_na_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      throw Error(DR_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_na_ptr[dev] = (unsigned char*)p;
+  }
+  return g_na_ptr[dev];
+}
+
+// Sums the partials of the prior (mode 0 spectral energy), the W product and
+// the W^T product in a fixed order and forms (log prior, log likelihood).
+__global__ void k_noalloc_finish(const double* epart, int neblk, const double* part, int maxblk, int nbw, int nbwt,
+                                 const ChainState* st, double N, int n_s, double* out) {
+  __shared__ double red[8];
+  double e = 0.0, rh = 0.0, rs = 0.0;
+  for (int i = threadIdx.x; i < neblk; i += blockDim.x) e += epart[i];
+  e = block_sum(e, red);
+  for (int i = threadIdx.x; i < nbwt; i += blockDim.x) rh += part[(long long)SL_RH0 * maxblk + i];
+  rh = block_sum(rh, red);
+  if (n_s > 0)
+    for (int i = threadIdx.x; i < nbw; i += blockDim.x) rs += part[(long long)SL_RS0 * maxblk + i];
+  rs = block_sum(rs, red);
+  if (threadIdx.x == 0) {
+    out[0] = -0.5 * e / N;
+    out[1] = -0.5 * ((double)st->sh * rh + (n_s > 0 ? (double)st->ss * rs : 0.0));
+  }
+}
+
+}  // namespace drb
+
+extern "C" int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_device, float s_hr, float s_sr,
+                                        double* out) {
+  API_BEGIN
+  if (!v || !mu_device || !out) throw Error(DR_ERR_INVALID, "dr_log_posterior_noalloc: NULL argument");
+  const DevVolume& dv = v->dv;
+  if (dv.N > NA_MAX_N)
+    throw Error(DR_ERR_UNSUPPORTED, "dr_log_posterior_noalloc: embedding of " + std::to_string(dv.N) +
+                                        " points exceeds the scratch limit of 2^21 (use dr_log_posterior)");
+  if (dv.n_h > NA_MAX_ROWS || dv.n_s > NA_MAX_ROWS)
+    throw Error(DR_ERR_UNSUPPORTED, "dr_log_posterior_noalloc: more than 2^20 data voxels (use dr_log_posterior)");
+  CK(cudaSetDevice(v->device));
+  unsigned char* base = noalloc_scratch(v->device);
+  float2* field = (float2*)(base + NA_FIELD);
+  ChainState* st = (ChainState*)(base + NA_ST);
+  DevChains ch{};
+  ch.C = 1;
+  ch.Cp = 1;
+  ch.CG = 1;
+  ch.muD = (float*)(base + NA_MUD);
+  ch.rs = (float*)(base + NA_RS);
+  ch.gD = (float*)(base + NA_GD);
+  ch.part = (double*)(base + NA_PART);
+  ch.maxblk = NA_MAXBLK;
+  ch.nb_w = std::max(1, std::min(cdiv_i(dv.n_s, 8), NA_MAXBLK));
+  ch.nb_wt = std::max(1, std::min(cdiv_i(dv.n_h, 8), NA_MAXBLK));
+  ch.st = st;
+  ChainState h;
+  std::memset(&h, 0, sizeof(h));
+  h.sh = s_hr;
+  h.ss = s_sr;
+  h.acc = 0;
+  h.L_cur = 0;
+  cudaStream_t s = 0;
+  CK(cudaMemcpyAsync(st, &h, sizeof(ChainState), cudaMemcpyHostToDevice, s));
+  // Re mu at the data voxels, then the kriging residuals and their norms
+  k_gather_re<<<cdiv_i(dv.n_h, 256), 256, 0, s>>>((const float2*)mu_device, dv.d_flat, dv.n_h, ch.muD, 1, 0);
+  CK_LAUNCH();
+  if (dv.n_s > 0) {
+    k_spmv_w<1><<<ch.nb_w, 256, 0, s>>>(dv, ch, -1, 0, 0);
+    CK_LAUNCH();
+  }
+  k_spmv_wt<1><<<ch.nb_wt, 256, 0, s>>>(dv, ch, -1, 0, 0);
+  CK_LAUNCH();
+  // u = IFFT(mu) in the scratch field, then the prior's spectral sum
+  CK(cudaMemcpyAsync(field, mu_device, sizeof(float2) * dv.N, cudaMemcpyDeviceToDevice, s));
+  DevChains none{};
+  fft3d<float2>(field, v->hv.E, +1, 0, 1, v->tw_f, s, dv, none);
+  double* epart = (double*)(base + NA_EPART);
+  k_spectral_energy<<<NA_EBLK, 256, 0, s>>>(field, dv.sinv, dv.N, s_hr, 0, epart);
+  CK_LAUNCH();
+  double* dout = (double*)(base + NA_OUT);
+  k_noalloc_finish<<<1, 256, 0, s>>>(epart, NA_EBLK, ch.part, NA_MAXBLK, ch.nb_w, ch.nb_wt, st, (double)dv.N, dv.n_s,
+                                     dout);
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(out, dout, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  API_END
+}

@@ -165,6 +165,27 @@ int dr_gradient(dr_chainset* cs, int chain, const float* mu, float* grad);
 int dr_leapfrog_fixed(dr_chainset* cs, int chain, const float* mu0, const float* p0, float eps,
                       int L, float* mu_out, float* p_out, double* energies);
 
+/* Same result as dr_log_posterior, but the call allocates no device memory.
+ * It is meant for callers that cannot call cudaMalloc or cudaFree at this
+ * point: code whose device memory belongs to another allocator (a framework's
+ * caching allocator or a fixed arena), or a serving loop that has stopped
+ * allocating after start-up, since cudaFree synchronises the whole device and
+ * allocations fragment a shared pool.  No reference counterpart: the reference
+ * runs on the CPU only.
+ *   v          volume (created beforehand; its creation does allocate)
+ *   mu_device  real-space field on the device, 2N floats (re, im), x fastest
+ *   s_hr, s_sr sigma^-2 of the high-res and std-res data
+ *   out        host, out[0] = log prior, out[1] = log likelihood
+ * Scratch is one library-owned array of ~32 MiB that every GPU loading the
+ * library holds until the process exits.  Limits: N <= 2^21 (e.g. 128^3),
+ * n_highres <= 2^20, n_stdres <= 2^20; larger volumes get DR_ERR_UNSUPPORTED.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (several host threads, or several devices sharing a
+ * context) race, so serialise them.  The call runs on the legacy default
+ * stream and returns when the result is on the host. */
+int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_device, float s_hr, float s_sr, double* out);
+
 /* ---- host-side set-up --------------------------------------------------- */
 /* The kriging matrix of get_sparse_kriging_matrix_data (kriging_matrix.h:
  * 148-343), built on the host (no GPU needed).  `highres` must already be
