@@ -65,6 +65,12 @@ static void set_pass_attrs() {
   }
 }
 
+template <int E>
+static void set_plane_attr() {
+  const int bytes = E * (E + 1) * (int)sizeof(float2);
+  CK(cudaFuncSetAttribute(k_xyplane<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
 template <class C>
 static void set_all_attrs() {
   set_pass_attrs<2, C>(); set_pass_attrs<4, C>(); set_pass_attrs<8, C>(); set_pass_attrs<16, C>();
@@ -95,6 +101,8 @@ static DeviceTables& device_tables(int dev) {
   t.tw_d = (const double2*)p;
   set_all_attrs<float2>();
   set_all_attrs<double2>();
+  set_plane_attr<4>(); set_plane_attr<8>(); set_plane_attr<16>(); set_plane_attr<32>();
+  set_plane_attr<64>(); set_plane_attr<128>();
   t.ready = true;
   return t;
 }
@@ -287,6 +295,7 @@ struct Chainset {
   double* tmp_part = nullptr;   // spectral-energy partials
   int tmp_blocks = 0;
   int NR = 1;
+  bool plane = false;           // fused xy-plane update (E0 == E1 <= 128)
 
   template <class T>
   T* alloc(size_t n, bool zero = true) {
@@ -306,21 +315,38 @@ struct Chainset {
   }
 };
 
-static void launch_spmv(Chainset* S, int step, int sel, int chain_only, bool w) {
-  const DevVolume& v = S->vol->dv;
-  const int rows = w ? v.n_s : v.n_h;
-  const int nb = std::max(1, std::min(cdiv_i(rows, 8), w ? S->dc.nb_w : S->dc.nb_wt));
-#define SPMV(NR_)                                                                                                     \
-  if (w) k_spmv_w<NR_><<<nb, 256, 0, S->stream>>>(v, S->dc, step, sel, chain_only);                                   \
-  else k_spmv_wt<NR_><<<nb, 256, 0, S->stream>>>(v, S->dc, step, sel, chain_only);
-  switch (S->NR) {
-    case 1: SPMV(1); break;
-    case 2: SPMV(2); break;
-    case 4: SPMV(4); break;
-    default: SPMV(8); break;
-  }
-#undef SPMV
+template <int CG, int NR>
+static void launch_spmv_t(const DevVolume& v, const DevChains& ch, int nb, int step, int sel, int chain_only, bool w,
+                          cudaStream_t s) {
+  if (w)
+    k_spmv_w<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
+  else
+    k_spmv_wt<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
   CK_LAUNCH();
+}
+
+// Kriging products for `ch` (chain group width CG = ch.CG, rounds NR).
+static void launch_spmv_dc(const DevVolume& v, const DevChains& ch, int NR, int step, int sel, int chain_only, bool w,
+                           cudaStream_t s) {
+  const int nb = w ? std::max(1, std::min(v.n_s, ch.nb_w)) : std::max(1, std::min(cdiv_i(v.n_h, 8), ch.nb_wt));
+  switch (ch.CG) {
+    case 1: launch_spmv_t<1, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
+    case 2: launch_spmv_t<2, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
+    case 4: launch_spmv_t<4, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
+    case 8: launch_spmv_t<8, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
+    case 16: launch_spmv_t<16, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
+    default:
+      switch (NR) {
+        case 1: launch_spmv_t<32, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
+        case 2: launch_spmv_t<32, 2>(v, ch, nb, step, sel, chain_only, w, s); break;
+        case 4: launch_spmv_t<32, 4>(v, ch, nb, step, sel, chain_only, w, s); break;
+        default: launch_spmv_t<32, 8>(v, ch, nb, step, sel, chain_only, w, s); break;
+      }
+  }
+}
+
+static void launch_spmv(Chainset* S, int step, int sel, int chain_only, bool w) {
+  launch_spmv_dc(S->vol->dv, S->dc, S->NR, step, sel, chain_only, w, S->stream);
 }
 
 static void launch_xline(Chainset* S, int step, int flags) {
@@ -343,6 +369,23 @@ static void launch_xline(Chainset* S, int step, int flags) {
   CK_LAUNCH();
 }
 
+static void launch_plane(Chainset* S, int step, int flags) {
+  const DevVolume& v = S->vol->dv;
+  const dim3 grid(v.E2, S->C);
+  const size_t smem = (size_t)v.E0 * (v.E0 + 1) * sizeof(float2);
+  const float2* tw = S->vol->tw_f;
+  switch (v.E0) {
+    case 4: k_xyplane<4><<<grid, PlaneCfg<4>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 8: k_xyplane<8><<<grid, PlaneCfg<8>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 16: k_xyplane<16><<<grid, PlaneCfg<16>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 32: k_xyplane<32><<<grid, PlaneCfg<32>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 64: k_xyplane<64><<<grid, PlaneCfg<64>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 128: k_xyplane<128><<<grid, PlaneCfg<128>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    default: throw Error(DR_ERR_UNSUPPORTED, "plane size not supported");
+  }
+  CK_LAUNCH();
+}
+
 // The gradient/leapfrog sequence for steps 0..L (see kernels.cu header).
 static void enqueue_steps(Chainset* S, int L, int flags) {
   const DevVolume& v = S->vol->dv;
@@ -352,10 +395,11 @@ static void enqueue_steps(Chainset* S, int L, int flags) {
   for (int s = 0; s <= L; s++) {
     const int sel = s == 0 ? 0 : 1;
     if (s > 0) {
-      // forward y then z (pruned to the box), gather mu at data / output voxels
-      launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE,
-                          pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by, 1.0, s), v, ch, tw,
-                          C, S->stream);
+      if (!S->plane)
+        launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE,
+                            pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by, 1.0, s), v, ch,
+                            tw, C, S->stream);
+      // forward z (pruned to the box), gather mu at data / output voxels
       launch_pass<float2>(v.E2, -1, PRO_LOAD, EPI_GATHER,
                           pass_args(ch.T2, nullptr, ch.t2_stride, 0, 1, v.by * v.bx, v.E2, v.bz,
                                     1.0 / (double)v.N, s, 1, 2),
@@ -363,14 +407,18 @@ static void enqueue_steps(Chainset* S, int L, int flags) {
     }
     if (v.n_s > 0) launch_spmv(S, s, sel, -1, true);
     launch_spmv(S, s, sel, -1, false);
-    // inverse z then y from the box back to the spectral planes
+    // inverse z from the box back to spectral z
     launch_pass<float2>(v.E2, +1, PRO_DATAGRAD, EPI_STORE,
                         pass_args(nullptr, ch.T2, 0, ch.t2_stride, 1, v.by * v.bx, v.bz, v.E2, 1.0, s), v, ch, tw, C,
                         S->stream);
-    launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE,
-                        pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1, 1.0, s), v, ch, tw,
-                        C, S->stream);
-    launch_xline(S, s, flags);
+    if (S->plane) {
+      launch_plane(S, s, flags);
+    } else {
+      launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE,
+                          pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1, 1.0, s), v, ch,
+                          tw, C, S->stream);
+      launch_xline(S, s, flags);
+    }
   }
 }
 
@@ -447,16 +495,23 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   const long long N = v.N;
   ch.U = S->alloc<float2>((size_t)C * 2 * N);
   ch.Q = S->alloc<float2>((size_t)C * N);
-  ch.t1_stride = (long long)v.E2 * v.E1 * v.bx;
+  S->plane = v.E0 == v.E1 && v.E0 >= 4 && v.E0 <= 128 && !std::getenv("DRB_NO_PLANE");
   ch.t2_stride = (long long)v.E2 * v.by * v.bx;
-  ch.T1 = S->alloc<float2>((size_t)C * ch.t1_stride);
+  if (S->plane) {
+    // T1 is only needed by the initial transforms: borrow the momentum buffer
+    ch.t1_stride = N;
+    ch.T1 = ch.Q;
+  } else {
+    ch.t1_stride = (long long)v.E2 * v.E1 * v.bx;
+    ch.T1 = S->alloc<float2>((size_t)C * ch.t1_stride);
+  }
   ch.T2 = S->alloc<float2>((size_t)C * ch.t2_stride);
   ch.muD = S->alloc<float>((size_t)2 * v.n_h * C);
   ch.muO = S->alloc<float>((size_t)2 * std::max(v.n_o, 1) * C);
   ch.gD = S->alloc<float>((size_t)v.n_h * C);
   ch.rs = S->alloc<float>((size_t)std::max(v.n_s, 1) * C);
-  ch.nb_x = cdiv_i((long long)v.E1 * v.E2, TILE_LINES);
-  ch.nb_w = std::max(1, std::min(cdiv_i(v.n_s, 8), 148 * 8));
+  ch.nb_x = S->plane ? v.E2 : cdiv_i((long long)v.E1 * v.E2, TILE_LINES);
+  ch.nb_w = std::max(1, std::min(v.n_s, 148 * 8));
   ch.nb_wt = std::max(1, std::min(cdiv_i(v.n_h, 8), 148 * 8));
   ch.maxblk = std::max(ch.nb_x, std::max(ch.nb_w, ch.nb_wt));
   ch.part = S->alloc<double>((size_t)C * NSLOT * ch.maxblk);
@@ -1000,13 +1055,15 @@ int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* a
   const double N = (double)v.N, t1 = (double)ch.t1_stride, t2 = (double)ch.t2_stride, z = (double)s->vol->hv.w_col.size();
   auto launch = [&]() {
     switch (which) {
-      case 0: launch_xline(s, stp, 0); break;
-      case 1: launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE, pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by, 1.0, stp), v, ch, tw, C, s->stream); break;
+      case 0: if (s->plane) launch_plane(s, stp, 0); else launch_xline(s, stp, 0); break;
+      case 1: if (s->plane) break;
+        launch_pass<float2>(v.E1, -1, PRO_LOAD, EPI_STORE, pass_args(ch.T1, ch.T2, ch.t1_stride, ch.t2_stride, v.E2, v.bx, v.E1, v.by, 1.0, stp), v, ch, tw, C, s->stream); break;
       case 2: launch_pass<float2>(v.E2, -1, PRO_LOAD, EPI_GATHER, pass_args(ch.T2, nullptr, ch.t2_stride, 0, 1, v.by * v.bx, v.E2, v.bz, 1.0 / N, stp, 1, 2), v, ch, tw, C, s->stream); break;
       case 3: if (v.n_s > 0) launch_spmv(s, stp, 1, -1, true); break;
       case 4: launch_spmv(s, stp, 1, -1, false); break;
       case 5: launch_pass<float2>(v.E2, +1, PRO_DATAGRAD, EPI_STORE, pass_args(nullptr, ch.T2, 0, ch.t2_stride, 1, v.by * v.bx, v.bz, v.E2, 1.0, stp), v, ch, tw, C, s->stream); break;
-      default: launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE, pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1, 1.0, stp), v, ch, tw, C, s->stream); break;
+      default: if (s->plane) break;
+        launch_pass<float2>(v.E1, +1, PRO_LOAD, EPI_STORE, pass_args(ch.T2, ch.T1, ch.t2_stride, ch.t1_stride, v.E2, v.bx, v.by, v.E1, 1.0, stp), v, ch, tw, C, s->stream); break;
     }
   };
   launch();  // warm-up
@@ -1028,14 +1085,14 @@ int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* a
     const double box = (double)v.bx * v.by * v.bz;
     double b = 0.0;
     switch (which) {
-      case 0: b = C * (2.0 * t1 * 8 + 4.0 * N * 8) + N * 4; break;                  // T1 in/out, U and q in/out, 1/lambda
-      case 1: b = C * (t1 + t2) * 8; break;
+      case 0: b = C * (2.0 * (s->plane ? t2 : t1) * 8 + 4.0 * N * 8) + N * 4; break;  // T in/out, U and q in/out, 1/lambda
+      case 1: b = s->plane ? 0.0 : C * (t1 + t2) * 8; break;
       case 2: b = C * (t2 * 8 + (v.n_h + v.n_o) * 4.0) + box * 8; break;            // box maps (2 x int32)
       case 3: b = z * 8 + C * ((double)v.n_h * 4 + (double)v.n_s * 4) + v.n_s * 8.0; // W values + columns, mu_D, rs
         break;
       case 4: b = z * 8 + C * ((double)v.n_s * 4 + 2.0 * v.n_h * 4) + v.n_h * 12.0; break;
       case 5: b = C * ((double)v.n_h * 4 + t2 * 8) + box * 4; break;
-      default: b = C * (t2 + t1) * 8; break;
+      default: b = s->plane ? 0.0 : C * (t2 + t1) * 8; break;
     }
     *algo_bytes = b;
   }
@@ -1176,7 +1233,7 @@ extern "C" int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_devi
   ch.gD = (float*)(base + NA_GD);
   ch.part = (double*)(base + NA_PART);
   ch.maxblk = NA_MAXBLK;
-  ch.nb_w = std::max(1, std::min(cdiv_i(dv.n_s, 8), NA_MAXBLK));
+  ch.nb_w = std::max(1, std::min(dv.n_s, NA_MAXBLK));
   ch.nb_wt = std::max(1, std::min(cdiv_i(dv.n_h, 8), NA_MAXBLK));
   ch.st = st;
   ChainState h;
@@ -1190,12 +1247,8 @@ extern "C" int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_devi
   // Re mu at the data voxels, then the kriging residuals and their norms
   k_gather_re<<<cdiv_i(dv.n_h, 256), 256, 0, s>>>((const float2*)mu_device, dv.d_flat, dv.n_h, ch.muD, 1, 0);
   CK_LAUNCH();
-  if (dv.n_s > 0) {
-    k_spmv_w<1><<<ch.nb_w, 256, 0, s>>>(dv, ch, -1, 0, 0);
-    CK_LAUNCH();
-  }
-  k_spmv_wt<1><<<ch.nb_wt, 256, 0, s>>>(dv, ch, -1, 0, 0);
-  CK_LAUNCH();
+  if (dv.n_s > 0) launch_spmv_dc(dv, ch, 1, -1, 0, 0, true, s);
+  launch_spmv_dc(dv, ch, 1, -1, 0, 0, false, s);
   // u = IFFT(mu) in the scratch field, then the prior's spectral sum
   CK(cudaMemcpyAsync(field, mu_device, sizeof(float2) * dv.N, cudaMemcpyDeviceToDevice, s));
   DevChains none{};

@@ -305,95 +305,229 @@ __global__ void __launch_bounds__(XCfg<E0>::NT) k_xline(DevVolume v, DevChains c
   }
 }
 
-// ----------------------------------------------------------------- kriging products
-// Chain-activity helpers shared by the kriging kernels.
-struct ChainLanes {
-  int cc, grp, G;
+// ----------------------------------------------------------------- xy-plane kernel
+// The leapfrog update fused with the x and y transforms of one z-plane of one
+// chain (E0 == E1 == E).  In shared memory the plane is [y][x] with an odd
+// pitch, so row FFTs (x) and column FFTs (y) are both bank-conflict free.
+//   T2[c][z][y < by][x < bx]  --inverse y, inverse x-->  spectral plane
+//   kick / drift (as k_xline), then forward x, forward y --> T2 (pruned).
+template <int E> struct PlaneCfg {
+  static constexpr int NT = E >= 128 ? 512 : 256;
 };
 
-// rs = Ys - W mu_D for every chain (MultiResParameters.h:361-363, 505-507):
-// warp per row of W (grid-stride), chains across lanes.  The chain-minor
-// layout makes each nonzero read one contiguous vector of chain values.
-// NR = chain rounds per lane (C <= CG * NR).
-template <int NR>
-__global__ void __launch_bounds__(256) k_spmv_w(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int C = ch.C, Cp = ch.Cp, CG = ch.CG, G = 32 / CG;
-  const int cc = lane % CG, grp = lane / CG;
-  __shared__ double red[8][32 * NR];
-  const float* mrow[NR];
-  bool act[NR];
-  double sq[NR];
-#pragma unroll
-  for (int r = 0; r < NR; r++) {
-    const int c = cc + CG * r;
-    act[r] = false;
-    mrow[r] = ch.muD;
-    sq[r] = 0.0;
-    if (c < C && (chain_only < 0 || c == chain_only)) {
-      const ChainState& st = ch.st[c];
-      act[r] = step < 0 || step <= st.L_cur;
-      mrow[r] = ch.muD + (long long)(st.acc ^ sel) * v.n_h * Cp + c;
-    }
-  }
-  for (int row = blockIdx.x * 8 + warp; row < v.n_s; row += gridDim.x * 8) {
-    float acc[NR];
-#pragma unroll
-    for (int r = 0; r < NR; r++) acc[r] = 0.f;
-    const int k0 = v.w_rowptr[row], k1 = v.w_rowptr[row + 1];
-    for (int k = k0 + grp; k < k1; k += G) {
-      const float w = __ldg(v.w_val + k);
-      const long long col = (long long)__ldg(v.w_col + k) * Cp;
-#pragma unroll
-      for (int r = 0; r < NR; r++)
-        if (act[r]) acc[r] = fmaf(w, mrow[r][col], acc[r]);
-    }
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-      for (int off = CG; off < 32; off <<= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
-    if (grp == 0) {
-      const float ys = v.Ys[row];
-#pragma unroll
-      for (int r = 0; r < NR; r++) {
-        if (!act[r]) continue;
-        const float rsv = ys - acc[r];
-        ch.rs[(long long)row * Cp + cc + CG * r] = rsv;
-        sq[r] += (double)rsv * rsv;
-      }
-    }
-  }
-  if (grp == 0) {
-#pragma unroll
-    for (int r = 0; r < NR; r++) red[warp][cc + CG * r] = sq[r];
+template <int E>
+__global__ void __launch_bounds__(PlaneCfg<E>::NT) k_xyplane(DevVolume v, DevChains ch, int step, int flags,
+                                                             const float2* __restrict__ tw) {
+  constexpr int P = E + 1, NT = PlaneCfg<E>::NT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2* sm = reinterpret_cast<float2*>(smraw);
+  __shared__ double red[NT / 32];
+  const int c = blockIdx.y, z = blockIdx.x;
+  const ChainState& st = ch.st[c];
+  const int Lc = st.L_cur;
+  if (step > Lc) return;
+  const bool first = step == 0, last = step == Lc;
+  const float eps = st.eps_cur, sh = st.sh;
+  const int acc = st.acc;
+  const long long N = v.N;
+  const int bx = v.bx, by = v.by;
+  float2* Ub = ch.U + (long long)c * 2 * N;
+  const float2* Usrc = Ub + (long long)(first ? acc : (acc ^ 1)) * N + (long long)z * E * E;
+  float2* Udst = Ub + (long long)(acc ^ 1) * N + (long long)z * E * E;
+  float2* Qc = ch.Q + (long long)c * N + (long long)z * E * E;
+  const float* sinv = v.sinv + (long long)z * E * E;
+  float2* T = ch.T2 + (long long)c * ch.t2_stride + (long long)z * by * bx;
+  const float2* twE = tw + tw_offset(E);
+
+  for (int e = threadIdx.x; e < E * E; e += NT) {
+    const int y = e / E, x = e % E;
+    sm[y * P + x] = (y < by && x < bx) ? T[y * bx + x] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < C; c += blockDim.x) {
-    if (chain_only >= 0 && c != chain_only) continue;
-    const ChainState& st = ch.st[c];
-    if (step >= 0 && step > st.L_cur) continue;
-    double s = 0.0;
-    for (int w = 0; w < 8; w++) s += red[w][c];
-    const int slot = step <= 0 ? SL_RS0 : (step == st.L_cur ? SL_RSL : SL_SCRATCH);
-    ch.part[((long long)c * NSLOT + slot) * ch.maxblk + blockIdx.x] = s;
+  fft_smem<E, +1, E, NT>(sm, 1, P, bx, twE);  // columns x < bx along y
+  fft_smem<E, +1, E, NT>(sm, P, 1, E, twE);   // rows along x
+
+  const bool fixed = (flags & XF_FIXED_MOMENTUM) != 0;
+  const bool write_q = !last || (flags & XF_WRITE_Q_LAST);
+  const float keps = ((first || last) ? 0.5f : 1.0f) * eps;
+  const float Nf = (float)N;
+  double pa = 0.0, pb = 0.0;
+  for (int e = threadIdx.x; e < E * (E / 2); e += NT) {
+    const int y = e / (E / 2), x = 2 * (e % (E / 2));
+    const int li = y * E + x;
+    const float4 u4 = *reinterpret_cast<const float4*>(Usrc + li);
+    const float2 s2 = *reinterpret_cast<const float2*>(sinv + li);
+    float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 w0 = make_float2(0.f, 0.f), w1 = w0;
+    if (first && !fixed) {
+      const long long gi = (long long)z * E * E + li;
+      const u32x4 r = philox(u32x4{(uint32_t)(gi >> 1), (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c),
+                                   RNG_MOMENTUM}, ch.seed);
+      w0 = box_muller(u01f(r.x), u01f(r.y));
+      w1 = box_muller(u01f(r.z), u01f(r.w));
+      pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
+    } else {
+      q4 = *reinterpret_cast<const float4*>(Qc + li);
+    }
+    float2 uo[2], qo[2];
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const float2 u = m == 0 ? make_float2(u4.x, u4.y) : make_float2(u4.z, u4.w);
+      const float s = m == 0 ? s2.x : s2.y;
+      const bool live = s > 0.0f;
+      const float lm = s + sh;
+      float2 q;
+      if (first && !fixed) {
+        const float2 w = m == 0 ? w0 : w1;
+        const float a = live ? sqrtf(Nf * lm) : 0.0f;
+        q = make_float2(a * w.x, a * w.y);
+      } else {
+        q = m == 0 ? make_float2(q4.x, q4.y) : make_float2(q4.z, q4.w);
+        if (first && live) pa += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+      }
+      if (first && live) pb += (double)(u.x * u.x + u.y * u.y) * (double)s;
+      const float2 g = sm[y * P + x + m];
+      float2 gt = g;
+      if (live) {
+        gt.x = fmaf(-u.x, s, g.x);
+        gt.y = fmaf(-u.y, s, g.y);
+      }
+      q.x = fmaf(keps, gt.x, q.x);
+      q.y = fmaf(keps, gt.y, q.y);
+      float2 un = u;
+      if (last) {
+        if (live) {
+          pa += (double)(u.x * u.x + u.y * u.y) * (double)s;
+          pb += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+        }
+      } else if (live) {
+        const float f = eps / lm;
+        un.x = fmaf(f, q.x, u.x);
+        un.y = fmaf(f, q.y, u.y);
+      }
+      uo[m] = un;
+      qo[m] = q;
+      sm[y * P + x + m] = un;
+    }
+    if (write_q) *reinterpret_cast<float4*>(Qc + li) = make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y);
+    if (!last) *reinterpret_cast<float4*>(Udst + li) = make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y);
+  }
+  if (first || last) {
+    const double ta = block_sum(pa, red);
+    if (threadIdx.x == 0) ch.part[((long long)c * NSLOT + (first ? SL_E0 : SL_LPL)) * ch.maxblk + blockIdx.x] = ta;
+    const double tb = block_sum(pb, red);
+    if (threadIdx.x == 0) ch.part[((long long)c * NSLOT + (first ? SL_LP0 : SL_KL)) * ch.maxblk + blockIdx.x] = tb;
+  }
+  if (last) return;
+  __syncthreads();
+  fft_smem<E, -1, E, NT>(sm, P, 1, E, twE);   // rows along x
+  fft_smem<E, -1, E, NT>(sm, 1, P, bx, twE);  // columns x < bx along y
+  for (int e = threadIdx.x; e < by * bx; e += NT) {
+    const int y = e / bx, x = e % bx;
+    T[y * bx + x] = sm[y * P + x];
   }
 }
 
-// gD = sigma_h^-2 (Yh - mu_D) + sigma_s^-2 W^T rs (MultiResParameters.h:357-364):
-// warp per data voxel over the transposed CSR (grid-stride), plus
-// ||Yh - mu_D||^2 partials.
-template <int NR>
+// ----------------------------------------------------------------- kriging products
+// Chain-minor operands: X[j * Cp + c].  A warp's lanes are CG chain lanes x
+// G = 32 / CG nonzero groups; each lane owns NR chains (c = cc + CG r).
+//
+// Accumulates sum_k val[k] X[col[k]] over the 32-nonzero batches b0, b0 + bs,
+// ... of [ks, ke): the batch's values and columns are loaded once, coalesced,
+// and broadcast by shuffle, so the X loads of a batch are independent and
+// stay in flight together.
+template <int CG, int NR>
+__device__ __forceinline__ void csr_batches(const float* __restrict__ val, const int* __restrict__ col, int ks, int ke,
+                                            int b0, int bs, const float* const (&x)[NR], int Cp, int lane,
+                                            float (&acc)[NR]) {
+  constexpr int G = 32 / CG;
+  const int grp = lane / CG;
+  for (int base = ks + b0 * 32; base < ke; base += bs * 32) {
+    const int n = min(32, ke - base);
+    const float mv = lane < n ? __ldg(val + base + lane) : 0.f;
+    const int mc = lane < n ? __ldg(col + base + lane) : 0;
+#pragma unroll
+    for (int j0 = 0; j0 < 32; j0 += G) {
+      const int j = j0 + grp;
+      const float w = __shfl_sync(0xffffffffu, mv, j);
+      const long long cidx = (long long)__shfl_sync(0xffffffffu, mc, j) * Cp;
+      if (j < n) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) acc[r] = fmaf(w, x[r][cidx], acc[r]);
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < NR; r++)
+#pragma unroll
+    for (int off = CG; off < 32; off <<= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
+}
+
+// rs = Ys - W mu_D for every chain (MultiResParameters.h:361-363, 505-507),
+// one block per row of W (grid-stride over rows); the 8 warps share the
+// row's 32-nonzero batches and combine their sums in a fixed order.
+template <int CG, int NR>
+__global__ void __launch_bounds__(256) k_spmv_w(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int C = ch.C, Cp = ch.Cp;
+  const int cc = lane % CG;
+  __shared__ float red[8][CG * NR];
+  const float* x[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int c = min(cc + CG * r, C - 1);
+    x[r] = ch.muD + (long long)(ch.st[c].acc ^ sel) * v.n_h * Cp + c;
+  }
+  // thread t < C owns chain t for the row sums
+  const int t = threadIdx.x;
+  bool tact = false;
+  if (t < C && (chain_only < 0 || t == chain_only)) tact = step < 0 || step <= ch.st[t].L_cur;
+  double sq = 0.0;
+  for (int row = blockIdx.x; row < v.n_s; row += gridDim.x) {
+    float acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = 0.f;
+    csr_batches<CG, NR>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], warp, 8, x, Cp, lane, acc);
+    if (lane < CG) {
+#pragma unroll
+      for (int r = 0; r < NR; r++) red[warp][lane + CG * r] = acc[r];
+    }
+    __syncthreads();
+    if (tact) {
+      float s = 0.f;
+#pragma unroll
+      for (int w = 0; w < 8; w++) s += red[w][t];
+      const float rsv = v.Ys[row] - s;
+      ch.rs[(long long)row * Cp + t] = rsv;
+      sq += (double)rsv * rsv;
+    }
+    __syncthreads();
+  }
+  if (tact) {
+    const int slot = step <= 0 ? SL_RS0 : (step == ch.st[t].L_cur ? SL_RSL : SL_SCRATCH);
+    ch.part[((long long)t * NSLOT + slot) * ch.maxblk + blockIdx.x] = sq;
+  }
+}
+
+// gD = sigma_h^-2 (Yh - mu_D) + sigma_s^-2 W^T rs (MultiResParameters.h:357-364),
+// one warp per data voxel over the transposed CSR (grid-stride), plus the
+// ||Yh - mu_D||^2 partials per block.
+template <int CG, int NR>
 __global__ void __launch_bounds__(256) k_spmv_wt(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int C = ch.C, Cp = ch.Cp, CG = ch.CG, G = 32 / CG;
-  const int cc = lane % CG, grp = lane / CG;
-  __shared__ double red[8][32 * NR];
+  const int C = ch.C, Cp = ch.Cp;
+  const int cc = lane % CG;
+  __shared__ double red[8][CG * NR];
   bool act[NR];
   double sq[NR];
   int half[NR];
   float shv[NR], ssv[NR];
+  const float* x[NR];
 #pragma unroll
   for (int r = 0; r < NR; r++) {
     const int c = cc + CG * r;
+    const int cs = min(c, C - 1);
+    x[r] = ch.rs + cs;
     act[r] = false;
     sq[r] = 0.0;
     half[r] = 0;
@@ -410,20 +544,8 @@ __global__ void __launch_bounds__(256) k_spmv_wt(DevVolume v, DevChains ch, int 
     float acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
-    if (v.n_s > 0) {
-      const int k0 = v.wt_rowptr[row], k1 = v.wt_rowptr[row + 1];
-      for (int k = k0 + grp; k < k1; k += G) {
-        const float w = __ldg(v.wt_val + k);
-        const long long col = (long long)__ldg(v.wt_col + k) * Cp;
-#pragma unroll
-        for (int r = 0; r < NR; r++)
-          if (act[r]) acc[r] = fmaf(w, ch.rs[col + cc + CG * r], acc[r]);
-      }
-#pragma unroll
-      for (int r = 0; r < NR; r++)
-        for (int off = CG; off < 32; off <<= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
-    }
-    if (grp == 0) {
+    if (v.n_s > 0) csr_batches<CG, NR>(v.wt_val, v.wt_col, v.wt_rowptr[row], v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc);
+    if (lane < CG) {
       const float yh = v.Yh[row];
 #pragma unroll
       for (int r = 0; r < NR; r++) {
@@ -436,9 +558,9 @@ __global__ void __launch_bounds__(256) k_spmv_wt(DevVolume v, DevChains ch, int 
       }
     }
   }
-  if (grp == 0) {
+  if (lane < CG) {
 #pragma unroll
-    for (int r = 0; r < NR; r++) red[warp][cc + CG * r] = sq[r];
+    for (int r = 0; r < NR; r++) red[warp][lane + CG * r] = sq[r];
   }
   __syncthreads();
   for (int c = threadIdx.x; c < C; c += blockDim.x) {

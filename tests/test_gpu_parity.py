@@ -30,6 +30,17 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+@pytest.fixture(params=["plane", "lines"])
+def update_path(request, monkeypatch):
+    """Both device update paths: the fused xy-plane kernel (E0 == E1 <= 128) and the
+    x-line kernel + separate y passes (used for other embeddings)."""
+    if request.param == "lines":
+        monkeypatch.setenv("DRB_NO_PLANE", "1")
+    else:
+        monkeypatch.delenv("DRB_NO_PLANE", raising=False)
+    return request.param
+
+
 def volume_of(g):
     import dualres_b200 as d
     return d.MultiResData(g["highres"], g["qform_hr"], g["stdres"], g["qform_sr"], tuple(g["theta"]),
@@ -70,7 +81,7 @@ def test_volume_setup(name):
 
 
 @pytest.mark.parametrize("name", golden_cases())
-def test_log_posterior_and_gradient(oracle, name):
+def test_log_posterior_and_gradient(oracle, name, update_path):
     g = load(name)
     v = volume_of(g)
     p = chains_of(v)
@@ -89,7 +100,7 @@ def test_log_posterior_and_gradient(oracle, name):
 
 
 @pytest.mark.parametrize("name", golden_cases())
-def test_fixed_momentum_leapfrog(oracle, name):
+def test_fixed_momentum_leapfrog(oracle, name, update_path):
     g = load(name)
     v = volume_of(g)
     p = chains_of(v)
@@ -156,7 +167,7 @@ class _OracleHmc:
         return self.L.orc_hmc_integrator_steps(self.C.byref(self.h))
 
 
-def test_sampler_runs_and_counts():
+def test_sampler_runs_and_counts(update_path):
     import dualres_b200 as d
     g = load("g1_rbf_e1")
     v = volume_of(g)
@@ -174,7 +185,7 @@ def test_sampler_runs_and_counts():
     assert np.all(np.isfinite(summ["mean"])) and np.all(summ["var"] >= -1e-6)
 
 
-def test_chain_is_independent_of_batch():
+def test_chain_is_independent_of_batch(update_path):
     """Chain 0 of a 4-chain set follows the same trajectory as a 1-chain set
     with the same seed (RNG keyed by (seed, chain, iteration), never by slot)."""
     import dualres_b200 as d
