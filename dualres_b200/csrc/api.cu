@@ -47,6 +47,8 @@ static int cdiv_i(long long a, long long b) { return (int)((a + b - 1) / b); }
 // ---------------------------------------------------------------- per-device set-up
 struct DeviceTables {
   bool ready = false;
+  int sms = 148;
+  int tma_dyn_max = 0;  // dynamic shared memory available to the bulk-copy plane kernel
   const float2* tw_f = nullptr;
   const double2* tw_d = nullptr;
 };
@@ -65,10 +67,11 @@ static void set_pass_attrs() {
   }
 }
 
-template <int E>
-static void set_plane_attr() {
-  const int bytes = E * (E + 1) * (int)sizeof(float2);
-  CK(cudaFuncSetAttribute(k_xyplane<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+template <int E, bool PF>
+static void set_plane_attr(int dyn_max) {
+  const PlaneLayout Ly = plane_layout(E, PlaneGeom<E>::SIZE, PF);
+  if (Ly.total <= dyn_max)
+    CK(cudaFuncSetAttribute(k_xyplane<E, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, Ly.total));
 }
 
 template <class C>
@@ -101,8 +104,19 @@ static DeviceTables& device_tables(int dev) {
   t.tw_d = (const double2*)p;
   set_all_attrs<float2>();
   set_all_attrs<double2>();
-  set_plane_attr<4>(); set_plane_attr<8>(); set_plane_attr<16>(); set_plane_attr<32>();
-  set_plane_attr<64>(); set_plane_attr<128>();
+  {
+    int sms = 0, optin = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    t.sms = sms;
+    t.tma_dyn_max = optin - 256;  // the plane kernels' static shared memory is at most 128 bytes
+    set_plane_attr<4, false>(t.tma_dyn_max); set_plane_attr<8, false>(t.tma_dyn_max);
+    set_plane_attr<16, false>(t.tma_dyn_max); set_plane_attr<32, false>(t.tma_dyn_max);
+    set_plane_attr<64, false>(t.tma_dyn_max); set_plane_attr<128, false>(t.tma_dyn_max);
+    set_plane_attr<4, true>(t.tma_dyn_max); set_plane_attr<8, true>(t.tma_dyn_max);
+    set_plane_attr<16, true>(t.tma_dyn_max); set_plane_attr<32, true>(t.tma_dyn_max);
+    set_plane_attr<64, true>(t.tma_dyn_max);
+  }
   t.ready = true;
   return t;
 }
@@ -296,6 +310,8 @@ struct Chainset {
   int tmp_blocks = 0;
   int NR = 1;
   bool plane = false;           // fused xy-plane update (E0 == E1 <= 128)
+  bool tma = false;             // ... in the persistent bulk-copy kernel (E0 <= 64, fits shared memory)
+  int tma_smem = 0, tma_grid = 0;
 
   template <class T>
   T* alloc(size_t n, bool zero = true) {
@@ -329,6 +345,7 @@ static void launch_spmv_t(const DevVolume& v, const DevChains& ch, int nb, int s
 static void launch_spmv_dc(const DevVolume& v, const DevChains& ch, int NR, int step, int sel, int chain_only, bool w,
                            cudaStream_t s) {
   const int nb = w ? std::max(1, std::min(v.n_s, ch.nb_w)) : std::max(1, std::min(cdiv_i(v.n_h, 8), ch.nb_wt));
+  if (nb > ch.maxblk || ch.part == nullptr) throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the block count");
   switch (ch.CG) {
     case 1: launch_spmv_t<1, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
     case 2: launch_spmv_t<2, 1>(v, ch, nb, step, sel, chain_only, w, s); break;
@@ -351,6 +368,8 @@ static void launch_spmv(Chainset* S, int step, int sel, int chain_only, bool w) 
 
 static void launch_xline(Chainset* S, int step, int flags) {
   const DevVolume& v = S->vol->dv;
+  if (cdiv_i((long long)v.E1 * v.E2, TILE_LINES) > S->dc.maxblk)
+    throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the x-line block count");
   const dim3 grid(cdiv_i((long long)v.E1 * v.E2, TILE_LINES), S->C);
   const size_t smem = (size_t)v.E0 * (TILE_LINES + 1) * sizeof(float2);
   const float2* tw = S->vol->tw_f;
@@ -369,21 +388,37 @@ static void launch_xline(Chainset* S, int step, int flags) {
   CK_LAUNCH();
 }
 
-static void launch_plane(Chainset* S, int step, int flags) {
+template <int E, bool PF>
+static void launch_plane_t(Chainset* S, int step, int flags) {
   const DevVolume& v = S->vol->dv;
   const dim3 grid(v.E2, S->C);
-  const size_t smem = (size_t)v.E0 * (v.E0 + 1) * sizeof(float2);
-  const float2* tw = S->vol->tw_f;
+  const size_t smem = (size_t)plane_layout(E, PlaneGeom<E>::SIZE, PF).total;
+  k_xyplane<E, PF><<<grid, PlaneCfg<E, PF>::NT, smem, S->stream>>>(v, S->dc, step, flags, S->vol->tw_f);
+  CK_LAUNCH();
+}
+
+static void launch_plane(Chainset* S, int step, int flags) {
+  const DevVolume& v = S->vol->dv;
+  if (v.E2 > S->dc.maxblk) throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the plane count");
+  if (S->tma) {
+    switch (v.E0) {
+      case 4: launch_plane_t<4, true>(S, step, flags); return;
+      case 8: launch_plane_t<8, true>(S, step, flags); return;
+      case 16: launch_plane_t<16, true>(S, step, flags); return;
+      case 32: launch_plane_t<32, true>(S, step, flags); return;
+      case 64: launch_plane_t<64, true>(S, step, flags); return;
+      default: throw Error(DR_ERR_UNSUPPORTED, "plane size not supported by the bulk-copy kernel");
+    }
+  }
   switch (v.E0) {
-    case 4: k_xyplane<4><<<grid, PlaneCfg<4>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 8: k_xyplane<8><<<grid, PlaneCfg<8>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 16: k_xyplane<16><<<grid, PlaneCfg<16>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 32: k_xyplane<32><<<grid, PlaneCfg<32>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 64: k_xyplane<64><<<grid, PlaneCfg<64>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 128: k_xyplane<128><<<grid, PlaneCfg<128>::NT, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 4: launch_plane_t<4, false>(S, step, flags); break;
+    case 8: launch_plane_t<8, false>(S, step, flags); break;
+    case 16: launch_plane_t<16, false>(S, step, flags); break;
+    case 32: launch_plane_t<32, false>(S, step, flags); break;
+    case 64: launch_plane_t<64, false>(S, step, flags); break;
+    case 128: launch_plane_t<128, false>(S, step, flags); break;
     default: throw Error(DR_ERR_UNSUPPORTED, "plane size not supported");
   }
-  CK_LAUNCH();
 }
 
 // The gradient/leapfrog sequence for steps 0..L (see kernels.cu header).
@@ -496,6 +531,16 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   ch.U = S->alloc<float2>((size_t)C * 2 * N);
   ch.Q = S->alloc<float2>((size_t)C * N);
   S->plane = v.E0 == v.E1 && v.E0 >= 4 && v.E0 <= 128 && !std::getenv("DRB_NO_PLANE");
+  if (S->plane) {
+    // the fused plane kernel needs the whole padded plane in shared memory
+    const DeviceTables& dt = device_tables(V->device);
+    const int elems = v.E0 == 64 ? PlaneGeom<64>::SIZE : (v.E0 == 128 ? PlaneGeom<128>::SIZE : v.E0 * (v.E0 + 1));
+    if (plane_layout(v.E0, elems, false).total > dt.tma_dyn_max) S->plane = false;
+    // optional variant with bulk prefetch of the U, q and 1/lambda planes
+    if (S->plane && v.E0 <= 64 && std::getenv("DRB_PLANE_PREFETCH") &&
+        plane_layout(v.E0, elems, true).total <= dt.tma_dyn_max)
+      S->tma = true;
+  }
   ch.t2_stride = (long long)v.E2 * v.by * v.bx;
   if (S->plane) {
     // T1 is only needed by the initial transforms: borrow the momentum buffer
@@ -522,6 +567,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   ch.samples = o->store_samples ? S->alloc<float>((size_t)std::max(o->nsave, 1) * std::max(v.n_o, 1) * C, false) : nullptr;
   ch.seed = o->seed;
   ch.chain0 = 0;
+  ch.err = S->alloc<int>(1);
   S->tmp = S->alloc<float2>(N);
   S->tmp_blocks = 296;
   S->tmp_part = S->alloc<double>(S->tmp_blocks);
@@ -594,6 +640,9 @@ static void step(Chainset* S, int iters, double* device_ms = nullptr) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
+  int err = 0;
+  CK(cudaMemcpy(&err, S->dc.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
 }
 
 // Spectral state of chain c from a real-space field (host, 2N floats).

@@ -92,6 +92,7 @@ struct DevChains {
   float* samples;           // [nsave][n_o][Cp] or null
   uint64_t seed;
   int chain0;               // global id of chain 0 (RNG key component)
+  int* err;                 // device error word: bounded waits that gave up
 };
 
 // Pass-kernel arguments: a batched 1D FFT along the middle axis of an

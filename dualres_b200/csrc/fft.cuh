@@ -142,6 +142,73 @@ __device__ __forceinline__ void fft_stage(C* sm, int ls, int es, int nlines, con
 
 constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 
+// Warp-synchronous Stockham stage: lane `b` of the line's lane group owns
+// butterfly b (lanes with b >= N/R idle).  A line never leaves its warp, so
+// the read / write phases need only __syncwarp.
+template <int N, int R, int P, int DIR, class C>
+__device__ __forceinline__ void warp_stage(C* L, int es, int b, bool on, const C* __restrict__ tw) {
+  constexpr int M = N / P, Mn = M / R, NB = N / R;
+  const bool act = on && b < NB;
+  const int p = b / Mn, t = b % Mn;
+  C x[R];
+  if (act) {
+#pragma unroll
+    for (int j = 0; j < R; j++) x[j] = L[(p * M + t + Mn * j) * es];
+    reg_fft<R, DIR>(x);
+    if (Mn > 1) {
+#pragma unroll
+      for (int k = 1; k < R; k++) {
+        C wv = tw[P * t * k];
+        if (DIR > 0) wv.y = -wv.y;
+        x[k] = cmul(x[k], wv);
+      }
+    }
+  }
+  __syncwarp();
+  if (act) {
+#pragma unroll
+    for (int k = 0; k < R; k++) L[((p + P * k) * Mn + t) * es] = x[k];
+  }
+  __syncwarp();
+}
+
+// Largest butterfly count per line over the stages of the plan for N.
+template <int N>
+__host__ __device__ constexpr int plan_nbmax() {
+  return N <= 16 ? 1 : (N == 32 ? 8 : (N == 64 ? 8 : (N == 128 ? 16 : 16)));
+}
+
+// Warp-synchronous FFT of nlines lines (N <= 256): each warp takes groups of
+// 32 / nbmax lines; every stage runs with warp-level synchronisation only.
+// The block synchronises once at the end, so the tile is complete on return.
+template <int N, int DIR, class C>
+__device__ __forceinline__ void fft_smem_warp(C* sm, int ls, int es, int nlines, const C* __restrict__ tw) {
+  constexpr int NBM = plan_nbmax<N>(), LPW = 32 / NBM;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int li = lane / NBM, b = lane % NBM;
+  for (int base = warp * LPW; base < nlines; base += nw * LPW) {
+    const int line = base + li;
+    const bool on = li < LPW && line < nlines;
+    C* L = sm + (on ? line : 0) * ls;
+    if constexpr (N <= 16) {
+      warp_stage<N, N, 1, DIR, C>(L, es, b, on, tw);
+    } else if constexpr (N == 32) {
+      warp_stage<32, 8, 1, DIR, C>(L, es, b, on, tw);
+      warp_stage<32, 4, 8, DIR, C>(L, es, b, on, tw);
+    } else if constexpr (N == 64) {
+      warp_stage<64, 8, 1, DIR, C>(L, es, b, on, tw);
+      warp_stage<64, 8, 8, DIR, C>(L, es, b, on, tw);
+    } else if constexpr (N == 128) {
+      warp_stage<128, 16, 1, DIR, C>(L, es, b, on, tw);
+      warp_stage<128, 8, 16, DIR, C>(L, es, b, on, tw);
+    } else {
+      warp_stage<256, 16, 1, DIR, C>(L, es, b, on, tw);
+      warp_stage<256, 16, 16, DIR, C>(L, es, b, on, tw);
+    }
+  }
+  __syncthreads();
+}
+
 // Full FFT of nlines lines of length N held in shared memory.  MAXLINES and
 // NTHR bound the per-thread butterfly count at compile time.  The caller must
 // have synchronised after filling the tile; on return the tile is complete.
@@ -175,5 +242,104 @@ __device__ __forceinline__ void fft_smem(C* sm, int ls, int es, int nlines, cons
 // (lengths 2, 4, ..., 512; entry m of length N is exp(-2 pi i m / N)).
 __host__ __device__ constexpr int tw_offset(int N) { return N - 2; }
 constexpr int TW_TOTAL = 1022;
+
+// ----------------------------------------------------------------- padded 2D planes
+// An E x E plane stored with one pad slot after every 8 elements along both
+// axes: phys(y, x) = (y + y/8) * RP + x + x/8, with the row pitch RP = 8 mod 16
+// (complex units).  With the lane mappings below, every shared-memory access
+// of the two radix stages (including the stride-8 transpose between them) hits
+// 16 distinct 8-byte bank pairs per half-warp.
+template <int E>
+struct PaddedPlane {
+  static constexpr int RP = (E + E / 8) + ((8 - (E + E / 8) % 16) + 16) % 16;  // >= E + E/8, = 8 mod 16
+  static constexpr int ROWS = E + E / 8;
+  static constexpr int SIZE = ROWS * RP;                       // complex elements
+  __device__ __forceinline__ static int phys(int y, int x) { return (y + (y >> 3)) * RP + x + (x >> 3); }
+};
+
+// Two-stage plan (radices R1 then R2) of one line, with the line's element i at
+// sm[idx(i)].  LINE_FAST = false: lane = li * NBM + b (rows); true: lane =
+// li + 8 * bb, each lane owning butterflies bb, bb + 4, ... (columns).
+template <int N, int R1, int R2>
+struct Plan2 {
+  static constexpr int NB1 = N / R1, NB2 = N / R2;
+  static constexpr int NBM = NB1 > NB2 ? NB1 : NB2;
+};
+
+template <int N, int R, int P, int DIR, int PER_LANE, class Idx>
+__device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)[PER_LANE], bool on,
+                                            const float2* __restrict__ tw) {
+  constexpr int M = N / P, Mn = M / R, NB = N / R;
+  float2 x[PER_LANE][R];
+#pragma unroll
+  for (int q = 0; q < PER_LANE; q++) {
+    const int b = bl[q];
+    if (on && b < NB) {
+      const int p = b / Mn, t = b % Mn;
+#pragma unroll
+      for (int j = 0; j < R; j++) x[q][j] = sm[idx(p * M + t + Mn * j)];
+      reg_fft<R, DIR>(x[q]);
+      if (Mn > 1) {
+#pragma unroll
+        for (int k = 1; k < R; k++) {
+          float2 wv = tw[P * t * k];
+          if (DIR > 0) wv.y = -wv.y;
+          x[q][k] = cmul(x[q][k], wv);
+        }
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < PER_LANE; q++) {
+    const int b = bl[q];
+    if (on && b < NB) {
+      const int p = b / Mn, t = b % Mn;
+#pragma unroll
+      for (int k = 0; k < R; k++) sm[idx((p + P * k) * Mn + t)] = x[q][k];
+    }
+  }
+  __syncwarp();
+}
+
+// Row FFTs (lines = y rows, elements along x) of a padded plane, all E rows.
+template <int E, int R1, int R2, int DIR>
+__device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict__ tw) {
+  using PL = PaddedPlane<E>;
+  constexpr int NBM = Plan2<E, R1, R2>::NBM, LPW = 32 / NBM;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int li = lane / NBM;
+  const int bl[1] = {lane % NBM};
+  for (int base = warp * LPW; base < E; base += nw * LPW) {
+    const int y = base + li;
+    const bool on = li < LPW && y < E;
+    const int row = on ? (y + (y >> 3)) * PL::RP : 0;
+    auto idx = [row](int i) { return row + i + (i >> 3); };
+    plane_stage<E, R1, 1, DIR, 1>(sm, idx, bl, on, tw);
+    plane_stage<E, R2, R1, DIR, 1>(sm, idx, bl, on, tw);
+  }
+  __syncthreads();
+}
+
+// Column FFTs (lines = x columns, elements along y) of the first ncols columns.
+template <int E, int R1, int R2, int DIR>
+__device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* __restrict__ tw) {
+  using PL = PaddedPlane<E>;
+  constexpr int NBM = Plan2<E, R1, R2>::NBM, PL_LANE = NBM / 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int li = lane & 7, bb = lane >> 3;
+  int bl[PL_LANE];
+#pragma unroll
+  for (int q = 0; q < PL_LANE; q++) bl[q] = bb + 4 * q;
+  for (int base = warp * 8; base < ncols; base += nw * 8) {
+    const int x = base + li;
+    const bool on = x < ncols;
+    const int col = on ? x + (x >> 3) : 0;
+    auto idx = [col](int i) { return (i + (i >> 3)) * PL::RP + col; };
+    plane_stage<E, R1, 1, DIR, PL_LANE>(sm, idx, bl, on, tw);
+    plane_stage<E, R2, R1, DIR, PL_LANE>(sm, idx, bl, on, tw);
+  }
+  __syncthreads();
+}
 
 }  // namespace drb

@@ -412,6 +412,9 @@ int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err) {
     for (int i = 0; i < n_o; i++) b = std::max(b, O[3 * i + k] + 1);
     hv->box[k] = b;
   }
+  // even x-extent: every z-plane of the pruned intermediate then starts on a
+  // 16-byte boundary (bulk copies need that); E0 is even, so bx stays <= E0
+  hv->box[0] += hv->box[0] & 1;
   const int bx = hv->box[0], by = hv->box[1], bz = hv->box[2];
   hv->box_to_d.assign((size_t)bx * by * bz, -1);
   hv->box_to_o.assign((size_t)bx * by * bz, -1);

@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "drb.h"
 #include "fft.cuh"
+#include "tma.cuh"
 
 namespace drb {
 
@@ -306,60 +307,145 @@ __global__ void __launch_bounds__(XCfg<E0>::NT) k_xline(DevVolume v, DevChains c
 }
 
 // ----------------------------------------------------------------- xy-plane kernel
-// The leapfrog update fused with the x and y transforms of one z-plane of one
-// chain (E0 == E1 == E).  In shared memory the plane is [y][x] with an odd
-// pitch, so row FFTs (x) and column FFTs (y) are both bank-conflict free.
-//   T2[c][z][y < by][x < bx]  --inverse y, inverse x-->  spectral plane
-//   kick / drift (as k_xline), then forward x, forward y --> T2 (pruned).
-template <int E> struct PlaneCfg {
-  static constexpr int NT = E >= 128 ? 512 : 256;
+// The leapfrog update fused with the y and x transforms of one z-plane of one
+// chain (E0 == E1 == E), one block per (z-plane, chain):
+//   T2[c][z][y < by][x < bx] --inverse y (columns x < bx), inverse x (rows)-->
+//   spectral plane; kick / drift as in k_xline; forward x, forward y --> T2.
+// For E = 64 and 128 the plane uses the padded layout of PaddedPlane (bank-
+// conflict free radix stages); other sizes use an odd row pitch.  With
+// PREFETCH the plane's U, q and 1/lambda planes are brought into shared
+// memory at entry by bulk asynchronous copies (1D TMA, completion on an
+// mbarrier) so that their DRAM latency overlaps the inverse transforms; the
+// wait is bounded and a time-out is recorded in ch.err.
+template <int E>
+struct PlaneGeom {
+  static constexpr bool PADDED = (E == 64 || E == 128);
+  static constexpr int R1 = E == 128 ? 16 : 8, R2 = 8;
+  static constexpr int P = E + 1;  // odd pitch of the unpadded layout
+  static constexpr int SIZE = PADDED ? PaddedPlane<E>::SIZE : E * (E + 1);
+  __device__ __forceinline__ static int at(int y, int x) {
+    if constexpr (PADDED) return PaddedPlane<E>::phys(y, x);
+    else return y * P + x;
+  }
 };
 
-template <int E>
-__global__ void __launch_bounds__(PlaneCfg<E>::NT) k_xyplane(DevVolume v, DevChains ch, int step, int flags,
-                                                             const float2* __restrict__ tw) {
-  constexpr int P = E + 1, NT = PlaneCfg<E>::NT;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  float2* sm = reinterpret_cast<float2*>(smraw);
+template <int E, bool PREFETCH> struct PlaneCfg {
+  static constexpr int NT = (E >= 128 || PREFETCH) ? 512 : 256;
+  static constexpr int MINB = (E <= 64 && !PREFETCH) ? 4 : 1;  // blocks per SM the register budget targets
+};
+
+// Shared-memory layout in bytes: [mbarrier | plane | U | q | 1/lambda].
+struct PlaneLayout {
+  int plane_off, u_off, q_off, s_off, total;
+};
+__host__ __device__ inline PlaneLayout plane_layout(int E, int plane_elems, bool prefetch) {
+  PlaneLayout L;
+  L.plane_off = prefetch ? 128 : 0;
+  const int pe = (L.plane_off + plane_elems * 8 + 127) / 128 * 128;
+  L.u_off = pe;
+  L.q_off = pe + E * E * 8;
+  L.s_off = pe + 2 * E * E * 8;
+  L.total = prefetch ? L.s_off + E * E * 4 : L.plane_off + plane_elems * 8;
+  return L;
+}
+
+template <int E, bool PREFETCH>
+__device__ __forceinline__ void plane_fft(float2* sm, int ncols, bool rows_first, int dir, const float2* tw) {
+  using G = PlaneGeom<E>;
+  if constexpr (G::PADDED) {
+    if (dir > 0) {
+      plane_cols<E, G::R1, G::R2, +1>(sm, ncols, tw);
+      plane_rows<E, G::R1, G::R2, +1>(sm, tw);
+    } else {
+      plane_rows<E, G::R1, G::R2, -1>(sm, tw);
+      plane_cols<E, G::R1, G::R2, -1>(sm, ncols, tw);
+    }
+  } else {
+    if (dir > 0) {
+      fft_smem_warp<E, +1>(sm, 1, G::P, ncols, tw);
+      fft_smem_warp<E, +1>(sm, G::P, 1, E, tw);
+    } else {
+      fft_smem_warp<E, -1>(sm, G::P, 1, E, tw);
+      fft_smem_warp<E, -1>(sm, 1, G::P, ncols, tw);
+    }
+  }
+}
+
+template <int E, bool PREFETCH>
+__global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETCH>::MINB) k_xyplane(DevVolume v, DevChains ch, int step, int flags,
+                                                                       const float2* __restrict__ tw) {
+  using G = PlaneGeom<E>;
+  constexpr int NT = PlaneCfg<E, PREFETCH>::NT;
+  extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ double red[NT / 32];
+  const PlaneLayout Ly = plane_layout(E, G::SIZE, PREFETCH);
+  float2* sm = reinterpret_cast<float2*>(smraw + Ly.plane_off);
   const int c = blockIdx.y, z = blockIdx.x;
   const ChainState& st = ch.st[c];
   const int Lc = st.L_cur;
   if (step > Lc) return;
   const bool first = step == 0, last = step == Lc;
+  const bool fixed = (flags & XF_FIXED_MOMENTUM) != 0;
+  const bool need_q = !(first && !fixed);
   const float eps = st.eps_cur, sh = st.sh;
   const int acc = st.acc;
   const long long N = v.N;
   const int bx = v.bx, by = v.by;
+  const int tid = threadIdx.x;
   float2* Ub = ch.U + (long long)c * 2 * N;
   const float2* Usrc = Ub + (long long)(first ? acc : (acc ^ 1)) * N + (long long)z * E * E;
   float2* Udst = Ub + (long long)(acc ^ 1) * N + (long long)z * E * E;
   float2* Qc = ch.Q + (long long)c * N + (long long)z * E * E;
-  const float* sinv = v.sinv + (long long)z * E * E;
+  const float* Sg = v.sinv + (long long)z * E * E;
   float2* T = ch.T2 + (long long)c * ch.t2_stride + (long long)z * by * bx;
   const float2* twE = tw + tw_offset(E);
-
-  for (int e = threadIdx.x; e < E * E; e += NT) {
+  const float2* srcU = Usrc;
+  const float2* srcQ = Qc;
+  const float* srcS = Sg;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
+  if constexpr (PREFETCH) {
+    srcU = reinterpret_cast<const float2*>(smraw + Ly.u_off);
+    srcQ = reinterpret_cast<const float2*>(smraw + Ly.q_off);
+    srcS = reinterpret_cast<const float*>(smraw + Ly.s_off);
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      mbar_fence_init();
+      const uint32_t bu = E * E * 8, bs = E * E * 4;
+      mbar_arrive_expect_tx(bar, bu + bs + (need_q ? bu : 0));
+      bulk_g2s(smraw + Ly.u_off, Usrc, bu, bar);
+      if (need_q) bulk_g2s(smraw + Ly.q_off, Qc, bu, bar);
+      bulk_g2s(smraw + Ly.s_off, Sg, bs, bar);
+    }
+  }
+  for (int e = tid; e < E * E; e += NT) {
     const int y = e / E, x = e % E;
-    sm[y * P + x] = (y < by && x < bx) ? T[y * bx + x] : make_float2(0.f, 0.f);
+    sm[G::at(y, x)] = (y < by && x < bx) ? T[y * bx + x] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_smem<E, +1, E, NT>(sm, 1, P, bx, twE);  // columns x < bx along y
-  fft_smem<E, +1, E, NT>(sm, P, 1, E, twE);   // rows along x
+  plane_fft<E, PREFETCH>(sm, bx, false, +1, twE);
+  if constexpr (PREFETCH) {
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(ch.err, 1);
+        mbar_wait_bounded(bar, 0, 1 << 20);
+      }
+      return;
+    }
+  }
 
-  const bool fixed = (flags & XF_FIXED_MOMENTUM) != 0;
   const bool write_q = !last || (flags & XF_WRITE_Q_LAST);
   const float keps = ((first || last) ? 0.5f : 1.0f) * eps;
   const float Nf = (float)N;
   double pa = 0.0, pb = 0.0;
-  for (int e = threadIdx.x; e < E * (E / 2); e += NT) {
+  for (int e = tid; e < E * (E / 2); e += NT) {
     const int y = e / (E / 2), x = 2 * (e % (E / 2));
     const int li = y * E + x;
-    const float4 u4 = *reinterpret_cast<const float4*>(Usrc + li);
-    const float2 s2 = *reinterpret_cast<const float2*>(sinv + li);
+    const float4 u4 = *reinterpret_cast<const float4*>(srcU + li);
+    const float2 s2 = *reinterpret_cast<const float2*>(srcS + li);
     float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
     float2 w0 = make_float2(0.f, 0.f), w1 = w0;
-    if (first && !fixed) {
+    if (!need_q) {
       const long long gi = (long long)z * E * E + li;
       const u32x4 r = philox(u32x4{(uint32_t)(gi >> 1), (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c),
                                    RNG_MOMENTUM}, ch.seed);
@@ -367,8 +453,9 @@ __global__ void __launch_bounds__(PlaneCfg<E>::NT) k_xyplane(DevVolume v, DevCha
       w1 = box_muller(u01f(r.z), u01f(r.w));
       pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
     } else {
-      q4 = *reinterpret_cast<const float4*>(Qc + li);
+      q4 = *reinterpret_cast<const float4*>(srcQ + li);
     }
+    const int pi0 = G::at(y, x), pi1 = G::at(y, x + 1);
     float2 uo[2], qo[2];
 #pragma unroll
     for (int m = 0; m < 2; m++) {
@@ -377,7 +464,7 @@ __global__ void __launch_bounds__(PlaneCfg<E>::NT) k_xyplane(DevVolume v, DevCha
       const bool live = s > 0.0f;
       const float lm = s + sh;
       float2 q;
-      if (first && !fixed) {
+      if (!need_q) {
         const float2 w = m == 0 ? w0 : w1;
         const float a = live ? sqrtf(Nf * lm) : 0.0f;
         q = make_float2(a * w.x, a * w.y);
@@ -386,7 +473,8 @@ __global__ void __launch_bounds__(PlaneCfg<E>::NT) k_xyplane(DevVolume v, DevCha
         if (first && live) pa += (double)(q.x * q.x + q.y * q.y) / (double)lm;
       }
       if (first && live) pb += (double)(u.x * u.x + u.y * u.y) * (double)s;
-      const float2 g = sm[y * P + x + m];
+      const int pi = m == 0 ? pi0 : pi1;
+      const float2 g = sm[pi];
       float2 gt = g;
       if (live) {
         gt.x = fmaf(-u.x, s, g.x);
@@ -407,24 +495,23 @@ __global__ void __launch_bounds__(PlaneCfg<E>::NT) k_xyplane(DevVolume v, DevCha
       }
       uo[m] = un;
       qo[m] = q;
-      sm[y * P + x + m] = un;
+      sm[pi] = un;
     }
     if (write_q) *reinterpret_cast<float4*>(Qc + li) = make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y);
     if (!last) *reinterpret_cast<float4*>(Udst + li) = make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y);
   }
   if (first || last) {
     const double ta = block_sum(pa, red);
-    if (threadIdx.x == 0) ch.part[((long long)c * NSLOT + (first ? SL_E0 : SL_LPL)) * ch.maxblk + blockIdx.x] = ta;
+    if (tid == 0) ch.part[((long long)c * NSLOT + (first ? SL_E0 : SL_LPL)) * ch.maxblk + z] = ta;
     const double tb = block_sum(pb, red);
-    if (threadIdx.x == 0) ch.part[((long long)c * NSLOT + (first ? SL_LP0 : SL_KL)) * ch.maxblk + blockIdx.x] = tb;
+    if (tid == 0) ch.part[((long long)c * NSLOT + (first ? SL_LP0 : SL_KL)) * ch.maxblk + z] = tb;
   }
   if (last) return;
   __syncthreads();
-  fft_smem<E, -1, E, NT>(sm, P, 1, E, twE);   // rows along x
-  fft_smem<E, -1, E, NT>(sm, 1, P, bx, twE);  // columns x < bx along y
-  for (int e = threadIdx.x; e < by * bx; e += NT) {
+  plane_fft<E, PREFETCH>(sm, bx, true, -1, twE);
+  for (int e = tid; e < by * bx; e += NT) {
     const int y = e / bx, x = e % bx;
-    T[y * bx + x] = sm[y * P + x];
+    T[y * bx + x] = sm[G::at(y, x)];
   }
 }
 

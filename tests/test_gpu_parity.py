@@ -30,14 +30,17 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.fixture(params=["plane", "lines"])
+@pytest.fixture(params=["plane", "prefetch", "lines"])
 def update_path(request, monkeypatch):
-    """Both device update paths: the fused xy-plane kernel (E0 == E1 <= 128) and the
-    x-line kernel + separate y passes (used for other embeddings)."""
+    """The three device update paths: the fused xy-plane kernel (E0 == E1 <= 128,
+    the default), the same kernel with bulk-copy prefetch of the state planes,
+    and the x-line kernel with separate y passes (every other embedding)."""
+    monkeypatch.delenv("DRB_NO_PLANE", raising=False)
+    monkeypatch.delenv("DRB_PLANE_PREFETCH", raising=False)
     if request.param == "lines":
         monkeypatch.setenv("DRB_NO_PLANE", "1")
-    else:
-        monkeypatch.delenv("DRB_NO_PLANE", raising=False)
+    elif request.param == "prefetch":
+        monkeypatch.setenv("DRB_PLANE_PREFETCH", "1")
     return request.param
 
 
