@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -73,6 +74,22 @@ static bool cholesky(double* A, int m) {
     }
   }
   return true;
+}
+
+// L L^T x = b with a row-major transposed copy Lt of L (contiguous backward pass).
+static void cholesky_solve_t(const double* L, const double* Lt, int m, double* b) {
+  for (int i = 0; i < m; i++) {
+    const double* Li = L + (size_t)i * m;
+    double s = b[i];
+    for (int p = 0; p < i; p++) s -= Li[p] * b[p];
+    b[i] = s / Li[i];
+  }
+  for (int i = m - 1; i >= 0; i--) {
+    const double* Ti = Lt + (size_t)i * m;
+    double s = b[i];
+    for (int p = i + 1; p < m; p++) s -= Ti[p] * b[p];
+    b[i] = s / Ti[i];
+  }
 }
 
 static void cholesky_solve(const double* L, int m, double* b) {
@@ -290,6 +307,39 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
     *err = "kriging: a neighbourhood index falls outside the bounded high-res index map (undefined in the reference)";
     return DR_ERR_DOMAIN;
   }
+  // S = K^-1 once per volume (FP64).  A row with present offsets A and absent
+  // offsets B then has (K_AA)^-1 = S_AA - S_AB (S_BB)^-1 S_BA, which costs
+  // O(|A|^2 + |B|^3) instead of the O(|A|^3) of a direct solve; each row takes
+  // the cheaper route.  Not positive definite K (variance > 1) -> direct solves.
+  std::vector<double> Sinv;
+  bool have_inv = false;
+  if (!std::getenv("DRB_KRIGING_DIRECT")) {
+    std::vector<double> Lf(K);
+    if (cholesky(Lf.data(), m)) {
+      Sinv.assign((size_t)m * m, 0.0);
+      std::vector<double> Lt((size_t)m * m, 0.0);
+      for (int i = 0; i < m; i++)
+        for (int j = 0; j <= i; j++) Lt[(size_t)j * m + i] = Lf[(size_t)i * m + j];
+#pragma omp parallel
+      {
+        std::vector<double> e(m);
+#pragma omp for schedule(dynamic, 8)
+        for (int j = 0; j < m; j++) {
+          std::fill(e.begin(), e.end(), 0.0);
+          e[j] = 1.0;
+          cholesky_solve_t(Lf.data(), Lt.data(), m, e.data());
+          for (int i = 0; i < m; i++) Sinv[(size_t)i * m + j] = e[i];
+        }
+      }
+      // symmetrise (the two triangular solves leave O(eps) asymmetry)
+      for (int i = 0; i < m; i++)
+        for (int j = 0; j < i; j++) {
+          const double a = 0.5 * (Sinv[(size_t)i * m + j] + Sinv[(size_t)j * m + i]);
+          Sinv[(size_t)i * m + j] = Sinv[(size_t)j * m + i] = a;
+        }
+      have_inv = true;
+    }
+  }
   // Rows whose neighbourhood is complete share K; identical k' then share w.
   std::map<std::vector<double>, std::vector<double>> full_cache;
   std::mutex cache_mtx;
@@ -307,12 +357,49 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
         auto it = full_cache.find(rkp[ri]);
         if (it != full_cache.end()) { rw[ri] = it->second; continue; }
       }
-      A.resize((size_t)cnt * cnt);
-      for (int a = 0; a < cnt; a++)
-        for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)rpid[ri][a] * m + rpid[ri][c]];
-      b = rkp[ri];
       x.assign(cnt, 0.0);
-      if (cholesky(A.data(), cnt)) {
+      const int nb = m - cnt;
+      bool solved = false;
+      if (have_inv && (double)nb * nb * nb / 3.0 + (double)cnt * cnt < (double)cnt * cnt * cnt / 3.0) {
+        // Schur route: w = S_AA k - S_AB (S_BB^-1 (S_BA k))
+        std::vector<char> present(m, 0);
+        for (int a = 0; a < cnt; a++) present[rpid[ri][a]] = 1;
+        std::vector<int> B;
+        B.reserve(nb);
+        for (int j = 0; j < m; j++)
+          if (!present[j]) B.push_back(j);
+        const std::vector<double>& k = rkp[ri];
+        std::vector<double> t(nb, 0.0);
+        for (int q = 0; q < nb; q++) {
+          const double* Srow = Sinv.data() + (size_t)B[q] * m;
+          double acc = 0.0;
+          for (int a = 0; a < cnt; a++) acc += Srow[rpid[ri][a]] * k[a];
+          t[q] = acc;
+        }
+        A.resize((size_t)nb * nb);
+        for (int q = 0; q < nb; q++)
+          for (int r = 0; r < nb; r++) A[(size_t)q * nb + r] = Sinv[(size_t)B[q] * m + B[r]];
+        if (nb == 0 || cholesky(A.data(), nb)) {
+          if (nb > 0) cholesky_solve(A.data(), nb, t.data());
+          for (int a = 0; a < cnt; a++) {
+            const double* Srow = Sinv.data() + (size_t)rpid[ri][a] * m;
+            double acc = 0.0;
+            for (int c = 0; c < cnt; c++) acc += Srow[rpid[ri][c]] * k[c];
+            for (int q = 0; q < nb; q++) acc -= Srow[B[q]] * t[q];
+            x[a] = acc;
+          }
+          solved = true;
+        }
+      }
+      if (!solved) {
+        A.resize((size_t)cnt * cnt);
+        for (int a = 0; a < cnt; a++)
+          for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)rpid[ri][a] * m + rpid[ri][c]];
+        b = rkp[ri];
+      }
+      if (solved) {
+        // x holds the Schur solution
+      } else if (cholesky(A.data(), cnt)) {
         cholesky_solve(A.data(), cnt, b.data());
         x = b;
       } else {
