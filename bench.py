@@ -8,7 +8,13 @@ MultiResParameters::update + HMCParameters::update per chain).  Metric: HMC
 gradient evaluations per second (sum over chains of L + 1 per iteration).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload batched64|single_c1|single_c2] [--no-ess]
+                    [--workload batched64|single_c1|single_c2|served|served_c1] [--no-ess]
+
+Served workloads ("served": the C4 size/parameter distribution; "served_c1":
+fixed C1-size jobs): --steps jobs arrive as a Poisson process (20 jobs/s) at
+a continuous-batching server; after --warmup untimed jobs, the line reports
+fits completed per second, gradient evaluations per second over the makespan,
+and p50/p99 job latency (submission to result on the host).
 
 Under torchrun each rank runs its own 64-chain set on its GPU (chains are
 independent: no collective on the data path, weak scaling); the timed region
@@ -47,7 +53,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched64", choices=["batched64", "single_c1", "single_c2"])
+    ap.add_argument("--workload", default="batched64", choices=sorted(WORKLOADS))
+    ap.add_argument("--rate", type=float, default=-1.0, help="served workloads: arrivals per second")
     ap.add_argument("--no-ess", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
@@ -107,20 +114,33 @@ WORKLOADS = {
     "batched64": dict(chains=64, vol="c1", burnin=500, nsave=500, thin=3, leapfrog=25),
     "single_c1": dict(chains=1, vol="c1", burnin=200, nsave=200, thin=1, leapfrog=25),
     "single_c2": dict(chains=1, vol="c2", burnin=200, nsave=200, thin=1, leapfrog=25),
+    "tiny": dict(chains=2, vol="small", burnin=10, nsave=10, thin=1, leapfrog=5),  # test-sized
+    # served streams: a step is one job; jobs arrive as a Poisson process
+    "served": dict(chains=1, vol="c4", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
+    "served_c1": dict(chains=1, vol="c1", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
+    "served_tiny": dict(chains=1, vol="small", burnin=20, nsave=20, thin=1, leapfrog=5, rate=50.0),  # test-sized
 }
 
 
 def make_volume(name):
     from dualres_b200 import synth
+    if name == "small":
+        return synth.small_volume()
+    if name == "c4":
+        return synth.config_c4_volume(0)
     return synth.config_c1() if name == "c1" else synth.config_c2()
 
 
 def config_of(w, extra=None):
+    vol = WORKLOADS[w]["vol"]
+    desc = {"c1": ("32x32x32 @ 1mm", "64^3", [0.806, 0.132, 1.0], 6.9),
+            "c2": ("64x64x48 @ 1.5mm", "128^3", [1.0, 0.4, 1.5], 6.9),
+            "small": ("10x9x7 @ 1mm", "32x16x16", [0.8, 0.3, 1.0], 3.2),
+            "c4": ("uniform over 32^3, 48x48x40, 64x64x48, 80x80x64 @ 1mm", "64^3 .. 256x256x128",
+                   "RBF v=1, b~U[0.1,0.6], e~U[1,2]", 6.9)}[vol]
     cfg = {"workload": w, **{k: v for k, v in WORKLOADS[w].items()},
-           "latent_grid": "32x32x32 @ 1mm" if WORKLOADS[w]["vol"] == "c1" else "64x64x48 @ 1.5mm",
-           "embedding": "64^3" if WORKLOADS[w]["vol"] == "c1" else "128^3",
-           "covariance": [0.806, 0.132, 1.0] if WORKLOADS[w]["vol"] == "c1" else [1.0, 0.4, 1.5],
-           "neighborhood_mm": 6.9, "parallelism": "independent chains per GPU (no collective)"}
+           "latent_grid": desc[0], "embedding": desc[1], "covariance": desc[2],
+           "neighborhood_mm": desc[3], "parallelism": "independent chains per GPU (no collective)"}
     if extra:
         cfg.update(extra)
     return cfg
@@ -247,6 +267,19 @@ def run_ours(args, dist):
     value = grads_all / t_max
 
     extra = {}
+    # ---- the plain single-chain GPU form on the same volume (same kernels, one chain)
+    if C > 1:
+        one = d.MultiResParameters(data, d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"],
+                                                         leapfrog=wl["leapfrog"], seed=args.seed + 3), 1)
+        one.update(args.warmup)
+        a = one.stats()[0]["grad_evals"]
+        one_ms = one.update_timed(args.steps)
+        g1 = one.stats()[0]["grad_evals"] - a
+        r1 = g1 / (one_ms / 1e3)
+        extra["single_chain_gpu"] = {"value": r1, "unit": UNIT, "ms_per_step": one_ms / args.steps,
+                                     "batched_over_single": (grads / (ms / 1e3)) / r1}
+        one.close()
+
     # ---- ESS/s of voxelwise posterior means on the full configured job (fresh chain set)
     if not args.no_ess and dist.rank == 0:
         hmc2 = d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"], leapfrog=wl["leapfrog"],
@@ -308,6 +341,86 @@ def run_ours(args, dist):
     }
     chains.close()
     data.close()
+    return line
+
+
+
+# ------------------------------------------------------------------ served stream
+def served_volume(wl, i, seed):
+    from dualres_b200 import synth
+    if wl["vol"] == "c4":
+        return synth.config_c4_volume(i, seed=seed)
+    if wl["vol"] == "small":
+        return synth.small_volume(seed=seed + i)
+    v = synth.config_c1()
+    return v
+
+
+def run_served(args, dist):
+    import dualres_b200 as d
+    wl = WORKLOADS[args.workload]
+    rate = args.rate if args.rate > 0 else wl["rate"]
+    hmc = lambda i: d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"],  # noqa: E731
+                                    leapfrog=wl["leapfrog"], seed=args.seed + 7919 * dist.rank + i)
+    t0 = time.perf_counter()
+    vols = [served_volume(wl, i, args.seed + dist.rank * 100003) for i in range(args.warmup + args.steps)]
+    gen_s = time.perf_counter() - t0
+    rng = np.random.default_rng(args.seed + dist.rank)
+    gaps = rng.exponential(1.0 / rate, size=args.steps)
+    sv = d.Server(device=0, iterations_per_round=8, host_threads=4)
+    # warm-up jobs (untimed): library tables, pools, first graphs
+    for i in range(args.warmup):
+        sv.submit_volume(vols[i], hmc(i), wl["chains"])
+    sv.drain(3600)
+    st0 = sv.stats()
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    dist.barrier()
+    clk.start()
+    t_start = time.perf_counter()
+    ids = []
+    t_next = t_start
+    for k in range(args.steps):
+        t_next += gaps[k]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(sv.submit_volume(vols[args.warmup + k], hmc(args.warmup + k), wl["chains"]))
+    sv.drain(3600)
+    makespan = time.perf_counter() - t_start
+    clocks = clk.stop()
+    st1 = sv.stats()
+    res = [sv.result(j) for j in ids]
+    lat = np.array([r.latency_s for r in res])
+    queue = np.array([r.queue_s for r in res])
+    grads = sum(r.grad_evals for r in res)
+    sizes = [v.highres.shape for v in vols[args.warmup:]]
+    makespan = dist.max(makespan)
+    grads_all = dist.sum(grads)
+    jobs_all = dist.sum(len(ids))
+    img_bytes = sum(v.highres.nbytes + (v.stdres.nbytes if v.stdres is not None else 0) for v in vols[args.warmup:])
+    out_bytes = sum(3 * 4 * len(r.mean) for r in res)
+    line = {
+        "metric": "served HMC gradient evals/sec", "value": grads_all / makespan, "unit": UNIT,
+        "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": makespan * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded GP draws)",
+        "config": config_of(args.workload, {"arrival_rate_per_s": rate, "jobs": args.steps,
+                                            "grids": [list(s[::-1]) for s in sizes],
+                                            "l2": "every job's state is its own; total resident state above L2",
+                                            "volume_generation_seconds": gen_s}),
+        "jobs_per_s": jobs_all / makespan,
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max()), "mean": float(lat.mean())},
+        "queue_s": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
+        "mh_rate": {"median": float(np.median([r.mh_rate for r in res]))},
+        "server": {"peak_running": int(st1.peak_running), "peak_device_bytes": int(st1.peak_device_bytes),
+                   "failed": int(st1.failed - st0.failed)},
+        "e2e": {"value": grads_all / makespan, "unit": UNIT,
+                "h2d_bytes_per_step": int(img_bytes / args.steps), "d2h_bytes_per_step": int(out_bytes / args.steps),
+                "includes": "arrival process + host set-up (masks, kriging) + device set-up + sampling + result d2h"},
+        "gpu_launches": int(st1.kernel_launches - st0.kernel_launches), "clocks": clocks,
+    }
+    sv.close()
     return line
 
 
@@ -428,6 +541,12 @@ def main():
         dist.close()
         return
     dist = Dist("nccl")
+    if "rate" in WORKLOADS[args.workload]:
+        line = run_served(args, dist)
+        if dist.rank == 0:
+            print(json.dumps(line), flush=True)
+        dist.close()
+        return
     line = run_ours(args, dist)
     if dist.rank == 0:
         if dist.world == 1 and not args.no_cpu:

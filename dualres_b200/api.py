@@ -69,6 +69,26 @@ class HmcOpts(C.Structure):
                 ("store_samples", C.c_int)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_int64), ("max_active", C.c_int),
+                ("iterations_per_round", C.c_int), ("host_threads", C.c_int)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int), ("error", C.c_int), ("submit_s", C.c_double), ("admit_s", C.c_double),
+                ("finish_s", C.c_double), ("grad_evals", C.c_int64), ("mh_rate", C.c_float),
+                ("n_output", C.c_int), ("device_bytes", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("done", C.c_int64), ("failed", C.c_int64), ("running", C.c_int64),
+                ("grad_evals", C.c_int64), ("peak_device_bytes", C.c_int64), ("peak_running", C.c_int),
+                ("busy_s", C.c_double), ("kernel_launches", C.c_int64)]
+
+
+JOB_QUEUED, JOB_READY, JOB_RUNNING, JOB_DONE, JOB_FAILED = range(5)
+
+
 class ChainStats(C.Structure):
     _fields_ = [("iteration", C.c_int), ("saved", C.c_int), ("integrator_steps", C.c_int), ("eps", C.c_float),
                 ("mh_rate", C.c_float), ("sigma_hr", C.c_float), ("sigma_sr", C.c_float),
@@ -133,6 +153,16 @@ def _declare(L):
     L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
+    L.dr_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
+    L.dr_server_submit.argtypes = [vp, C.POINTER(VolumeDesc), C.POINTER(HmcOpts), C.c_int, C.POINTER(C.c_uint64)]
+    L.dr_server_status.argtypes = [vp, C.c_uint64, C.POINTER(JobStatus)]
+    L.dr_server_result.argtypes = [vp, C.c_uint64, vp, vp, vp]
+    L.dr_server_wait.argtypes = [vp, C.c_uint64, C.c_double]
+    L.dr_server_drain.argtypes = [vp, C.c_double]
+    L.dr_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
+    L.dr_server_forget.argtypes = [vp, C.c_uint64]
+    L.dr_server_destroy.argtypes = [vp]
+    L.dr_server_destroy.restype = None
     L.dr_debug_dual_averaging.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, vp,
                                           vp, vp, C.c_int]
 
@@ -178,6 +208,39 @@ def kriging_matrix(highres, qform_hr, stdres, qform_sr, covariance, neighborhood
     return rowptr, col, val
 
 
+def _volume_desc(keep, highres, qform_hr, stdres, qform_sr, covariance, neighborhood, hmask, omask, smask,
+                 covfun, device):
+    """A dr_volume_desc over float32 copies of the images (kept alive in ``keep``)."""
+    hr = _f32(highres)
+    nz, ny, nx = hr.shape
+    d = VolumeDesc()
+    d.nx, d.ny, d.nz = nx, ny, nz
+
+    def fp(a):
+        if a is None:
+            return None
+        a = _f32(a)
+        keep.append(a)
+        return a.ctypes.data_as(_fp)
+
+    d.highres = fp(hr)
+    d.qform_hr = fp(qform_hr)
+    d.hmask = fp(hmask)
+    d.omask = fp(omask)
+    if stdres is not None:
+        sr = _f32(stdres)
+        d.sz, d.sy, d.sx = sr.shape
+        d.stdres = fp(sr)
+        d.qform_sr = fp(qform_sr)
+        d.smask = fp(smask)
+    for i in range(3):
+        d.covariance[i] = float(covariance[i])
+    d.covfun = covfun
+    d.neighborhood = float(neighborhood)
+    d.device = device
+    return d
+
+
 class MultiResData:
     """A volume on the GPU: the inputs of MultiResData<T> (MultiResData.h:96-127) plus
     the one-time part of the MultiResParameters<T> constructor."""
@@ -186,33 +249,8 @@ class MultiResData:
                  neighborhood=-1.0, hmask=None, omask=None, smask=None, covfun=DR_COV_RBF, device=0):
         L = lib()
         self._keep = []
-        hr = _f32(highres)
-        nz, ny, nx = hr.shape
-        d = VolumeDesc()
-        d.nx, d.ny, d.nz = nx, ny, nz
-
-        def fp(a):
-            if a is None:
-                return None
-            a = _f32(a)
-            self._keep.append(a)
-            return a.ctypes.data_as(_fp)
-
-        d.highres = fp(hr)
-        d.qform_hr = fp(qform_hr)
-        d.hmask = fp(hmask)
-        d.omask = fp(omask)
-        if stdres is not None:
-            sr = _f32(stdres)
-            d.sz, d.sy, d.sx = sr.shape
-            d.stdres = fp(sr)
-            d.qform_sr = fp(qform_sr)
-            d.smask = fp(smask)
-        for i in range(3):
-            d.covariance[i] = float(covariance[i])
-        d.covfun = covfun
-        d.neighborhood = float(neighborhood)
-        d.device = device
+        d = _volume_desc(self._keep, highres, qform_hr, stdres, qform_sr, covariance, neighborhood, hmask, omask,
+                         smask, covfun, device)
         h = C.c_void_p()
         check(L.dr_volume_create(C.byref(d), C.byref(h)))
         self._keep = []
@@ -439,3 +477,92 @@ def log_posterior_noalloc(data: MultiResData, mu_device_ptr: int, s_hr: float, s
 
 def kernel_launches(reset=False):
     return int(lib().dr_kernel_launches(1 if reset else 0))
+
+
+@dataclass
+class JobResult:
+    mean: np.ndarray
+    var: np.ndarray
+    activation: np.ndarray
+    mh_rate: float
+    grad_evals: int
+    latency_s: float          # submission to result on the host
+    queue_s: float            # submission to admission on the device
+    device_bytes: int
+
+
+class Server:
+    """Continuous batching of independent fits on one GPU (dr_server_*).
+
+    ``submit`` copies the images and returns a job id at once; host set-up runs
+    on worker threads, and a scheduler thread admits prepared jobs while their
+    device footprint fits ``hbm_budget_bytes``, advancing every resident job
+    ``iterations_per_round`` iterations per round on its own stream.  A job's
+    result does not depend on what else runs beside it."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=64, iterations_per_round=8, host_threads=4):
+        L = lib()
+        o = ServerOpts(device, int(hbm_budget_bytes), max_active, iterations_per_round, host_threads)
+        h = C.c_void_p()
+        check(L.dr_server_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def submit(self, highres, qform_hr, stdres=None, qform_sr=None, covariance=(1.0, 0.6, 1.5), neighborhood=-1.0,
+               hmask=None, omask=None, smask=None, covfun=DR_COV_RBF, hmc: HMCParameters | None = None,
+               n_chains=1):
+        keep = []
+        d = _volume_desc(keep, highres, qform_hr, stdres, qform_sr, covariance, neighborhood, hmask, omask, smask,
+                         covfun, self.device)
+        o = (hmc or HMCParameters()).c()
+        jid = C.c_uint64(0)
+        check(lib().dr_server_submit(self.h, C.byref(d), C.byref(o), int(n_chains), C.byref(jid)))
+        return int(jid.value)
+
+    def submit_volume(self, vol, hmc: HMCParameters | None = None, n_chains=1):
+        """Submit a ``dualres_b200.synth.Volume``."""
+        return self.submit(vol.highres, vol.qform_hr, vol.stdres, vol.qform_sr, vol.theta, vol.radius,
+                           hmask=vol.hmask, omask=vol.omask, hmc=hmc, n_chains=n_chains)
+
+    def status(self, job):
+        st = JobStatus()
+        check(lib().dr_server_status(self.h, job, C.byref(st)))
+        return st
+
+    def wait(self, job, timeout=600.0):
+        check(lib().dr_server_wait(self.h, job, float(timeout)))
+
+    def drain(self, timeout=3600.0):
+        check(lib().dr_server_drain(self.h, float(timeout)))
+
+    def result(self, job, forget=False):
+        st = self.status(job)
+        n = st.n_output
+        mean, var, act = (np.empty(n, np.float32) for _ in range(3))
+        check(lib().dr_server_result(self.h, job, _ptr(mean), _ptr(var), _ptr(act)))
+        if forget:
+            check(lib().dr_server_forget(self.h, job))
+        return JobResult(mean, var, act, float(st.mh_rate), int(st.grad_evals), st.finish_s - st.submit_s,
+                         st.admit_s - st.submit_s, int(st.device_bytes))
+
+    def stats(self):
+        s = ServerStats()
+        check(lib().dr_server_stats_get(self.h, C.byref(s)))
+        return s
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dr_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

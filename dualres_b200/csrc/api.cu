@@ -3,7 +3,13 @@
 // One translation unit holds every kernel (kernels.cu) so that template
 // instantiation and the twiddle tables stay in one module.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -16,6 +22,10 @@
 #include "../../include/dualres_b200.h"
 #include "host_setup.h"
 #include "kernels.cu"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace drb {
 
@@ -196,6 +206,11 @@ static void fft3d(C* f, const int* E, int dir, long long cs, int nch, const C* t
 // ---------------------------------------------------------------- volume
 struct Volume {
   int device = 0;
+  cudaStream_t stream = nullptr;  // uploads, spectrum and stream-ordered frees
+  // Chain sets bound to this volume; a volume released while some remain is
+  // freed by the last of them (g_vol_mtx guards both fields).
+  int n_chainsets = 0;
+  bool released = false;
   HostVolume hv;
   DevVolume dv{};
   std::vector<void*> allocs;
@@ -211,8 +226,8 @@ struct Volume {
   T* alloc(size_t n) {
     void* p = nullptr;
     if (n == 0) n = 1;
-    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    const cudaError_t e = cudaMallocAsync(&p, n * sizeof(T), stream);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     allocs.push_back(p);
     bytes += (int64_t)(n * sizeof(T));
     return (T*)p;
@@ -220,29 +235,33 @@ struct Volume {
   template <class T>
   T* upload(const std::vector<T>& h) {
     T* d = alloc<T>(h.size());
-    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (!h.empty()) CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     return d;
   }
-  ~Volume() {
-    if (!allocs.empty()) {
+  virtual ~Volume() {
+    if (stream) {
       cudaSetDevice(device);
-      for (void* p : allocs) cudaFree(p);
+      for (void* p : allocs) cudaFreeAsync(p, stream);
+      cudaStreamDestroy(stream);
+      cudaGetLastError();  // a failed release must not surface in the caller's next launch check
     }
   }
 };
 
-static void volume_build(Volume* V, const dr_volume_desc* d) {
+static std::mutex g_vol_mtx;
+
+// Device part of a volume from an already prepared HostVolume (V->hv).
+static void volume_build_device(Volume* V, const float* covariance, int covfun, int device) {
   const auto t0 = std::chrono::steady_clock::now();
-  V->device = d->device;
-  DeviceTables& dt = device_tables(d->device);
-  CK(cudaSetDevice(d->device));
+  V->device = device;
+  DeviceTables& dt = device_tables(device);
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&V->stream, cudaStreamNonBlocking));
   V->tw_f = dt.tw_f;
   V->tw_d = dt.tw_d;
-  std::string err;
-  const int rc = host_prepare(d, &V->hv, &err);
-  if (rc != DR_OK) throw Error(rc, err);
   HostVolume& hv = V->hv;
   DevVolume& dv = V->dv;
+  cudaStream_t st = V->stream;
   dv.E0 = hv.E[0]; dv.E1 = hv.E[1]; dv.E2 = hv.E[2]; dv.N = hv.N;
   dv.bx = hv.box[0]; dv.by = hv.box[1]; dv.bz = hv.box[2];
   dv.n_h = (int)hv.Yh.size(); dv.n_s = (int)hv.Ys.size(); dv.n_o = (int)hv.o_flat.size();
@@ -264,35 +283,50 @@ static void volume_build(Volume* V, const dr_volume_desc* d) {
   float* sinv = V->alloc<float>(N);
   V->lam_re = V->alloc<double>(N);
   double2* base = nullptr;
-  CK(cudaMalloc(&base, sizeof(double2) * N));
   int* nS = nullptr;
-  CK(cudaMalloc(&nS, sizeof(int)));
+  CK(cudaMallocAsync(&base, sizeof(double2) * N, st));
+  const cudaError_t e2 = cudaMallocAsync(&nS, sizeof(int), st);
+  if (e2 != cudaSuccess) {
+    cudaFreeAsync(base, st);
+    throw Error(DR_ERR_NOMEM, "cudaMallocAsync (spectrum scratch)");
+  }
   try {
-    CK(cudaMemset(nS, 0, sizeof(int)));
+    CK(cudaMemsetAsync(nS, 0, sizeof(int), st));
     const float* Q = hv.Q;
-    k_base<<<cdiv_i(N, 256), 256>>>(base, hv.E[0], hv.E[1], hv.E[2], Q[0], Q[1], Q[2], Q[4], Q[5], Q[6], Q[8], Q[9],
-                                      Q[10], (double)d->covariance[0], (double)d->covariance[1],
-                                      (double)d->covariance[2], d->covfun);
+    k_base<<<cdiv_i(N, 256), 256, 0, st>>>(base, hv.E[0], hv.E[1], hv.E[2], Q[0], Q[1], Q[2], Q[4], Q[5], Q[6], Q[8],
+                                           Q[9], Q[10], (double)covariance[0], (double)covariance[1],
+                                           (double)covariance[2], covfun);
     CK_LAUNCH();
     DevChains none{};
-    fft3d<double2>(base, hv.E, -1, 0, 1, V->tw_d, 0, dv, none);
-    k_spectrum<<<cdiv_i(N, 256), 256>>>(base, sinv, V->lam_re, N, nS);
+    fft3d<double2>(base, hv.E, -1, 0, 1, V->tw_d, st, dv, none);
+    k_spectrum<<<cdiv_i(N, 256), 256, 0, st>>>(base, sinv, V->lam_re, N, nS);
     CK_LAUNCH();
     double2 l0;
-    CK(cudaMemcpy(&l0, base, sizeof(double2), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&V->n_S, nS, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&l0, base, sizeof(double2), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&V->n_S, nS, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     V->max_eig = l0.x / (double)N;
   } catch (...) {
-    cudaFree(base);
-    cudaFree(nS);
+    cudaFreeAsync(base, st);
+    cudaFreeAsync(nS, st);
     throw;
   }
-  cudaFree(base);
-  cudaFree(nS);
+  cudaFreeAsync(base, st);
+  cudaFreeAsync(nS, st);
   dv.sinv = sinv;
   if ((long long)V->n_S >= N / 2) throw Error(DR_ERR_DOMAIN, "Too many negative eigen values");
-  CK(cudaDeviceSynchronize());
+  CK(cudaStreamSynchronize(st));
+  V->setup_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+static void volume_build(Volume* V, const dr_volume_desc* d) {
+  const auto t0 = std::chrono::steady_clock::now();
+  device_tables(d->device);
+  std::string err;
+  const int rc = host_prepare(d, &V->hv, &err);
+  if (rc != DR_OK) throw Error(rc, err);
   V->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  volume_build_device(V, d->covariance, d->covfun, d->device);
 }
 
 // ---------------------------------------------------------------- chainset
@@ -313,23 +347,51 @@ struct Chainset {
   bool tma = false;             // ... in the persistent bulk-copy kernel (E0 <= 64, fits shared memory)
   int tma_smem = 0, tma_grid = 0;
 
+  int64_t bytes = 0;
+  cudaEvent_t done_event = nullptr;  // recorded after the last launched iteration (server)
+
   template <class T>
   T* alloc(size_t n, bool zero = true) {
     void* p = nullptr;
     if (n == 0) n = 1;
-    const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    const cudaError_t e = cudaMallocAsync(&p, n * sizeof(T), stream);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     allocs.push_back(p);
-    if (zero) CK(cudaMemset(p, 0, n * sizeof(T)));
+    bytes += (int64_t)(n * sizeof(T));
+    if (zero) CK(cudaMemsetAsync(p, 0, n * sizeof(T), stream));
     return (T*)p;
   }
+  int device = 0;
   ~Chainset() {
-    if (vol) cudaSetDevice(vol->device);
+    cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
-    if (stream) cudaStreamDestroy(stream);
-    for (void* p : allocs) cudaFree(p);
+    if (done_event) cudaEventDestroy(done_event);
+    if (stream) {
+      for (void* p : allocs) cudaFreeAsync(p, stream);
+      cudaStreamDestroy(stream);
+    }
+    cudaGetLastError();
+    if (vol) {
+      bool last = false;
+      {
+        std::lock_guard<std::mutex> lk(g_vol_mtx);
+        last = --vol->n_chainsets == 0 && vol->released;
+      }
+      if (last) delete vol;
+    }
   }
 };
+
+// Frees a volume now, or when its last chain set is destroyed.
+static void volume_release(Volume* v) {
+  if (!v) return;
+  {
+    std::lock_guard<std::mutex> lk(g_vol_mtx);
+    v->released = true;
+    if (v->n_chainsets > 0) return;
+  }
+  delete v;
+}
 
 template <int CG, int NR>
 static void launch_spmv_t(const DevVolume& v, const DevChains& ch, int nb, int step, int sel, int chain_only, bool w,
@@ -500,7 +562,8 @@ static void init_chain_states(Chainset* S) {
     h.done = o.nsave <= 0 ? 1 : 0;
     st[c] = h;
   }
-  CK(cudaMemcpy(S->dc.st, st.data(), sizeof(ChainState) * S->C, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(S->dc.st, st.data(), sizeof(ChainState) * S->C, cudaMemcpyHostToDevice, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
 }
 
 static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) {
@@ -511,7 +574,12 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   if (o->thin < 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: thin must be >= 0");
   if (o->leapfrog <= 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: integrator_steps must be > 0");
   if (!(o->mhtarget > 0 && o->mhtarget < 1)) throw Error(DR_ERR_DOMAIN, "HMCParameters: mh_target should be within (0, 1)");
-  S->vol = V;
+  {
+    std::lock_guard<std::mutex> lk(g_vol_mtx);
+    S->vol = V;
+    V->n_chainsets++;
+  }
+  S->device = V->device;
   S->C = C;
   S->opts = *o;
   CK(cudaSetDevice(V->device));
@@ -601,26 +669,48 @@ static void write_states(Chainset* S, const std::vector<ChainState>& st) {
   CK(cudaStreamSynchronize(S->stream));
 }
 
+static void ensure_graph(Chainset* S) {
+  if (S->graph) return;
+  cudaGraph_t g = nullptr;
+  const int64_t before = g_launches;
+  CK(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_iteration(S);
+  } catch (...) {
+    cudaStreamEndCapture(S->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    g_launches = before;
+    throw;
+  }
+  CK(cudaStreamEndCapture(S->stream, &g));
+  S->graph_nodes = g_launches - before;
+  g_launches = before;
+  const cudaError_t e = cudaGraphInstantiate(&S->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) throw Error(DR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+}
+
+// Enqueues `iters` iterations without waiting (the server's round).
+static void launch_iterations(Chainset* S, int iters) {
+  ensure_graph(S);
+  for (int i = 0; i < iters; i++) {
+    CK(cudaGraphLaunch(S->graph, S->stream));
+    g_launches += S->graph_nodes;
+  }
+  if (!S->done_event) CK(cudaEventCreateWithFlags(&S->done_event, cudaEventDisableTiming));
+  CK(cudaEventRecord(S->done_event, S->stream));
+}
+
+static void check_device_error(Chainset* S) {
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, S->dc.err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+  CK(cudaStreamSynchronize(S->stream));
+  if (err) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+}
+
 static void step(Chainset* S, int iters, double* device_ms = nullptr) {
   CK(cudaSetDevice(S->vol->device));
-  if (!S->graph) {
-    cudaGraph_t g = nullptr;
-    const int64_t before = g_launches;
-    CK(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
-    try {
-      enqueue_iteration(S);
-    } catch (...) {
-      cudaStreamEndCapture(S->stream, &g);
-      if (g) cudaGraphDestroy(g);
-      throw;
-    }
-    CK(cudaStreamEndCapture(S->stream, &g));
-    S->graph_nodes = g_launches - before;
-    g_launches = before;
-    const cudaError_t e = cudaGraphInstantiate(&S->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) throw Error(DR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-  }
+  ensure_graph(S);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (device_ms) {
     CK(cudaEventCreate(&e0));
@@ -640,9 +730,42 @@ static void step(Chainset* S, int iters, double* device_ms = nullptr) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
-  int err = 0;
-  CK(cudaMemcpy(&err, S->dc.err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+  check_device_error(S);
+}
+
+// Posterior summary of mcmc_summary<T> (gaussian_process_model.h:191-316) over
+// chain `chain`, or pooled over all chains when chain = -1.
+static void summary_of(Chainset* s, int chain, float* mean, float* var, float* activation) {
+  const DevVolume& v = s->vol->dv;
+  const size_t n = (size_t)v.n_o * s->C;
+  std::vector<double> s1(n), s2(n), sa(n);
+  CK(cudaSetDevice(s->vol->device));
+  CK(cudaMemcpyAsync(s1.data(), s->dc.s1, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(s2.data(), s->dc.s2, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(sa.data(), s->dc.sa, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const int c0 = chain < 0 ? 0 : chain, c1 = chain < 0 ? s->C : chain + 1;
+  double ns = 0.0;
+  for (int c = c0; c < c1; c++) ns += st[c].saved;
+  if (ns <= 0) ns = 1;  // mcmc_summary::samples() (gaussian_process_model.h:255-258)
+  std::vector<double> act(v.n_o);
+  double amax = -1e300;
+  for (int o = 0; o < v.n_o; o++) {
+    double a1 = 0, a2 = 0, aa = 0;
+    for (int c = c0; c < c1; c++) {
+      a1 += s1[(size_t)o * s->C + c];
+      a2 += s2[(size_t)o * s->C + c];
+      aa += sa[(size_t)o * s->C + c];
+    }
+    const double m = a1 / ns, vr = (a2 - a1 * a1 / ns) / ns;
+    if (mean) mean[o] = (float)m;
+    if (var) var[o] = (float)vr;
+    act[o] = aa / (ns * std::sqrt(vr));
+    amax = std::max(amax, act[o]);
+  }
+  if (activation)
+    for (int o = 0; o < v.n_o; o++) activation[o] = (float)(act[o] / amax);
 }
 
 // Spectral state of chain c from a real-space field (host, 2N floats).
@@ -790,7 +913,7 @@ int dr_volume_data_get(const dr_volume* v, float* Yh, float* Ys) {
   API_END
 }
 
-void dr_volume_destroy(dr_volume* v) { delete v; }
+void dr_volume_destroy(dr_volume* v) { volume_release(v); }
 
 int dr_chainset_create(dr_volume* v, int n_chains, const dr_hmc_opts* opts, dr_chainset** out) {
   API_BEGIN
@@ -862,36 +985,7 @@ int dr_chain_stats_get(dr_chainset* s, dr_chain_stats* out) {
 int dr_summary_get(dr_chainset* s, int chain, float* mean, float* var, float* activation) {
   API_BEGIN
   if (!s || chain < -1 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad chain");
-  const DevVolume& v = s->vol->dv;
-  const size_t n = (size_t)v.n_o * s->C;
-  std::vector<double> s1(n), s2(n), sa(n);
-  CK(cudaSetDevice(s->vol->device));
-  CK(cudaMemcpy(s1.data(), s->dc.s1, sizeof(double) * n, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(s2.data(), s->dc.s2, sizeof(double) * n, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(sa.data(), s->dc.sa, sizeof(double) * n, cudaMemcpyDeviceToHost));
-  std::vector<ChainState> st;
-  read_states(s, &st);
-  const int c0 = chain < 0 ? 0 : chain, c1 = chain < 0 ? s->C : chain + 1;
-  double ns = 0.0;
-  for (int c = c0; c < c1; c++) ns += st[c].saved;
-  if (ns <= 0) ns = 1;  // mcmc_summary::samples() (gaussian_process_model.h:255-258)
-  std::vector<double> act(v.n_o);
-  double amax = -1e300;
-  for (int o = 0; o < v.n_o; o++) {
-    double a1 = 0, a2 = 0, aa = 0;
-    for (int c = c0; c < c1; c++) {
-      a1 += s1[(size_t)o * s->C + c];
-      a2 += s2[(size_t)o * s->C + c];
-      aa += sa[(size_t)o * s->C + c];
-    }
-    const double m = a1 / ns, vr = (a2 - a1 * a1 / ns) / ns;
-    if (mean) mean[o] = (float)m;
-    if (var) var[o] = (float)vr;
-    act[o] = aa / (ns * std::sqrt(vr));
-    amax = std::max(amax, act[o]);
-  }
-  if (activation)
-    for (int o = 0; o < v.n_o; o++) activation[o] = (float)(act[o] / amax);
+  summary_of(s, chain, mean, var, activation);
   API_END
 }
 
@@ -1191,6 +1285,415 @@ int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starti
   API_END
 }
 
+
+}  // extern "C"
+
+
+// ==================================================================== server
+namespace drb {
+
+struct Job {
+  uint64_t id = 0;
+  std::vector<float> hr, hm, om, sr, sm;
+  float qh[16], qs[16];
+  dr_volume_desc desc{};
+  dr_hmc_opts opts{};
+  int C = 1;
+  int state = DR_JOB_QUEUED;
+  int error = 0;
+  std::string msg;
+  double t_submit = 0, t_admit = 0, t_finish = 0;
+  std::unique_ptr<Volume> vol;
+  std::unique_ptr<Chainset> cs;
+  int64_t est_bytes = 0, bytes = 0;
+  int iters_total = 0, iters_launched = 0;
+  bool in_flight = false;
+  std::vector<float> mean, var, act;
+  int64_t grads = 0;
+  float mh = 0.f;
+  int n_output = 0;
+};
+
+// Device bytes of a volume + chain set before creating them (admission).
+static int64_t estimate_bytes(const HostVolume& hv, int C, const dr_hmc_opts& o) {
+  const double N = (double)hv.N, box = (double)hv.box[0] * hv.box[1] * hv.box[2];
+  const double nh = (double)hv.Yh.size(), ns = (double)hv.Ys.size(), no = (double)hv.o_flat.size();
+  const double nnz = (double)hv.w_col.size();
+  const double t2 = (double)hv.E[2] * hv.box[1] * hv.box[0];
+  double vol = box * 8 + (nh + no) * 4 + (nh + ns) * 4 + (ns + nh + 2) * 4 + nnz * 16 + N * 12 + N * 16;
+  double cs = C * (3 * N * 8 + t2 * 8 + (hv.E[0] == hv.E[1] ? 0.0 : (double)hv.E[2] * hv.E[1] * hv.box[0] * 8)) +
+              C * (2 * (nh + no) * 4 + (nh + ns) * 4 + no * 24) + N * 8 + (double)C * 9 * 2048 * 8;
+  if (o.store_samples) cs += (double)std::max(o.nsave, 1) * no * C * 4;
+  return (int64_t)(1.10 * (vol + cs)) + (16 << 20);
+}
+
+struct Server {
+  dr_server_opts o{};
+  std::mutex mtx;
+  std::condition_variable cv_work, cv_done;
+  std::map<uint64_t, std::shared_ptr<Job>> jobs;
+  std::deque<std::shared_ptr<Job>> setup_q, ready_q;
+  std::vector<std::shared_ptr<Job>> active;  // scheduler thread only
+  std::vector<std::thread> workers;
+  std::thread sched;
+  bool stop = false;
+  uint64_t next_id = 1;
+  int64_t budget = 0, in_use = 0, peak_bytes = 0;
+  int peak_running = 0;
+  int64_t n_submitted = 0, n_done = 0, n_failed = 0, grads_done = 0, launches = 0;
+  double last_finish = 0;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+
+  void fail(const std::shared_ptr<Job>& j, int code, const std::string& msg) {
+    // caller holds mtx
+    j->state = DR_JOB_FAILED;
+    j->error = code;
+    j->msg = msg;
+    j->t_finish = now();
+    n_failed++;
+    cv_done.notify_all();
+  }
+
+  void worker_loop(int nthreads) {
+#ifdef _OPENMP
+    omp_set_num_threads(std::max(1, nthreads));
+#endif
+    for (;;) {
+      std::shared_ptr<Job> j;
+      {
+        std::unique_lock<std::mutex> lk(mtx);
+        cv_work.wait(lk, [&] { return stop || !setup_q.empty(); });
+        if (stop) return;
+        j = setup_q.front();
+        setup_q.pop_front();
+      }
+      auto vol = std::make_unique<Volume>();
+      std::string err;
+      int rc = DR_OK;
+      try {
+        rc = host_prepare(&j->desc, &vol->hv, &err);
+      } catch (const std::exception& e) {
+        rc = DR_ERR_INVALID;
+        err = e.what();
+      }
+      std::lock_guard<std::mutex> lk(mtx);
+      j->hr.clear(); j->hr.shrink_to_fit();
+      j->hm.clear(); j->om.clear(); j->sr.clear(); j->sm.clear();
+      if (rc != DR_OK) {
+        fail(j, rc, err);
+        continue;
+      }
+      j->est_bytes = estimate_bytes(vol->hv, j->C, j->opts);
+      j->vol = std::move(vol);
+      j->state = DR_JOB_READY;
+      ready_q.push_back(j);
+      cv_work.notify_all();
+    }
+  }
+
+  void finalize(const std::shared_ptr<Job>& j) {
+    Chainset* cs = j->cs.get();
+    check_device_error(cs);
+    j->n_output = cs->vol->dv.n_o;
+    j->mean.resize(j->n_output);
+    j->var.resize(j->n_output);
+    j->act.resize(j->n_output);
+    summary_of(cs, -1, j->mean.data(), j->var.data(), j->act.data());
+    std::vector<ChainState> st;
+    read_states(cs, &st);
+    int64_t g = 0;
+    double mh = 0;
+    for (const auto& h : st) {
+      g += h.grad_evals;
+      const int d = h.iteration - h.burnin;
+      mh += h.mh_running_sum / std::max(d, 1);
+    }
+    j->grads = g;
+    j->mh = (float)(mh / st.size());
+    j->cs.reset();
+    j->vol.reset();
+  }
+
+  void scheduler_loop() {
+    cudaSetDevice(o.device);
+    for (;;) {
+      // admit prepared jobs that fit
+      while ((int)active.size() < o.max_active) {
+        std::shared_ptr<Job> j;
+        {
+          std::lock_guard<std::mutex> lk(mtx);
+          if (stop || ready_q.empty()) break;
+          j = ready_q.front();
+          if (in_use + j->est_bytes > budget && !active.empty()) break;
+          ready_q.pop_front();
+        }
+        try {
+          volume_build_device(j->vol.get(), j->desc.covariance, j->desc.covfun, o.device);
+          auto cs = std::make_unique<Chainset>();
+          chainset_build(cs.get(), j->vol.get(), j->C, &j->opts);
+          j->bytes = j->vol->bytes + cs->bytes;
+          j->cs = std::move(cs);
+          j->iters_total = j->opts.burnin + (j->opts.thin == 0 ? 1 : j->opts.thin) * j->opts.nsave;
+        } catch (const Error& e) {
+          j->cs.reset();
+          j->vol.reset();
+          std::lock_guard<std::mutex> lk(mtx);
+          fail(j, e.code, e.what());
+          continue;
+        }
+        std::lock_guard<std::mutex> lk(mtx);
+        j->state = DR_JOB_RUNNING;
+        j->t_admit = now();
+        in_use += j->bytes;
+        peak_bytes = std::max(peak_bytes, in_use);
+        active.push_back(j);
+        peak_running = std::max(peak_running, (int)active.size());
+      }
+      // advance every resident job by one round, finalise finished ones
+      bool launched = false, waiting = false;
+      for (auto& j : active) {
+        try {
+          if (j->in_flight) {
+            const cudaError_t q = cudaEventQuery(j->cs->done_event);
+            if (q == cudaErrorNotReady) {
+              waiting = true;
+              continue;
+            }
+            if (q != cudaSuccess) throw Error(DR_ERR_CUDA, cudaGetErrorString(q));
+            j->in_flight = false;
+          }
+          if (j->iters_launched < j->iters_total) {
+            const int n = std::min(o.iterations_per_round, j->iters_total - j->iters_launched);
+            launch_iterations(j->cs.get(), n);
+            j->iters_launched += n;
+            j->in_flight = true;
+            launched = true;
+          } else {
+            const int64_t b = j->bytes;
+            finalize(j);
+            std::lock_guard<std::mutex> lk(mtx);
+            j->state = DR_JOB_DONE;
+            j->t_finish = now();
+            in_use -= b;
+            n_done++;
+            grads_done += j->grads;
+            last_finish = j->t_finish;
+            cv_done.notify_all();
+          }
+        } catch (const Error& e) {
+          const int64_t b = j->bytes;
+          j->cs.reset();
+          j->vol.reset();
+          std::lock_guard<std::mutex> lk(mtx);
+          in_use -= b;
+          fail(j, e.code, e.what());
+        }
+      }
+      active.erase(std::remove_if(active.begin(), active.end(),
+                                  [](const std::shared_ptr<Job>& j) {
+                                    return j->state == DR_JOB_DONE || j->state == DR_JOB_FAILED;
+                                  }),
+                   active.end());
+      std::unique_lock<std::mutex> lk(mtx);
+      launches = g_launches;
+      if (stop) break;
+      if (!launched) {
+        if (waiting)
+          cv_work.wait_for(lk, std::chrono::microseconds(50));
+        else if (ready_q.empty())
+          cv_work.wait_for(lk, std::chrono::milliseconds(2));
+      }
+    }
+    // shutdown: wait for in-flight work, release device objects
+    for (auto& j : active) {
+      if (j->cs) cudaStreamSynchronize(j->cs->stream);
+      j->cs.reset();
+      j->vol.reset();
+    }
+    active.clear();
+  }
+};
+
+}  // namespace drb
+
+struct dr_server : Server {};
+
+extern "C" {
+
+int dr_server_create(const dr_server_opts* opts, dr_server** out) {
+  API_BEGIN
+  if (!opts || !out) throw Error(DR_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  device_tables(opts->device);
+  CK(cudaSetDevice(opts->device));
+  auto* sv = new dr_server();
+  sv->o = *opts;
+  if (sv->o.max_active <= 0) sv->o.max_active = 64;
+  if (sv->o.iterations_per_round <= 0) sv->o.iterations_per_round = 8;
+  if (sv->o.host_threads <= 0) sv->o.host_threads = 4;
+  {
+    // Keep freed device memory in the pool between jobs instead of returning it at every synchronisation.
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, opts->device));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  if (sv->o.hbm_budget_bytes > 0) {
+    sv->budget = sv->o.hbm_budget_bytes;
+  } else {
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    sv->budget = (int64_t)(0.8 * (double)fr);
+  }
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int per = std::max(1, hw / sv->o.host_threads);
+  for (int i = 0; i < sv->o.host_threads; i++) sv->workers.emplace_back([sv, per] { sv->worker_loop(per); });
+  sv->sched = std::thread([sv] { sv->scheduler_loop(); });
+  *out = sv;
+  API_END
+}
+
+void dr_server_destroy(dr_server* sv) {
+  if (!sv) return;
+  {
+    std::lock_guard<std::mutex> lk(sv->mtx);
+    sv->stop = true;
+  }
+  sv->cv_work.notify_all();
+  for (auto& t : sv->workers) t.join();
+  if (sv->sched.joinable()) sv->sched.join();
+  delete sv;
+}
+
+int dr_server_submit(dr_server* sv, const dr_volume_desc* d, const dr_hmc_opts* opts, int n_chains, uint64_t* job_id) {
+  API_BEGIN
+  if (!sv || !d || !opts || !job_id || !d->highres || !d->qform_hr) throw Error(DR_ERR_INVALID, "NULL argument");
+  if (n_chains <= 0 || n_chains > 256) throw Error(DR_ERR_UNSUPPORTED, "n_chains must be in [1, 256]");
+  if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0) throw Error(DR_ERR_INVALID, "bad high-res grid");
+  auto j = std::make_shared<Job>();
+  const size_t nh = (size_t)d->nx * d->ny * d->nz;
+  j->hr.assign(d->highres, d->highres + nh);
+  if (d->hmask) j->hm.assign(d->hmask, d->hmask + nh);
+  if (d->omask) j->om.assign(d->omask, d->omask + nh);
+  std::memcpy(j->qh, d->qform_hr, sizeof(j->qh));
+  j->desc = *d;
+  j->desc.highres = j->hr.data();
+  j->desc.hmask = d->hmask ? j->hm.data() : nullptr;
+  j->desc.omask = d->omask ? j->om.data() : nullptr;
+  j->desc.qform_hr = j->qh;
+  if (d->stdres) {
+    if (!d->qform_sr || d->sx <= 0 || d->sy <= 0 || d->sz <= 0) throw Error(DR_ERR_INVALID, "bad std-res grid");
+    const size_t ns = (size_t)d->sx * d->sy * d->sz;
+    j->sr.assign(d->stdres, d->stdres + ns);
+    if (d->smask) j->sm.assign(d->smask, d->smask + ns);
+    std::memcpy(j->qs, d->qform_sr, sizeof(j->qs));
+    j->desc.stdres = j->sr.data();
+    j->desc.smask = d->smask ? j->sm.data() : nullptr;
+    j->desc.qform_sr = j->qs;
+  }
+  j->desc.device = sv->o.device;
+  j->opts = *opts;
+  if (j->opts.leapfrog <= 0 || j->opts.burnin < 0 || j->opts.nsave < 0 || j->opts.thin < 0 ||
+      !(j->opts.mhtarget > 0 && j->opts.mhtarget < 1))
+    throw Error(DR_ERR_DOMAIN, "HMCParameters: invalid settings");
+  j->C = n_chains;
+  std::lock_guard<std::mutex> lk(sv->mtx);
+  j->id = sv->next_id++;
+  j->t_submit = sv->now();
+  sv->jobs[j->id] = j;
+  sv->setup_q.push_back(j);
+  sv->n_submitted++;
+  *job_id = j->id;
+  sv->cv_work.notify_all();
+  API_END
+}
+
+static std::shared_ptr<Job> find_job(dr_server* sv, uint64_t id) {
+  auto it = sv->jobs.find(id);
+  if (it == sv->jobs.end()) throw Error(DR_ERR_INVALID, "unknown job id");
+  return it->second;
+}
+
+int dr_server_status(dr_server* sv, uint64_t job_id, dr_job_status* out) {
+  API_BEGIN
+  if (!sv || !out) throw Error(DR_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(sv->mtx);
+  auto j = find_job(sv, job_id);
+  std::memset(out, 0, sizeof(*out));
+  out->state = j->state;
+  out->error = j->error;
+  out->submit_s = j->t_submit;
+  out->admit_s = j->t_admit;
+  out->finish_s = j->t_finish;
+  out->grad_evals = j->grads;
+  out->mh_rate = j->mh;
+  out->n_output = j->n_output;
+  out->device_bytes = j->bytes;
+  API_END
+}
+
+int dr_server_result(dr_server* sv, uint64_t job_id, float* mean, float* var, float* activation) {
+  API_BEGIN
+  if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(sv->mtx);
+  auto j = find_job(sv, job_id);
+  if (j->state == DR_JOB_FAILED) throw Error(j->error ? j->error : DR_ERR_STATE, "job failed: " + j->msg);
+  if (j->state != DR_JOB_DONE) throw Error(DR_ERR_STATE, "job not finished");
+  if (mean) std::memcpy(mean, j->mean.data(), sizeof(float) * j->mean.size());
+  if (var) std::memcpy(var, j->var.data(), sizeof(float) * j->var.size());
+  if (activation) std::memcpy(activation, j->act.data(), sizeof(float) * j->act.size());
+  API_END
+}
+
+int dr_server_wait(dr_server* sv, uint64_t job_id, double timeout_s) {
+  API_BEGIN
+  if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(sv->mtx);
+  auto j = find_job(sv, job_id);
+  const bool ok = sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    return j->state == DR_JOB_DONE || j->state == DR_JOB_FAILED;
+  });
+  if (!ok) throw Error(DR_ERR_TIMEOUT, "job still running");
+  if (j->state == DR_JOB_FAILED) throw Error(j->error ? j->error : DR_ERR_STATE, "job failed: " + j->msg);
+  API_END
+}
+
+int dr_server_drain(dr_server* sv, double timeout_s) {
+  API_BEGIN
+  if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(sv->mtx);
+  const bool ok = sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                       [&] { return sv->n_done + sv->n_failed >= sv->n_submitted; });
+  if (!ok) throw Error(DR_ERR_TIMEOUT, "jobs still running");
+  API_END
+}
+
+int dr_server_stats_get(dr_server* sv, dr_server_stats* out) {
+  API_BEGIN
+  if (!sv || !out) throw Error(DR_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(sv->mtx);
+  out->submitted = sv->n_submitted;
+  out->done = sv->n_done;
+  out->failed = sv->n_failed;
+  out->running = sv->n_submitted - sv->n_done - sv->n_failed;
+  out->grad_evals = sv->grads_done;
+  out->peak_device_bytes = sv->peak_bytes;
+  out->peak_running = sv->peak_running;
+  out->busy_s = sv->last_finish;
+  out->kernel_launches = sv->launches;
+  API_END
+}
+
+int dr_server_forget(dr_server* sv, uint64_t job_id) {
+  API_BEGIN
+  if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(sv->mtx);
+  auto j = find_job(sv, job_id);
+  if (j->state != DR_JOB_DONE && j->state != DR_JOB_FAILED) throw Error(DR_ERR_STATE, "job not finished");
+  sv->jobs.erase(job_id);
+  API_END
+}
 
 }  // extern "C"
 

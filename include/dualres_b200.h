@@ -96,6 +96,8 @@ int dr_volume_lambda_get(const dr_volume* v, double* lambda_re);
 int dr_volume_indices_get(const dr_volume* v, int* data_idx, int* out_idx);
 /* Observed data vectors; MultiResData::Yh()/Ys() (MultiResData.h:139-150). */
 int dr_volume_data_get(const dr_volume* v, float* Yh, float* Ys);
+/* Releases the handle.  Device memory is freed now, or when the last chain set
+ * created on the volume is destroyed. */
 void dr_volume_destroy(dr_volume* v);
 
 /* HMC settings: HMCParameters<T>(burnin, nsave, thin, L, eps0, mhtarget)
@@ -185,6 +187,68 @@ int dr_leapfrog_fixed(dr_chainset* cs, int chain, const float* mu0, const float*
  * context) race, so serialise them.  The call runs on the legacy default
  * stream and returns when the result is on the host. */
 int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_device, float s_hr, float s_sr, double* out);
+
+/* ---- serving: continuous batching of denoising jobs --------------------- */
+/* A request loop that the reference does not have (it fits one volume per
+ * process).  Each job is one dualgpmf fit (volume + n_chains chains).  Host
+ * set-up (masks, indices, kriging) runs on worker threads; a scheduler thread
+ * admits prepared jobs while their device footprint fits the HBM budget, keeps
+ * each job's chain state resident, and advances every admitted job a few
+ * iterations per round on its own stream, so jobs that arrive while others run
+ * overlap with them on the device.  Results are identical to running the job
+ * alone: every job's random streams depend only on its seed. */
+typedef struct dr_server dr_server;
+
+typedef struct {
+  int device;
+  int64_t hbm_budget_bytes;    /* admission budget; <= 0: 80 % of the device memory free at creation */
+  int max_active;              /* jobs resident on the device at once; <= 0: 64 */
+  int iterations_per_round;    /* iterations each admitted job advances per round; <= 0: 8 */
+  int host_threads;            /* set-up workers; <= 0: 4 */
+} dr_server_opts;
+
+#define DR_JOB_QUEUED 0   /* waiting for host set-up */
+#define DR_JOB_READY 1    /* set up on the host, waiting for device memory */
+#define DR_JOB_RUNNING 2  /* resident on the device */
+#define DR_JOB_DONE 3
+#define DR_JOB_FAILED 4
+
+typedef struct {
+  int state;                   /* DR_JOB_* */
+  int error;                   /* DR_ERR_* when failed */
+  double submit_s;             /* server clock (s) at submission */
+  double admit_s;              /* ... when admitted to the device */
+  double finish_s;             /* ... when the summary was read back */
+  int64_t grad_evals;          /* sum over chains of L + 1 per iteration */
+  float mh_rate;               /* mean over chains */
+  int n_output;                /* output voxels */
+  int64_t device_bytes;        /* footprint while resident */
+} dr_job_status;
+
+typedef struct {
+  int64_t submitted, done, failed, running;
+  int64_t grad_evals;          /* over finished jobs */
+  int64_t peak_device_bytes;   /* largest resident footprint */
+  int peak_running;            /* largest number of resident jobs */
+  double busy_s;               /* server clock of the last finish */
+  int64_t kernel_launches;     /* kernels the scheduler enqueued (graph nodes counted) */
+} dr_server_stats;
+
+int dr_server_create(const dr_server_opts* opts, dr_server** out);
+/* Copies the images; returns immediately with the job id. */
+int dr_server_submit(dr_server* sv, const dr_volume_desc* desc, const dr_hmc_opts* opts, int n_chains,
+                     uint64_t* job_id);
+int dr_server_status(dr_server* sv, uint64_t job_id, dr_job_status* out);
+/* Posterior mean / variance / activation of a finished job (n_output each, any may be NULL). */
+int dr_server_result(dr_server* sv, uint64_t job_id, float* mean, float* var, float* activation);
+/* Waits (host side) until the job finished or failed, or timeout_s passed (DR_ERR_TIMEOUT). */
+int dr_server_wait(dr_server* sv, uint64_t job_id, double timeout_s);
+/* Waits until every submitted job finished or failed. */
+int dr_server_drain(dr_server* sv, double timeout_s);
+int dr_server_stats_get(dr_server* sv, dr_server_stats* out);
+/* Releases a finished job's host record (results are no longer available). */
+int dr_server_forget(dr_server* sv, uint64_t job_id);
+void dr_server_destroy(dr_server* sv);
 
 /* ---- host-side set-up --------------------------------------------------- */
 /* The kriging matrix of get_sparse_kriging_matrix_data (kriging_matrix.h:
