@@ -153,6 +153,11 @@ def _declare(L):
     L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
+    L.dr_mce_offsets.argtypes = [vp, C.c_int, _ip]
+    L.dr_mce_summary.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, vp]
+    L.dr_fit_rbf_parameters.argtypes = [vp, vp, vp, C.c_int, vp]
+    L.dr_estimate_covariance.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp]
+    L.dr_sample_records_get.argtypes = [vp, C.c_int, vp, C.c_int, _ip]
     L.dr_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
     L.dr_server_submit.argtypes = [vp, C.POINTER(VolumeDesc), C.POINTER(HmcOpts), C.c_int, C.POINTER(C.c_uint64)]
     L.dr_server_status.argtypes = [vp, C.c_uint64, C.POINTER(JobStatus)]
@@ -566,3 +571,57 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ covariance estimation
+def mce_offsets():
+    """perturbation_matrix_3d offsets, (n, 3) int32."""
+    L = lib()
+    n = C.c_int(0)
+    check(L.dr_mce_offsets(None, 0, C.byref(n)))
+    P = np.zeros(3 * n.value, np.int32)
+    check(L.dr_mce_offsets(_ptr(P), n.value, C.byref(n)))
+    return P.reshape(-1, 3)
+
+
+def mce_summary(img, qform, device=0, with_sums=False):
+    """compute_mce_summary_data on the GPU: distance, covariance and pair count per offset."""
+    L = lib()
+    a = _f32(img)
+    nz, ny, nx = a.shape
+    n = C.c_int(0)
+    check(L.dr_mce_offsets(None, 0, C.byref(n)))
+    n = n.value
+    dist, cov = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    npairs = np.zeros(n, np.int32)
+    sums = np.zeros(3 * n) if with_sums else None
+    check(L.dr_mce_summary(_ptr(a), nx, ny, nz, _ptr(_f32(qform)), device, _ptr(dist), _ptr(cov), _ptr(npairs),
+                           _ptr(sums)))
+    out = dict(distance=dist, covariance=cov, npairs=npairs)
+    if with_sums:
+        out["sums"] = sums.reshape(n, 3)
+    return out
+
+
+def fit_rbf_parameters(distance, covariance, npairs, theta0=(1.0, 0.6, 1.5)):
+    """compute_rbf_parameters (host): COBYLA fit of the RBF model to an MCE summary."""
+    th = np.asarray(theta0, np.float64).copy()
+    d, c = _f32(distance), _f32(covariance)
+    n = np.ascontiguousarray(npairs, np.int32)
+    check(lib().dr_fit_rbf_parameters(_ptr(d), _ptr(c), _ptr(n), len(d), _ptr(th)))
+    return tuple(float(x) for x in th)
+
+
+def estimate_covariance(img, qform, theta0=(1.0, 0.6, 1.5), device=0):
+    """compute_covar_parameters_if_needed: MCE summary on the GPU, then the COBYLA fit."""
+    th = np.asarray(theta0, np.float64).copy()
+    a = _f32(img)
+    nz, ny, nx = a.shape
+    check(lib().dr_estimate_covariance(_ptr(a), nx, ny, nz, _ptr(_f32(qform)), device, _ptr(th)))
+    return tuple(float(x) for x in th)
+
+
+def cli_path():
+    """The dualgpmf command line (built next to the library)."""
+    _build.build()
+    return _build.CLI

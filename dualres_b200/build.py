@@ -16,8 +16,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libdualres_b200.so")
-SOURCES = ["api.cu", "host_setup.cpp"]
-DEPS = ["api.cu", "kernels.cu", "common.cuh", "fft.cuh", "drb.h", "host_setup.cpp", "host_setup.h"]
+SOURCES = ["api.cu", "host_setup.cpp", "estimate.cpp"]
+DEPS = ["api.cu", "kernels.cu", "common.cuh", "fft.cuh", "tma.cuh", "mce.cuh", "drb.h", "host_setup.cpp",
+        "host_setup.h", "estimate.cpp", "estimate.h"]
+CLI = os.path.join(LIBDIR, "dualgpmf")
+CLI_SOURCES = ["dualgpmf.cpp", "nifti.cpp"]
+CLI_DEPS = CLI_SOURCES + ["nifti.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,8 +41,36 @@ def _stale():
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
+def _cli_stale():
+    if not os.path.exists(CLI):
+        return True
+    t = os.path.getmtime(CLI)
+    inc = os.path.join(HERE, "..", "include", "dualres_b200.h")
+    deps = [os.path.join(CSRC, d) for d in CLI_DEPS] + [inc, LIB]
+    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+
+
+def build_cli(force=False, verbose=False):
+    """The dualgpmf command line, linked against the library (found next to it at run time)."""
+    if not force and not _cli_stale():
+        return CLI
+    gxx = shutil.which("g++") or "g++"
+    cmd = [gxx, "-std=c++17", "-O2", "-fopenmp", "-o", CLI + ".tmp",
+           *[os.path.join(CSRC, s) for s in CLI_SOURCES], "-L" + LIBDIR, "-ldualres_b200", "-lz",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=not verbose, text=True)
+    if res.returncode != 0:
+        sys.stderr.write((res.stdout or "") + (res.stderr or ""))
+        raise RuntimeError("g++ failed (dualgpmf)")
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 def build(force=False, verbose=False):
     if not force and not _stale():
+        build_cli(force, verbose)
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     gxx = shutil.which("g++") or "g++"
@@ -54,6 +86,7 @@ def build(force=False, verbose=False):
         sys.stderr.write((res.stdout or "") + (res.stderr or ""))
         raise RuntimeError("nvcc failed")
     os.replace(LIB + ".tmp", LIB)
+    build_cli(True, verbose)
     return LIB
 
 

@@ -22,6 +22,8 @@
 #include "../../include/dualres_b200.h"
 #include "host_setup.h"
 #include "kernels.cu"
+#include "mce.cuh"
+#include "estimate.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -633,6 +635,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   ch.s2 = S->alloc<double>((size_t)std::max(v.n_o, 1) * C);
   ch.sa = S->alloc<double>((size_t)std::max(v.n_o, 1) * C);
   ch.samples = o->store_samples ? S->alloc<float>((size_t)std::max(o->nsave, 1) * std::max(v.n_o, 1) * C, false) : nullptr;
+  ch.save_rec = o->store_samples ? S->alloc<double>((size_t)std::max(o->nsave, 1) * C * 3, true) : nullptr;
   ch.seed = o->seed;
   ch.chain0 = 0;
   ch.err = S->alloc<int>(1);
@@ -836,6 +839,13 @@ struct dr_chainset : Chainset {};
   }                                                                 \
   return DR_OK;
 
+// Calls another entry point and rethrows its failure with its message.
+#define CK_API(call)                                   \
+  do {                                                 \
+    const int rc_ = (call);                            \
+    if (rc_ != DR_OK) throw Error(rc_, std::string(g_err)); \
+  } while (0)
+
 extern "C" {
 
 const char* dr_last_error(void) { return g_err.c_str(); }
@@ -1004,6 +1014,21 @@ int dr_samples_get(dr_chainset* s, int chain, float* samples, int max_saved, int
     CK(cudaMemcpy(buf.data(), s->dc.samples + i * per, sizeof(float) * per, cudaMemcpyDeviceToHost));
     for (int o = 0; o < v.n_o; o++) samples[(size_t)i * v.n_o + o] = buf[(size_t)o * s->C + chain];
   }
+  API_END
+}
+
+int dr_sample_records_get(dr_chainset* s, int chain, double* rec, int max_saved, int* n_saved) {
+  API_BEGIN
+  if (!s || !rec || chain < 0 || chain >= s->C || !n_saved) throw Error(DR_ERR_INVALID, "bad argument");
+  if (!s->dc.save_rec) throw Error(DR_ERR_STATE, "samples were not stored (store_samples = 0)");
+  std::vector<ChainState> st;
+  read_states(s, &st);
+  const int ns = std::min(std::min(st[chain].saved, max_saved), std::max(s->opts.nsave, 1));
+  *n_saved = ns;
+  std::vector<double> buf((size_t)std::max(ns, 1) * s->C * 3);
+  if (ns > 0) CK(cudaMemcpy(buf.data(), s->dc.save_rec, sizeof(double) * ns * s->C * 3, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < ns; i++)
+    for (int k = 0; k < 3; k++) rec[(size_t)i * 3 + k] = buf[((size_t)i * s->C + chain) * 3 + k];
   API_END
 }
 
@@ -1323,7 +1348,7 @@ static int64_t estimate_bytes(const HostVolume& hv, int C, const dr_hmc_opts& o)
   double vol = box * 8 + (nh + no) * 4 + (nh + ns) * 4 + (ns + nh + 2) * 4 + nnz * 16 + N * 12 + N * 16;
   double cs = C * (3 * N * 8 + t2 * 8 + (hv.E[0] == hv.E[1] ? 0.0 : (double)hv.E[2] * hv.E[1] * hv.box[0] * 8)) +
               C * (2 * (nh + no) * 4 + (nh + ns) * 4 + no * 24) + N * 8 + (double)C * 9 * 2048 * 8;
-  if (o.store_samples) cs += (double)std::max(o.nsave, 1) * no * C * 4;
+  if (o.store_samples) cs += (double)std::max(o.nsave, 1) * (no * 4 + 24) * C;
   return (int64_t)(1.10 * (vol + cs)) + (16 << 20);
 }
 
@@ -1692,6 +1717,97 @@ int dr_server_forget(dr_server* sv, uint64_t job_id) {
   auto j = find_job(sv, job_id);
   if (j->state != DR_JOB_DONE && j->state != DR_JOB_FAILED) throw Error(DR_ERR_STATE, "job not finished");
   sv->jobs.erase(job_id);
+  API_END
+}
+
+}  // extern "C"
+
+// ==================================================================== covariance estimation
+extern "C" {
+
+int dr_mce_offsets(int* offsets, int max_out, int* n) {
+  API_BEGIN
+  if (!n) throw Error(DR_ERR_INVALID, "NULL argument");
+  const std::vector<int> P = mce_offsets();
+  *n = (int)(P.size() / 3);
+  if (offsets) std::memcpy(offsets, P.data(), sizeof(int) * 3 * std::min(*n, std::max(max_out, 0)));
+  API_END
+}
+
+int dr_mce_summary(const float* img, int nx, int ny, int nz, const float* qform, int device, float* distance,
+                   float* covariance, int* npairs, double* sums) {
+  API_BEGIN
+  if (!img || !qform || !distance || !covariance || !npairs) throw Error(DR_ERR_INVALID, "NULL argument");
+  if (nx <= 0 || ny <= 0 || nz <= 0) throw Error(DR_ERR_INVALID, "bad grid");
+  const std::vector<int> P = mce_offsets();
+  const int n_off = (int)(P.size() / 3);
+  const std::vector<float> d = mce_distances(P, qform);
+  std::memcpy(distance, d.data(), sizeof(float) * n_off);
+  device_tables(device);
+  CK(cudaSetDevice(device));
+  const long long nvox = (long long)nx * ny * nz;
+  const int rows = ny * nz;
+  int n_slabs = std::max(1, std::min(32, rows / 256));
+  const int rows_per_slab = cdiv_i(rows, n_slabs);
+  n_slabs = cdiv_i(rows, rows_per_slab);
+  cudaStream_t st = nullptr;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  std::vector<void*> bufs;
+  auto dalloc = [&](size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    bufs.push_back(p);
+    return p;
+  };
+  try {
+    float* d_img = (float*)dalloc(sizeof(float) * nvox);
+    int* d_P = (int*)dalloc(sizeof(int) * P.size());
+    MceSums* d_part = (MceSums*)dalloc(sizeof(MceSums) * (size_t)n_slabs * n_off);
+    float* d_cov = (float*)dalloc(sizeof(float) * n_off);
+    int* d_np = (int*)dalloc(sizeof(int) * n_off);
+    double* d_sums = sums ? (double*)dalloc(sizeof(double) * 3 * n_off) : nullptr;
+    CK(cudaMemcpyAsync(d_img, img, sizeof(float) * nvox, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_P, P.data(), sizeof(int) * P.size(), cudaMemcpyHostToDevice, st));
+    const dim3 grid(n_slabs, cdiv_i(n_off, MCE_OFFSETS_PER_CTA));
+    k_mce_partial<<<grid, MCE_THREADS, 0, st>>>(d_img, nx, ny, nz, d_P, n_off, rows_per_slab, d_part);
+    CK_LAUNCH();
+    k_mce_finish<<<cdiv_i(n_off, 256), 256, 0, st>>>(d_part, n_slabs, n_off, d_cov, d_np, d_sums);
+    CK_LAUNCH();
+    CK(cudaMemcpyAsync(covariance, d_cov, sizeof(float) * n_off, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(npairs, d_np, sizeof(int) * n_off, cudaMemcpyDeviceToHost, st));
+    if (sums) CK(cudaMemcpyAsync(sums, d_sums, sizeof(double) * 3 * n_off, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  } catch (...) {
+    for (void* p : bufs) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    cudaGetLastError();
+    throw;
+  }
+  for (void* p : bufs) cudaFreeAsync(p, st);
+  CK(cudaStreamSynchronize(st));
+  cudaStreamDestroy(st);
+  API_END
+}
+
+int dr_fit_rbf_parameters(const float* distance, const float* covariance, const int* npairs, int n, double* theta) {
+  API_BEGIN
+  if (!distance || !covariance || !npairs || !theta) throw Error(DR_ERR_INVALID, "NULL argument");
+  std::string err;
+  if (fit_rbf_parameters(distance, covariance, npairs, n, theta, &err) != 0) throw Error(DR_ERR_DOMAIN, err);
+  API_END
+}
+
+int dr_estimate_covariance(const float* img, int nx, int ny, int nz, const float* qform, int device, double* theta) {
+  API_BEGIN
+  if (!theta) throw Error(DR_ERR_INVALID, "NULL argument");
+  int n = 0;
+  CK_API(dr_mce_offsets(nullptr, 0, &n));
+  std::vector<float> dist(n), cov(n);
+  std::vector<int> np(n);
+  CK_API(dr_mce_summary(img, nx, ny, nz, qform, device, dist.data(), cov.data(), np.data(), nullptr));
+  CK_API(dr_fit_rbf_parameters(dist.data(), cov.data(), np.data(), n, theta));
   API_END
 }
 

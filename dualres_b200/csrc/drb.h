@@ -90,6 +90,7 @@ struct DevChains {
   double* s2;               // [n_o][Cp] sum mu^2
   double* sa;               // [n_o][Cp] sum |mu| / max|mu|
   float* samples;           // [nsave][n_o][Cp] or null
+  double* save_rec;         // [nsave][C][3]: sigma_h, sigma_s, log likelihood per saved iteration, or null
   uint64_t seed;
   int chain0;               // global id of chain 0 (RNG key component)
   int* err;                 // device error word: bounded waits that gave up

@@ -738,9 +738,17 @@ __global__ void __launch_bounds__(256) k_accept(DevVolume v, DevChains ch) {
   if (hmc_save_iteration(st)) {
     st.save_now = 1;
     st.saved += 1;
-    st.ll_sum += -0.5 * ((double)st.sh * Rh + (v.n_s > 0 ? (double)st.ss * Rs : 0.0));
+    const double ll = -0.5 * ((double)st.sh * Rh + (v.n_s > 0 ? (double)st.ss * Rs : 0.0));
+    st.ll_sum += ll;
     st.sigh_sum += sqrt(1.0 / (double)st.sh);
     st.sigs_sum += v.n_s > 0 ? sqrt(1.0 / (double)st.ss) : 0.0;
+    if (ch.save_rec != nullptr && st.saved <= st.n_save) {
+      // MultiResParameters::sigma (MultiResParameters.h:613-619) is sqrt(1 / sigma^-2) in float
+      double* r = ch.save_rec + ((long long)(st.saved - 1) * ch.C + c) * 3;
+      r[0] = (double)sqrtf(1.0f / st.sh);
+      r[1] = v.n_s > 0 ? (double)sqrtf(1.0f / st.ss) : 0.0;
+      r[2] = ll;
+    }
     if (st.saved >= st.n_save) st.done = 1;
   }
 }

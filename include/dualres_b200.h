@@ -148,6 +148,10 @@ int dr_summary_get(dr_chainset* cs, int chain, float* mean, float* var, float* a
 /* Saved samples of one chain at the output voxels: n_saved x n_output floats
  * (requires store_samples). */
 int dr_samples_get(dr_chainset* cs, int chain, float* samples, int max_saved, int* n_saved);
+/* Per saved iteration of one chain: sigma_hr, sigma_sr (0 in single-resolution
+ * mode) and the log likelihood, n_saved x 3 doubles (requires store_samples);
+ * the columns after mu in the --samples stream (gaussian_process_model.h:149-163). */
+int dr_sample_records_get(dr_chainset* cs, int chain, double* rec, int max_saved, int* n_saved);
 void dr_chainset_destroy(dr_chainset* cs);
 
 /* ---- fixed-input evaluation (MultiResParameters public API) ------------- */
@@ -249,6 +253,26 @@ int dr_server_stats_get(dr_server* sv, dr_server_stats* out);
 /* Releases a finished job's host record (results are no longer available). */
 int dr_server_forget(dr_server* sv, uint64_t job_id);
 void dr_server_destroy(dr_server* sv);
+
+/* ---- covariance estimation (dualgpmf without --covariance) -------------- */
+/* Lattice offsets of the minimum-contrast summary, perturbation_matrix_3d
+ * (perturbation_matrix.h:62-109): *n = 25348; offsets (3 ints each, at most
+ * max_out) may be NULL. */
+int dr_mce_offsets(int* offsets, int max_out, int* n);
+/* compute_mce_summary_data (estimate_kernel_parameters.h:50-115) on the GPU:
+ * for every offset p, the distance |Q p| (mm), the covariance of the pairs of
+ * non-zero, non-NaN voxels (x, x + p) and their count.  img is nx*ny*nz
+ * floats, x fastest; qform row-major 4x4.  sums (3 doubles per offset: sum xy,
+ * sum x, sum y) may be NULL. */
+int dr_mce_summary(const float* img, int nx, int ny, int nz, const float* qform, int device, float* distance,
+                   float* covariance, int* npairs, double* sums);
+/* compute_rbf_parameters (estimate_kernel_parameters.h:267-390) with the
+ * defaults dualgpm.cpp uses: bounded least squares of the RBF model to the
+ * summary, bandwidth <= exponent, minimised by COBYLA.  theta: start values in
+ * (dualgpm.cpp starts from 1, 0.6, 1.5), estimate out.  Host only. */
+int dr_fit_rbf_parameters(const float* distance, const float* covariance, const int* npairs, int n, double* theta);
+/* Both steps: compute_covar_parameters_if_needed (src/dualgpm.cpp:375-404). */
+int dr_estimate_covariance(const float* img, int nx, int ny, int nz, const float* qform, int device, double* theta);
 
 /* ---- host-side set-up --------------------------------------------------- */
 /* The kriging matrix of get_sparse_kriging_matrix_data (kriging_matrix.h:

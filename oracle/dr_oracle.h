@@ -78,6 +78,18 @@ int64_t orc_kriging_build(const float* hr, int nx, int ny, int nz, const float* 
 /* Covariance functions (kernels.inl:8-15, 59-74). covfun 0 = rbf, 1 = rational quadratic. */
 double orc_cov(int covfun, double d, const double* theta);
 
+/* Minimum contrast estimation summary (estimate_kernel_parameters.h:50-101):
+ * the lattice offsets of perturbation_matrix_3d (perturbation_matrix.h:19-109),
+ * in its order, deduplicated keeping first occurrences; returns the count
+ * (25348) and fills P (3 ints per offset) when P is not NULL. */
+int orc_mce_offsets(int* P, int max_out);
+/* For every offset: distance |Q_3x3 p| (float), the covariance of the pairs of
+ * non-zero, non-NaN voxels (x, x + p) inside the grid (double sums, stored as
+ * float) and the pair counts.  Also returns the raw double sums (3 per offset)
+ * when sums is not NULL. */
+int orc_mce_summary(const float* img, int nx, int ny, int nz, const float* Q, const int* P, int n_off,
+                    float* distance, float* covariance, int* npairs, double* sums);
+
 /* HMCParameters (HMCParameters.h:97-297), double state. */
 typedef struct {
   int warmup, eps_start_found, burnin, integrator_steps, iteration, n_save, thin;

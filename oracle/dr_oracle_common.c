@@ -531,3 +531,99 @@ void orc_hmc_update(orc_hmc* h, double mh_rate_in) {
   }
   h->iteration++;
 }
+
+
+/* ------------------------------------------------------------------ minimum contrast summary */
+/* perturbation_matrix_3d (perturbation_matrix.h:62-109): 14 unit directions
+ * (perturbations_3d_unit_directions, :19-38) times every (a, b, c) in
+ * {1..18}^3 with a fastest (perturbation_permutations_3d, :44-56), then the
+ * axis offsets 19..25, duplicates removed keeping the first. */
+int orc_mce_offsets(int* P, int max_out) {
+  static const int U[14][3] = {{0, 0, 0},  {1, 0, 0}, {0, 1, 0},  {0, 0, 1},  {1, 1, 0},  {1, 0, 1},   {-1, 1, 0},
+                               {1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {1, 1, 1},  {1, 1, -1}, {-1, 1, 1}, {-1, 1, -1}};
+  const int n = 18, extra = 25 - 18;
+  const int total = 14 * n * n * n + 3 * extra;
+  int* all = (int*)malloc(sizeof(int) * 3 * total);
+  int r = 0;
+  for (int c = 1; c <= n; c++)
+    for (int b = 1; b <= n; b++)
+      for (int a = 1; a <= n; a++)
+        for (int j = 0; j < 14; j++, r++) {
+          all[3 * r] = U[j][0] * a;
+          all[3 * r + 1] = U[j][1] * b;
+          all[3 * r + 2] = U[j][2] * c;
+        }
+  for (int i = 0; i < extra; i++)
+    for (int j = 0; j < 3; j++, r++) {
+      all[3 * r] = all[3 * r + 1] = all[3 * r + 2] = 0;
+      all[3 * r + j] = n + i + 1;
+    }
+  /* dedupe through a presence grid over [-25, 25]^3 */
+  const int W = 51;
+  unsigned char* seen = (unsigned char*)calloc(W * W * W, 1);
+  int u = 0;
+  for (int i = 0; i < total; i++) {
+    const int key = ((all[3 * i + 2] + 25) * W + (all[3 * i + 1] + 25)) * W + (all[3 * i] + 25);
+    if (seen[key]) continue;
+    seen[key] = 1;
+    if (P && u < max_out) {
+      P[3 * u] = all[3 * i];
+      P[3 * u + 1] = all[3 * i + 1];
+      P[3 * u + 2] = all[3 * i + 2];
+    }
+    u++;
+  }
+  free(seen);
+  free(all);
+  return u;
+}
+
+/* compute_mce_summary_data_impl (estimate_kernel_parameters.h:50-101). */
+int orc_mce_summary(const float* img, int nx, int ny, int nz, const float* Q, const int* P, int n_off,
+                    float* distance, float* covariance, int* npairs, double* sums) {
+  for (int o = 0; o < n_off; o++) {
+    /* (P with a zero 4th column) * Q^T, row norm, in float */
+    float s2 = 0.0f;
+    for (int r = 0; r < 4; r++) {
+      float t = 0.0f;
+      for (int c = 0; c < 3; c++) t += (float)P[3 * o + c] * Q[4 * r + c];
+      s2 += t * t;
+    }
+    distance[o] = sqrtf(s2);
+  }
+  const long long nxy = (long long)nx * ny;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int o = 0; o < n_off; o++) {
+    const int dx = P[3 * o], dy = P[3 * o + 1], dz = P[3 * o + 2];
+    double sxy = 0, sx = 0, sy = 0;
+    int n = 0;
+    for (int k = 0; k < nz; k++) {
+      const int k2 = k + dz;
+      if (k2 < 0 || k2 >= nz) continue;
+      for (int j = 0; j < ny; j++) {
+        const int j2 = j + dy;
+        if (j2 < 0 || j2 >= ny) continue;
+        const float* xr = img + k * nxy + (long long)j * nx;
+        const float* yr = img + k2 * nxy + (long long)j2 * nx;
+        for (int i = 0; i < nx; i++) {
+          const int i2 = i + dx;
+          if (i2 < 0 || i2 >= nx) continue;
+          const double x = xr[i], y = yr[i2];
+          if (isnan(x) || x == 0 || isnan(y) || y == 0) continue;
+          sxy += x * y;
+          sx += x;
+          sy += y;
+          n++;
+        }
+      }
+    }
+    npairs[o] = n;
+    covariance[o] = n > 1 ? (float)((sxy - sx * sy / n) / (n - 1)) : 0.0f;
+    if (sums) {
+      sums[3 * o] = sxy;
+      sums[3 * o + 1] = sx;
+      sums[3 * o + 2] = sy;
+    }
+  }
+  return 0;
+}

@@ -56,6 +56,11 @@ def _declare(L):
     L.orc_kriging_build.restype = C.c_int64
     L.orc_cov.argtypes = [C.c_int, C.c_double, _f64p]
     L.orc_cov.restype = C.c_double
+    L.orc_mce_offsets.argtypes = [C.c_void_p, C.c_int]
+    L.orc_mce_offsets.restype = C.c_int
+    L.orc_mce_summary.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_mce_summary.restype = C.c_int
     for sfx, rp, rt in (("_d", _f64p, C.c_double), ("_f", _f32p, C.c_float)):
         g = lambda n: getattr(L, n + sfx)
         g("orc_fft3d").argtypes = [rp, _i32p, C.c_int]
@@ -257,6 +262,32 @@ class Model:
 
     def run_iterations(self, iters, L, eps, seed):
         return int(self._f("orc_run_iterations")(self.h, iters, L, eps, seed))
+
+
+def mce_offsets():
+    """perturbation_matrix_3d offsets (n x 3, int32)."""
+    n = lib().orc_mce_offsets(None, 0)
+    P = np.zeros(3 * n, np.int32)
+    lib().orc_mce_offsets(P.ctypes.data_as(C.c_void_p), n)
+    return P.reshape(n, 3)
+
+
+def mce_summary(img, Q, P=None):
+    """compute_mce_summary_data: distance, covariance, npairs and the raw double sums per offset."""
+    if P is None:
+        P = mce_offsets()
+    nz, ny, nx = img.shape
+    n = len(P)
+    dist = np.zeros(n, np.float32)
+    cov = np.zeros(n, np.float32)
+    npairs = np.zeros(n, np.int32)
+    sums = np.zeros(3 * n)
+    P = np.ascontiguousarray(P, np.int32)
+    lib().orc_mce_summary(_img(img), nx, ny, nz, np.ascontiguousarray(Q, np.float32).ravel(),
+                          P.ctypes.data_as(C.c_void_p), n, dist.ctypes.data_as(C.c_void_p),
+                          cov.ctypes.data_as(C.c_void_p), npairs.ctypes.data_as(C.c_void_p),
+                          sums.ctypes.data_as(C.c_void_p))
+    return dict(distance=dist, covariance=cov, npairs=npairs, sums=sums.reshape(n, 3))
 
 
 def set_threads(n):
