@@ -516,16 +516,22 @@ def run_reference(args, dist):
 
 
 def profile_kernel(args):
+    """Set up the workload, run --warmup iterations, then launch kernel K four times inside an NVTX range
+    named "profile" (ncu --nvtx --nvtx-include "profile/" captures exactly those launches)."""
+    import torch
+
     import dualres_b200 as d
     wl = WORKLOADS[args.workload]
     hmc = d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"], leapfrog=wl["leapfrog"],
                           seed=args.seed)
     data = d.MultiResData.from_volume(make_volume(wl["vol"]))
     chains = d.MultiResParameters(data, hmc, wl["chains"])
-    chains.update(args.warmup)
+    chains.update(max(args.warmup, 3))
+    torch.cuda.nvtx.range_push("profile")
     ms, b = d.api.time_kernel(chains, args.profile_kernel, step=1, reps=3)
+    torch.cuda.nvtx.range_pop()
     print(json.dumps({"kernel": d.api.KERNEL_NAMES[args.profile_kernel], "ms": ms, "algorithmic_bytes": b,
-                      "steps": [s["integrator_steps"] for s in chains.stats()][:4]}))
+                      "chains": wl["chains"], "steps": [s["integrator_steps"] for s in chains.stats()][:4]}))
 
 
 def main():

@@ -60,7 +60,9 @@ class VolumeInfo(C.Structure):
     _fields_ = [("E", C.c_int * 3), ("N", C.c_int64), ("box", C.c_int * 3), ("n_highres", C.c_int),
                 ("n_stdres", C.c_int), ("n_output", C.c_int), ("kriging_nnz", C.c_int64),
                 ("n_nonpositive", C.c_int), ("max_eigenvalue", C.c_double), ("setup_seconds", C.c_double),
-                ("kriging_seconds", C.c_double), ("neighborhood", C.c_float), ("device_bytes", C.c_int64)]
+                ("kriging_seconds", C.c_double), ("neighborhood", C.c_float), ("device_bytes", C.c_int64),
+                ("kriging_plan_seconds", C.c_double), ("kriging_solve_seconds", C.c_double),
+                ("kriging_device_rows", C.c_int), ("kriging_host_rows", C.c_int)]
 
 
 class HmcOpts(C.Structure):
@@ -453,7 +455,7 @@ def debug_dual_averaging(burnin, nsave, thin, L, starting_eps, mhtarget, rates, 
     return e, s
 
 
-KERNEL_NAMES = ["x-line update (k_xline)", "forward y pass (k_pass)", "forward z pass + gather (k_pass)",
+KERNEL_NAMES = ["state update (k_xyplane when E0 == E1 <= 128, else k_xline)", "forward y pass (k_pass)", "forward z pass + gather (k_pass)",
                 "W product (k_spmv_w)", "W^T product (k_spmv_wt)", "inverse z pass (k_pass)",
                 "inverse y pass (k_pass)"]
 

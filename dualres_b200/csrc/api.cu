@@ -23,6 +23,7 @@
 #include "host_setup.h"
 #include "kernels.cu"
 #include "mce.cuh"
+#include "kriging.cuh"
 #include "estimate.h"
 
 #ifdef _OPENMP
@@ -128,6 +129,7 @@ static DeviceTables& device_tables(int dev) {
     set_plane_attr<4, true>(t.tma_dyn_max); set_plane_attr<8, true>(t.tma_dyn_max);
     set_plane_attr<16, true>(t.tma_dyn_max); set_plane_attr<32, true>(t.tma_dyn_max);
     set_plane_attr<64, true>(t.tma_dyn_max);
+    CK(cudaFuncSetAttribute(k_kriging_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
   }
   t.ready = true;
   return t;
@@ -252,6 +254,156 @@ struct Volume {
 
 static std::mutex g_vol_mtx;
 
+
+// Kriging weights of a prepared volume on the device (k_kriging_rows), then
+// the CSR, its transpose and the host copies.  Rows whose system is not
+// numerically positive definite are solved on the host by the same rule as
+// the host builder (QR).
+static bool device_kriging_enabled() { return std::getenv("DRB_HOST_KRIGING") == nullptr; }
+
+static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const KrigingPlan& P = hv.kplan;
+  const int m = P.m, nrows = P.nrows;
+  const bool have_inv = !P.S.empty();
+  std::vector<double> w(P.col.size(), 0.0);
+  std::vector<char> keep(nrows, 1);
+  // tasks: every row with neighbours; complete rows with equal k' are solved once
+  std::map<std::vector<double>, int> rep;
+  std::vector<int> dup_of(nrows, -1);
+  std::vector<std::pair<double, int>> order;
+  std::vector<int> route(nrows, 0);
+  int nmax = 1;
+  for (int ri = 0; ri < nrows; ri++) {
+    const int r0 = P.row_start[ri], cnt = P.row_start[ri + 1] - r0;
+    if (cnt == 0) continue;
+    if (cnt == m) {
+      std::vector<double> key(P.kp.begin() + r0, P.kp.begin() + r0 + cnt);
+      auto it = rep.find(key);
+      if (it != rep.end()) {
+        dup_of[ri] = it->second;
+        continue;
+      }
+      rep.emplace(std::move(key), ri);
+    }
+    const bool schur = kriging_schur_route(cnt, m, have_inv);
+    route[ri] = schur ? KR_ROUTE_SCHUR : KR_ROUTE_DIRECT;
+    const int n = schur ? m - cnt : cnt;
+    nmax = std::max(nmax, n);
+    const double cost = (double)n * n * n / 3.0 + (schur ? 2.0 * m * cnt : 0.0);
+    order.emplace_back(-cost, ri);
+  }
+  std::sort(order.begin(), order.end());
+  const int ntasks = (int)order.size();
+  std::vector<int> task_row(std::max(ntasks, 1)), task_route(std::max(ntasks, 1));
+  for (int t = 0; t < ntasks; t++) {
+    task_row[t] = order[t].second;
+    task_route[t] = route[order[t].second];
+  }
+  std::vector<int> status(nrows, KR_OK);
+  if (ntasks > 0) {
+    DeviceTables& dt = device_tables(device);
+    CK(cudaSetDevice(device));
+    const size_t slot = (size_t)nmax * nmax + m + nmax + (m + 1) / 2 + 1;
+    int grid = std::min(ntasks, 2 * dt.sms);
+    const size_t budget = (size_t)2 << 30;  // scratch cap
+    grid = std::max(1, std::min(grid, (int)(budget / (slot * sizeof(double)))));
+    std::vector<void*> bufs;
+    auto dalloc = [&](size_t bytes) {
+      void* p = nullptr;
+      const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+      if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync (kriging): ") + cudaGetErrorString(e));
+      bufs.push_back(p);
+      return p;
+    };
+    auto upload = [&](void* dst, const void* src, size_t bytes) {
+      if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    };
+    try {
+      KrigArgs a{};
+      a.m = m;
+      double* dK = (double*)dalloc(sizeof(double) * (size_t)m * m);
+      upload(dK, P.K.data(), sizeof(double) * (size_t)m * m);
+      a.K = dK;
+      if (have_inv) {
+        double* dS = (double*)dalloc(sizeof(double) * (size_t)m * m);
+        upload(dS, P.S.data(), sizeof(double) * (size_t)m * m);
+        a.S = dS;
+      }
+      int* d_rs = (int*)dalloc(sizeof(int) * (nrows + 1));
+      upload(d_rs, P.row_start.data(), sizeof(int) * (nrows + 1));
+      int* d_pid = (int*)dalloc(sizeof(int) * P.pid.size());
+      upload(d_pid, P.pid.data(), sizeof(int) * P.pid.size());
+      double* d_kp = (double*)dalloc(sizeof(double) * P.kp.size());
+      upload(d_kp, P.kp.data(), sizeof(double) * P.kp.size());
+      int* d_tr = (int*)dalloc(sizeof(int) * ntasks);
+      upload(d_tr, task_row.data(), sizeof(int) * ntasks);
+      int* d_tt = (int*)dalloc(sizeof(int) * ntasks);
+      upload(d_tt, task_route.data(), sizeof(int) * ntasks);
+      int* d_cnt = (int*)dalloc(sizeof(int));
+      CK(cudaMemsetAsync(d_cnt, 0, sizeof(int), st));
+      double* d_w = (double*)dalloc(sizeof(double) * w.size());
+      CK(cudaMemsetAsync(d_w, 0, sizeof(double) * w.size(), st));
+      int* d_status = (int*)dalloc(sizeof(int) * nrows);
+      CK(cudaMemsetAsync(d_status, 0, sizeof(int) * nrows, st));
+      double* d_scr = (double*)dalloc(sizeof(double) * slot * grid);
+      a.row_start = d_rs;
+      a.pid = d_pid;
+      a.kp = d_kp;
+      a.task_row = d_tr;
+      a.task_route = d_tt;
+      a.ntasks = ntasks;
+      a.counter = d_cnt;
+      a.w = d_w;
+      a.status = d_status;
+      a.scratch = d_scr;
+      a.slot = slot;
+      a.nmax = nmax;
+      k_kriging_rows<<<grid, KR_NT, sizeof(KrigSmem), st>>>(a);
+      CK_LAUNCH();
+      CK(cudaMemcpyAsync(w.data(), d_w, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(status.data(), d_status, sizeof(int) * nrows, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    } catch (...) {
+      for (void* p : bufs) cudaFreeAsync(p, st);
+      cudaStreamSynchronize(st);
+      cudaGetLastError();
+      throw;
+    }
+    for (void* p : bufs) cudaFreeAsync(p, st);
+    CK(cudaStreamSynchronize(st));
+  }
+  // rows the device could not factor: host route (Cholesky / QR)
+  std::vector<int> redo;
+  for (int ri = 0; ri < nrows; ri++) {
+    if (dup_of[ri] >= 0) continue;
+    if (status[ri] == KR_DROP) keep[ri] = 0;
+    if (status[ri] == KR_NOT_SPD) redo.push_back(ri);
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < (int)redo.size(); i++) {
+    std::vector<double> x;
+    const int ri = redo[i];
+    if (kriging_solve_row_host(P, ri, &x)) std::copy(x.begin(), x.end(), w.begin() + P.row_start[ri]);
+    else keep[ri] = 0;
+  }
+  for (int ri = 0; ri < nrows; ri++) {
+    const int src = dup_of[ri];
+    if (src < 0) continue;
+    keep[ri] = keep[src];
+    std::copy(w.begin() + P.row_start[src], w.begin() + P.row_start[src + 1], w.begin() + P.row_start[ri]);
+  }
+  kriging_assemble(P, w, keep, &hv.w_rowptr, &hv.w_col, &hv.w_val);
+  hv.kplan = KrigingPlan();
+  hv.kriging_pending = false;
+  hv.kriging_device_rows = ntasks;
+  hv.kriging_host_rows = (int)redo.size();
+  build_transpose(&hv);
+  const double dt_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  hv.kriging_solve_seconds = dt_s;
+  hv.kriging_seconds += dt_s;
+}
+
 // Device part of a volume from an already prepared HostVolume (V->hv).
 static void volume_build_device(Volume* V, const float* covariance, int covfun, int device) {
   const auto t0 = std::chrono::steady_clock::now();
@@ -262,6 +414,7 @@ static void volume_build_device(Volume* V, const float* covariance, int covfun, 
   V->tw_f = dt.tw_f;
   V->tw_d = dt.tw_d;
   HostVolume& hv = V->hv;
+  if (hv.kriging_pending) kriging_solve_device(hv, device, V->stream);
   DevVolume& dv = V->dv;
   cudaStream_t st = V->stream;
   dv.E0 = hv.E[0]; dv.E1 = hv.E[1]; dv.E2 = hv.E[2]; dv.N = hv.N;
@@ -325,7 +478,7 @@ static void volume_build(Volume* V, const dr_volume_desc* d) {
   const auto t0 = std::chrono::steady_clock::now();
   device_tables(d->device);
   std::string err;
-  const int rc = host_prepare(d, &V->hv, &err);
+  const int rc = host_prepare(d, &V->hv, &err, device_kriging_enabled());
   if (rc != DR_OK) throw Error(rc, err);
   V->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   volume_build_device(V, d->covariance, d->covfun, d->device);
@@ -882,6 +1035,10 @@ int dr_volume_info_get(const dr_volume* v, dr_volume_info* info) {
   info->n_output = v->dv.n_o;
   info->kriging_nnz = (int64_t)v->hv.w_col.size();
   info->n_nonpositive = v->n_S;
+  info->kriging_plan_seconds = v->hv.kriging_plan_seconds;
+  info->kriging_solve_seconds = v->hv.kriging_solve_seconds;
+  info->kriging_device_rows = v->hv.kriging_device_rows;
+  info->kriging_host_rows = v->hv.kriging_host_rows;
   info->max_eigenvalue = v->max_eig;
   info->setup_seconds = v->setup_seconds;
   info->kriging_seconds = v->hv.kriging_seconds;
@@ -1397,7 +1554,7 @@ struct Server {
       std::string err;
       int rc = DR_OK;
       try {
-        rc = host_prepare(&j->desc, &vol->hv, &err);
+        rc = host_prepare(&j->desc, &vol->hv, &err, device_kriging_enabled());
       } catch (const std::exception& e) {
         rc = DR_ERR_INVALID;
         err = e.what();

@@ -207,9 +207,9 @@ static void mat4_inverse(const double* a, double* inv) {
   for (int i = 0; i < 4; i++) for (int j = 0; j < 4; j++) inv[4 * i + j] = m[i][j + 4];
 }
 
-int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
-                  const float* Qsr, const float* theta, float radius, std::vector<int>* rowptr, std::vector<int>* col,
-                  std::vector<float>* val, int* n_offsets, std::string* err) {
+int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
+                 const float* Qsr, const float* theta, float radius, KrigingPlan* plan, int* n_offsets,
+                 std::string* err) {
   if (radius < 0) { *err = "neighborhood_perturbation: radius cannot be negative"; return DR_ERR_INVALID; }
   std::vector<int> P;
   const int m = neighbourhood(Qhr, radius, &P);
@@ -218,7 +218,9 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
   if (m > 5000) { *err = "get_sparse_kriging_array_data: neighborhood >5e3 voxels"; return DR_ERR_DOMAIN; }
   const double th[3] = {theta[0], theta[1], theta[2]};
   // K over the offsets (kriging_matrix.h:111-138): unit diagonal.
-  std::vector<double> Pm(3 * (size_t)m), K((size_t)m * m);
+  std::vector<double> Pm(3 * (size_t)m);
+  std::vector<double>& K = plan->K;
+  K.assign((size_t)m * m, 0.0);
   for (int i = 0; i < m; i++)
     for (int r = 0; r < 3; r++)
       Pm[3 * i + r] = (double)Qhr[4 * r] * P[3 * i] + (double)Qhr[4 * r + 1] * P[3 * i + 1] +
@@ -311,7 +313,8 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
   // offsets B then has (K_AA)^-1 = S_AA - S_AB (S_BB)^-1 S_BA, which costs
   // O(|A|^2 + |B|^3) instead of the O(|A|^3) of a direct solve; each row takes
   // the cheaper route.  Not positive definite K (variance > 1) -> direct solves.
-  std::vector<double> Sinv;
+  std::vector<double>& Sinv = plan->S;
+  Sinv.clear();
   bool have_inv = false;
   if (!std::getenv("DRB_KRIGING_DIRECT")) {
     std::vector<double> Lf(K);
@@ -340,101 +343,177 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
       have_inv = true;
     }
   }
+  (void)have_inv;
+  plan->m = m;
+  plan->nrows = nrows;
+  plan->row_start.assign(nrows + 1, 0);
+  for (int ri = 0; ri < nrows; ri++) plan->row_start[ri + 1] = plan->row_start[ri] + (int)rcol[ri].size();
+  const size_t tot = (size_t)plan->row_start[nrows];
+  plan->pid.resize(tot);
+  plan->col.resize(tot);
+  plan->kp.resize(tot);
+  for (int ri = 0; ri < nrows; ri++) {
+    const size_t o = (size_t)plan->row_start[ri];
+    std::copy(rpid[ri].begin(), rpid[ri].end(), plan->pid.begin() + o);
+    std::copy(rcol[ri].begin(), rcol[ri].end(), plan->col.begin() + o);
+    std::copy(rkp[ri].begin(), rkp[ri].end(), plan->kp.begin() + o);
+  }
+  return DR_OK;
+}
+
+// One row of the host solve: Schur route or direct Cholesky, QR when the
+// direct system is not numerically positive definite.  x gets the normalised
+// weights; false when the weight sum is NaN (the row is dropped).
+bool kriging_solve_row_host(const KrigingPlan& plan, int ri, std::vector<double>* xout) {
+  const int m = plan.m;
+  const std::vector<double>& K = plan.K;
+  const std::vector<double>& Sinv = plan.S;
+  const bool have_inv = !Sinv.empty();
+  const int r0 = plan.row_start[ri];
+  const int cnt = plan.row_start[ri + 1] - r0;
+  const double* k = plan.kp.data() + r0;
+  const int* pid = plan.pid.data() + r0;
+  std::vector<double> A, b(k, k + cnt), x(cnt, 0.0);
+  const int nb = m - cnt;
+  bool solved = false;
+  if (kriging_schur_route(cnt, m, have_inv)) {
+    // Schur route: w = S_AA k - S_AB (S_BB^-1 (S_BA k))
+    std::vector<char> present(m, 0);
+    for (int a = 0; a < cnt; a++) present[pid[a]] = 1;
+    std::vector<int> B;
+    B.reserve(nb);
+    for (int j = 0; j < m; j++)
+      if (!present[j]) B.push_back(j);
+    std::vector<double> t(nb, 0.0);
+    for (int q = 0; q < nb; q++) {
+      const double* Srow = Sinv.data() + (size_t)B[q] * m;
+      double acc = 0.0;
+      for (int a = 0; a < cnt; a++) acc += Srow[pid[a]] * k[a];
+      t[q] = acc;
+    }
+    A.resize((size_t)nb * nb);
+    for (int q = 0; q < nb; q++)
+      for (int r = 0; r < nb; r++) A[(size_t)q * nb + r] = Sinv[(size_t)B[q] * m + B[r]];
+    if (nb == 0 || cholesky(A.data(), nb)) {
+      if (nb > 0) cholesky_solve(A.data(), nb, t.data());
+      for (int a = 0; a < cnt; a++) {
+        const double* Srow = Sinv.data() + (size_t)pid[a] * m;
+        double acc = 0.0;
+        for (int c = 0; c < cnt; c++) acc += Srow[pid[c]] * k[c];
+        for (int q = 0; q < nb; q++) acc -= Srow[B[q]] * t[q];
+        x[a] = acc;
+      }
+      solved = true;
+    }
+  }
+  if (!solved) {
+    A.resize((size_t)cnt * cnt);
+    for (int a = 0; a < cnt; a++)
+      for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)pid[a] * m + pid[c]];
+    if (cholesky(A.data(), cnt)) {
+      cholesky_solve(A.data(), cnt, b.data());
+      x = b;
+    } else {
+      for (int a = 0; a < cnt; a++)
+        for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)pid[a] * m + pid[c]];
+      b.assign(k, k + cnt);
+      qr_solve(A.data(), cnt, b.data(), x.data());
+    }
+  }
+  double wsum = 0.0;
+  for (int a = 0; a < cnt; a++) wsum += x[a];
+  if (wsum == 0.0) wsum = 1.0;  // kriging_matrix.h:318-319
+  if (std::isnan(wsum)) return false;
+  for (int a = 0; a < cnt; a++) x[a] /= wsum;
+  *xout = std::move(x);
+  return true;
+}
+
+void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, std::vector<int>* col,
+                        std::vector<float>* val) {
+  const int m = plan.m, nrows = plan.nrows;
   // Rows whose neighbourhood is complete share K; identical k' then share w.
   std::map<std::vector<double>, std::vector<double>> full_cache;
   std::mutex cache_mtx;
   std::vector<std::vector<double>> rw(nrows);
   std::vector<char> keep(nrows, 1);
-#pragma omp parallel
-  {
-    std::vector<double> A, b, x;
-#pragma omp for schedule(dynamic, 1)
-    for (int ri = 0; ri < nrows; ri++) {
-      const int cnt = (int)rcol[ri].size();
-      if (cnt == 0) continue;
-      if (cnt == m) {
-        std::lock_guard<std::mutex> lk(cache_mtx);
-        auto it = full_cache.find(rkp[ri]);
-        if (it != full_cache.end()) { rw[ri] = it->second; continue; }
-      }
-      x.assign(cnt, 0.0);
-      const int nb = m - cnt;
-      bool solved = false;
-      if (have_inv && (double)nb * nb * nb / 3.0 + (double)cnt * cnt < (double)cnt * cnt * cnt / 3.0) {
-        // Schur route: w = S_AA k - S_AB (S_BB^-1 (S_BA k))
-        std::vector<char> present(m, 0);
-        for (int a = 0; a < cnt; a++) present[rpid[ri][a]] = 1;
-        std::vector<int> B;
-        B.reserve(nb);
-        for (int j = 0; j < m; j++)
-          if (!present[j]) B.push_back(j);
-        const std::vector<double>& k = rkp[ri];
-        std::vector<double> t(nb, 0.0);
-        for (int q = 0; q < nb; q++) {
-          const double* Srow = Sinv.data() + (size_t)B[q] * m;
-          double acc = 0.0;
-          for (int a = 0; a < cnt; a++) acc += Srow[rpid[ri][a]] * k[a];
-          t[q] = acc;
-        }
-        A.resize((size_t)nb * nb);
-        for (int q = 0; q < nb; q++)
-          for (int r = 0; r < nb; r++) A[(size_t)q * nb + r] = Sinv[(size_t)B[q] * m + B[r]];
-        if (nb == 0 || cholesky(A.data(), nb)) {
-          if (nb > 0) cholesky_solve(A.data(), nb, t.data());
-          for (int a = 0; a < cnt; a++) {
-            const double* Srow = Sinv.data() + (size_t)rpid[ri][a] * m;
-            double acc = 0.0;
-            for (int c = 0; c < cnt; c++) acc += Srow[rpid[ri][c]] * k[c];
-            for (int q = 0; q < nb; q++) acc -= Srow[B[q]] * t[q];
-            x[a] = acc;
-          }
-          solved = true;
-        }
-      }
-      if (!solved) {
-        A.resize((size_t)cnt * cnt);
-        for (int a = 0; a < cnt; a++)
-          for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)rpid[ri][a] * m + rpid[ri][c]];
-        b = rkp[ri];
-      }
-      if (solved) {
-        // x holds the Schur solution
-      } else if (cholesky(A.data(), cnt)) {
-        cholesky_solve(A.data(), cnt, b.data());
-        x = b;
-      } else {
-        for (int a = 0; a < cnt; a++)
-          for (int c = 0; c < cnt; c++) A[(size_t)a * cnt + c] = K[(size_t)rpid[ri][a] * m + rpid[ri][c]];
-        b = rkp[ri];
-        qr_solve(A.data(), cnt, b.data(), x.data());
-      }
-      double wsum = 0.0;
-      for (int a = 0; a < cnt; a++) wsum += x[a];
-      if (wsum == 0.0) wsum = 1.0;       // kriging_matrix.h:318-319
-      if (std::isnan(wsum)) { keep[ri] = 0; continue; }
-      for (int a = 0; a < cnt; a++) x[a] /= wsum;
-      rw[ri] = x;
-      if (cnt == m) {
-        std::lock_guard<std::mutex> lk(cache_mtx);
-        full_cache.emplace(rkp[ri], x);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ri = 0; ri < nrows; ri++) {
+    const int r0 = plan.row_start[ri];
+    const int cnt = plan.row_start[ri + 1] - r0;
+    if (cnt == 0) continue;
+    std::vector<double> krow;
+    if (cnt == m) {
+      krow.assign(plan.kp.begin() + r0, plan.kp.begin() + r0 + cnt);
+      std::lock_guard<std::mutex> lk(cache_mtx);
+      auto it = full_cache.find(krow);
+      if (it != full_cache.end()) {
+        rw[ri] = it->second;
+        continue;
       }
     }
+    std::vector<double> x;
+    if (!kriging_solve_row_host(plan, ri, &x)) {
+      keep[ri] = 0;
+      continue;
+    }
+    rw[ri] = x;
+    if (cnt == m) {
+      std::lock_guard<std::mutex> lk(cache_mtx);
+      full_cache.emplace(krow, x);
+    }
   }
-  rowptr->assign(nrows + 1, 0);
+  std::vector<double> flat(plan.col.size(), 0.0);
+  for (int ri = 0; ri < nrows; ri++)
+    if (keep[ri]) std::copy(rw[ri].begin(), rw[ri].end(), flat.begin() + plan.row_start[ri]);
+  kriging_assemble(plan, flat, keep, rowptr, col, val);
+}
+
+void kriging_assemble(const KrigingPlan& plan, const std::vector<double>& w, const std::vector<char>& keep,
+                      std::vector<int>* rowptr, std::vector<int>* col, std::vector<float>* val) {
+  rowptr->assign(plan.nrows + 1, 0);
   col->clear();
   val->clear();
-  for (int ri = 0; ri < nrows; ri++) {
-    if (keep[ri] && !rcol[ri].empty()) {
-      col->insert(col->end(), rcol[ri].begin(), rcol[ri].end());
-      for (double w : rw[ri]) val->push_back((float)w);
+  for (int ri = 0; ri < plan.nrows; ri++) {
+    const int r0 = plan.row_start[ri], r1 = plan.row_start[ri + 1];
+    if (keep[ri] && r1 > r0) {
+      col->insert(col->end(), plan.col.begin() + r0, plan.col.begin() + r1);
+      for (int k = r0; k < r1; k++) val->push_back((float)w[k]);
     }
     (*rowptr)[ri + 1] = (int)col->size();
   }
+}
+
+int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
+                  const float* Qsr, const float* theta, float radius, std::vector<int>* rowptr, std::vector<int>* col,
+                  std::vector<float>* val, int* n_offsets, std::string* err) {
+  KrigingPlan plan;
+  const int rc = kriging_plan(hr, nx, ny, nz, Qhr, sr, sx, sy, sz, Qsr, theta, radius, &plan, n_offsets, err);
+  if (rc != DR_OK) return rc;
+  kriging_solve_host(plan, rowptr, col, val);
   return DR_OK;
 }
 
+
 // ---------------------------------------------------------------- preparation
-int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err) {
+void build_transpose(HostVolume* hv) {
+  const int n_h = (int)hv->Yh.size(), n_s = (int)hv->Ys.size();
+  hv->wt_rowptr.assign(n_h + 1, 0);
+  for (int c : hv->w_col) hv->wt_rowptr[c + 1]++;
+  for (int i = 0; i < n_h; i++) hv->wt_rowptr[i + 1] += hv->wt_rowptr[i];
+  hv->wt_col.resize(hv->w_col.size());
+  hv->wt_val.resize(hv->w_col.size());
+  std::vector<int> fill(hv->wt_rowptr.begin(), hv->wt_rowptr.end() - 1);
+  for (int r = 0; r < n_s; r++)
+    for (int k = hv->w_rowptr[r]; k < hv->w_rowptr[r + 1]; k++) {
+      const int c = hv->w_col[k];
+      hv->wt_col[fill[c]] = r;
+      hv->wt_val[fill[c]] = hv->w_val[k];
+      fill[c]++;
+    }
+}
+
+int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err, bool defer_kriging) {
   if (!d || !d->highres || !d->qform_hr || d->nx <= 0 || d->ny <= 0 || d->nz <= 0) {
     *err = "dr_volume_create: highres image and qform are required";
     return DR_ERR_INVALID;
@@ -543,27 +622,22 @@ int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err) {
     }
     hv->radius = radius;
     const auto t0 = std::chrono::steady_clock::now();
-    const int rc = kriging_build(hr.data(), nx, ny, nz_, d->qform_hr, sr.data(), d->sx, d->sy, d->sz, d->qform_sr,
-                                 d->covariance, radius, &hv->w_rowptr, &hv->w_col, &hv->w_val, &hv->n_offsets, err);
-    hv->kriging_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const int rc = kriging_plan(hr.data(), nx, ny, nz_, d->qform_hr, sr.data(), d->sx, d->sy, d->sz, d->qform_sr,
+                                d->covariance, radius, &hv->kplan, &hv->n_offsets, err);
     if (rc != DR_OK) return rc;
-    for (int c : hv->w_col)
+    hv->kriging_plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int c : hv->kplan.col)
       if (c < 0 || c >= n_h) { *err = "kriging: column outside the data range"; return DR_ERR_DOMAIN; }
-    // transpose (rows ordered by data voxel, columns ascending)
-    const int n_s = (int)hv->Ys.size();
-    hv->wt_rowptr.assign(n_h + 1, 0);
-    for (int c : hv->w_col) hv->wt_rowptr[c + 1]++;
-    for (int i = 0; i < n_h; i++) hv->wt_rowptr[i + 1] += hv->wt_rowptr[i];
-    hv->wt_col.resize(hv->w_col.size());
-    hv->wt_val.resize(hv->w_col.size());
-    std::vector<int> fill(hv->wt_rowptr.begin(), hv->wt_rowptr.end() - 1);
-    for (int r = 0; r < n_s; r++)
-      for (int k = hv->w_rowptr[r]; k < hv->w_rowptr[r + 1]; k++) {
-        const int c = hv->w_col[k];
-        hv->wt_col[fill[c]] = r;
-        hv->wt_val[fill[c]] = hv->w_val[k];
-        fill[c]++;
-      }
+    if (defer_kriging) {
+      hv->kriging_pending = true;
+    } else {
+      kriging_solve_host(hv->kplan, &hv->w_rowptr, &hv->w_col, &hv->w_val);
+      hv->kplan = KrigingPlan();
+      build_transpose(hv);
+      hv->kriging_solve_seconds =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - hv->kriging_plan_seconds;
+    }
+    hv->kriging_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   } else {
     hv->wt_rowptr.assign(n_h + 1, 0);
   }

@@ -8,6 +8,26 @@
 
 namespace drb {
 
+// The part of the kriging build that fixes the sparsity (kriging_matrix.h:148-299)
+// and the covariances the per-row solves need.
+struct KrigingPlan {
+  int m = 0;                   // neighbourhood offsets
+  int nrows = 0;               // std-res data voxels
+  std::vector<double> K;       // m x m covariance of the offsets (unit diagonal)
+  std::vector<double> S;       // K^-1, empty when K is not positive definite
+  std::vector<int> row_start;  // nrows + 1, into pid / col / kp
+  std::vector<int> pid;        // offset id of each present neighbour
+  std::vector<int> col;        // its high-res data ordinal (the CSR column)
+  std::vector<double> kp;      // its covariance with the std-res voxel centre
+};
+
+// A row with cnt of m neighbours present solves through the Schur complement of
+// S when that is cheaper than a direct solve.
+inline bool kriging_schur_route(int cnt, int m, bool have_inv) {
+  const double nb = (double)(m - cnt), c = (double)cnt;
+  return have_inv && nb * nb * nb / 3.0 + c * c < c * c * c / 3.0;
+}
+
 struct HostVolume {
   int g[3] = {0, 0, 0};       // grid of the data voxels (max ijk + 1)
   int E[3] = {0, 0, 0};       // embedding
@@ -25,11 +45,33 @@ struct HostVolume {
   int covfun = 0;
   float radius = 0.f;
   double kriging_seconds = 0.0;
+  double kriging_plan_seconds = 0.0;
+  double kriging_solve_seconds = 0.0;
   int n_offsets = 0;
+  KrigingPlan kplan;           // kept until the weights are solved
+  bool kriging_pending = false;
+  int kriging_device_rows = 0;  // rows solved on the device
+  int kriging_host_rows = 0;    // rows the device left to the host (not positive definite)
 };
 
-// Returns DR_OK or a DR_ERR_* code with a message in *err.
-int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err);
+// Returns DR_OK or a DR_ERR_* code with a message in *err.  With defer_kriging
+// the kriging weights are left to the device (hv->kriging_pending, hv->kplan).
+int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err, bool defer_kriging = false);
+
+// W^T from W (rows ordered by data voxel, columns ascending).
+void build_transpose(HostVolume* hv);
+
+int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
+                 const float* Qsr, const float* theta, float radius, KrigingPlan* plan, int* n_offsets,
+                 std::string* err);
+void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, std::vector<int>* col,
+                        std::vector<float>* val);
+// One row by the host route (Schur or Cholesky, QR if not positive definite);
+// false when its weight sum is NaN.
+bool kriging_solve_row_host(const KrigingPlan& plan, int ri, std::vector<double>* x);
+// CSR from per-candidate weights; rows with keep = 0 are emptied (NaN weight sums).
+void kriging_assemble(const KrigingPlan& plan, const std::vector<double>& w, const std::vector<char>& keep,
+                      std::vector<int>* rowptr, std::vector<int>* col, std::vector<float>* val);
 
 // Kriging CSR of kriging_matrix.h:148-343 (exposed for tests through the volume).
 int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,

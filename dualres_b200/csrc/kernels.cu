@@ -438,67 +438,91 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   const float keps = ((first || last) ? 0.5f : 1.0f) * eps;
   const float Nf = (float)N;
   double pa = 0.0, pb = 0.0;
-  for (int e = tid; e < E * (E / 2); e += NT) {
-    const int y = e / (E / 2), x = 2 * (e % (E / 2));
-    const int li = y * E + x;
-    const float4 u4 = *reinterpret_cast<const float4*>(srcU + li);
-    const float2 s2 = *reinterpret_cast<const float2*>(srcS + li);
-    float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    float2 w0 = make_float2(0.f, 0.f), w1 = w0;
-    if (!need_q) {
-      const long long gi = (long long)z * E * E + li;
-      const u32x4 r = philox(u32x4{(uint32_t)(gi >> 1), (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c),
-                                   RNG_MOMENTUM}, ch.seed);
-      w0 = box_muller(u01f(r.x), u01f(r.y));
-      w1 = box_muller(u01f(r.z), u01f(r.w));
-      pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
-    } else {
-      q4 = *reinterpret_cast<const float4*>(srcQ + li);
-    }
-    const int pi0 = G::at(y, x), pi1 = G::at(y, x + 1);
-    float2 uo[2], qo[2];
+  // Pairs of x-adjacent points: element pair e sits at li = 2e of the plane (x = 2 (e mod E/2), y = e / (E/2)),
+  // so U, q and 1/lambda are read as float4 / float4 / float2 at index e.  Each thread first issues the loads
+  // of B pairs, then computes and stores them, so B loads per array are in flight at once.  A thread reads and
+  // writes only its own elements, which is why the in-place state buffers may be marked non-aliasing.
+  constexpr int TOTAL = E * (E / 2);
+  constexpr int B = TOTAL >= 2 * NT ? 2 : 1;
+  const float4* __restrict__ gU = reinterpret_cast<const float4*>(srcU);
+  const float4* __restrict__ gQ = reinterpret_cast<const float4*>(srcQ);
+  const float2* __restrict__ gS = reinterpret_cast<const float2*>(srcS);
+  float4* __restrict__ oQ = reinterpret_cast<float4*>(Qc);
+  float4* __restrict__ oU = reinterpret_cast<float4*>(Udst);
+  for (int e0 = tid; e0 < TOTAL; e0 += B * NT) {
+    float4 u4v[B], q4v[B];
+    float2 s2v[B];
 #pragma unroll
-    for (int m = 0; m < 2; m++) {
-      const float2 u = m == 0 ? make_float2(u4.x, u4.y) : make_float2(u4.z, u4.w);
-      const float s = m == 0 ? s2.x : s2.y;
-      const bool live = s > 0.0f;
-      const float lm = s + sh;
-      float2 q;
-      if (!need_q) {
-        const float2 w = m == 0 ? w0 : w1;
-        const float a = live ? sqrtf(Nf * lm) : 0.0f;
-        q = make_float2(a * w.x, a * w.y);
-      } else {
-        q = m == 0 ? make_float2(q4.x, q4.y) : make_float2(q4.z, q4.w);
-        if (first && live) pa += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+    for (int b = 0; b < B; b++) {
+      const int e = e0 + b * NT;
+      if (e < TOTAL) {
+        u4v[b] = gU[e];
+        s2v[b] = gS[e];
+        q4v[b] = need_q ? gQ[e] : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      if (first && live) pb += (double)(u.x * u.x + u.y * u.y) * (double)s;
-      const int pi = m == 0 ? pi0 : pi1;
-      const float2 g = sm[pi];
-      float2 gt = g;
-      if (live) {
-        gt.x = fmaf(-u.x, s, g.x);
-        gt.y = fmaf(-u.y, s, g.y);
-      }
-      q.x = fmaf(keps, gt.x, q.x);
-      q.y = fmaf(keps, gt.y, q.y);
-      float2 un = u;
-      if (last) {
-        if (live) {
-          pa += (double)(u.x * u.x + u.y * u.y) * (double)s;
-          pb += (double)(q.x * q.x + q.y * q.y) / (double)lm;
-        }
-      } else if (live) {
-        const float f = eps / lm;
-        un.x = fmaf(f, q.x, u.x);
-        un.y = fmaf(f, q.y, u.y);
-      }
-      uo[m] = un;
-      qo[m] = q;
-      sm[pi] = un;
     }
-    if (write_q) *reinterpret_cast<float4*>(Qc + li) = make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y);
-    if (!last) *reinterpret_cast<float4*>(Udst + li) = make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y);
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      const int e = e0 + b * NT;
+      if (e >= TOTAL) continue;
+      const int y = e / (E / 2), x = 2 * (e % (E / 2));
+      const float4 u4 = u4v[b];
+      const float2 s2 = s2v[b];
+      const float4 q4 = q4v[b];
+      float2 w0 = make_float2(0.f, 0.f), w1 = w0;
+      if (!need_q) {
+        const long long gi = (long long)z * E * E + 2 * e;
+        const u32x4 r = philox(u32x4{(uint32_t)(gi >> 1), (uint32_t)st.iteration, (uint32_t)(ch.chain0 + c),
+                                     RNG_MOMENTUM}, ch.seed);
+        w0 = box_muller(u01f(r.x), u01f(r.y));
+        w1 = box_muller(u01f(r.z), u01f(r.w));
+        pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
+      }
+      const int pi0 = G::at(y, x), pi1 = G::at(y, x + 1);
+      float2 uo[2], qo[2];
+#pragma unroll
+      for (int m = 0; m < 2; m++) {
+        const float2 u = m == 0 ? make_float2(u4.x, u4.y) : make_float2(u4.z, u4.w);
+        const float s = m == 0 ? s2.x : s2.y;
+        const bool live = s > 0.0f;
+        const float lm = s + sh;
+        float2 q;
+        if (!need_q) {
+          const float2 w = m == 0 ? w0 : w1;
+          const float a = live ? sqrtf(Nf * lm) : 0.0f;
+          q = make_float2(a * w.x, a * w.y);
+        } else {
+          q = m == 0 ? make_float2(q4.x, q4.y) : make_float2(q4.z, q4.w);
+          if (first && live) pa += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+        }
+        if (first && live) pb += (double)(u.x * u.x + u.y * u.y) * (double)s;
+        const int pi = m == 0 ? pi0 : pi1;
+        const float2 g = sm[pi];
+        float2 gt = g;
+        if (live) {
+          gt.x = fmaf(-u.x, s, g.x);
+          gt.y = fmaf(-u.y, s, g.y);
+        }
+        q.x = fmaf(keps, gt.x, q.x);
+        q.y = fmaf(keps, gt.y, q.y);
+        float2 un = u;
+        if (last) {
+          if (live) {
+            pa += (double)(u.x * u.x + u.y * u.y) * (double)s;
+            pb += (double)(q.x * q.x + q.y * q.y) / (double)lm;
+          }
+        } else if (live) {
+          const float f = eps / lm;
+          un.x = fmaf(f, q.x, u.x);
+          un.y = fmaf(f, q.y, u.y);
+        }
+        uo[m] = un;
+        qo[m] = q;
+        sm[pi] = un;
+      }
+      if (write_q) oQ[e] = make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y);
+      if (!last) oU[e] = make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y);
+    }
   }
   if (first || last) {
     const double ta = block_sum(pa, red);

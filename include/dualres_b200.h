@@ -76,6 +76,10 @@ typedef struct {
   double kriging_seconds;     /* of which the kriging build */
   float neighborhood;         /* radius used (mm) */
   int64_t device_bytes;       /* device memory held by the volume */
+  double kriging_plan_seconds;   /* of the kriging build: sparsity, covariances and K^-1 */
+  double kriging_solve_seconds;  /* ... the per-row solves (device, or host) */
+  int kriging_device_rows;    /* rows solved on the device (complete rows with equal k' once) */
+  int kriging_host_rows;      /* rows left to the host (not numerically positive definite) */
 } dr_volume_info;
 
 /* Replaces MultiResData<T>(h_res, s_res, theta, r) (MultiResData.h:96-127), the
