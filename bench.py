@@ -164,6 +164,9 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()  # the first sample arrives once nvidia-smi is up: start timing after it
+            while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
@@ -174,6 +177,12 @@ class ClockSampler:
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        try:  # one more sample at the end of the timed region
+            out = subprocess.run(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                  "-i", str(self.gpu)], capture_output=True, text=True, timeout=10).stdout
+            self.lines.extend(ln.strip() for ln in out.splitlines())
+        except Exception:
+            pass
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
