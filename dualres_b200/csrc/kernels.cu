@@ -578,7 +578,7 @@ __device__ __forceinline__ void csr_batches(const float* __restrict__ val, const
 // one block per row of W (grid-stride over rows); the 8 warps share the
 // row's 32-nonzero batches and combine their sums in a fixed order.
 template <int CG, int NR>
-__global__ void __launch_bounds__(256) k_spmv_w(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+__global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int C = ch.C, Cp = ch.Cp;
   const int cc = lane % CG;
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(256) k_spmv_w(DevVolume v, DevChains ch, int s
 // one warp per data voxel over the transposed CSR (grid-stride), plus the
 // ||Yh - mu_D||^2 partials per block.
 template <int CG, int NR>
-__global__ void __launch_bounds__(256) k_spmv_wt(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+__global__ void __launch_bounds__(256, 4) k_spmv_wt(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int C = ch.C, Cp = ch.Cp;
   const int cc = lane % CG;
