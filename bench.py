@@ -334,7 +334,8 @@ def run_ours(args, dist):
     cfg = config_of(args.workload, {
         "global_batch": C * dist.world, "l2": "working set larger than L2 (state 0.5 GB per GPU)",
         "n_highres": info.n_highres, "n_stdres": info.n_stdres, "kriging_nnz": int(info.kriging_nnz),
-        "setup_seconds": info.setup_seconds, "kriging_seconds": info.kriging_seconds})
+        "setup_seconds": info.setup_seconds, "kriging_seconds": info.kriging_seconds,
+        "chain_set_config": chains.config()})
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,

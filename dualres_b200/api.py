@@ -135,6 +135,7 @@ def _declare(L):
     L.dr_volume_destroy.argtypes = [vp]
     L.dr_volume_destroy.restype = None
     L.dr_chainset_create.argtypes = [vp, C.c_int, C.POINTER(HmcOpts), C.POINTER(vp)]
+    L.dr_chainset_config_get.argtypes = [vp, _ip, _ip, _dp]
     L.dr_chainset_destroy.argtypes = [vp]
     L.dr_chainset_destroy.restype = None
     L.dr_step.argtypes = [vp, C.c_int]
@@ -364,6 +365,14 @@ class MultiResParameters:
     def _field(self, x):
         a = np.ascontiguousarray(x, dtype=np.complex64).reshape(self.data.shape)
         return a
+
+    PATHS = ("plane", "plane+prefetch", "lines")
+
+    def config(self):
+        """The chain set's update path, kriging-product blocks per SM, and tuned iteration time (ms, 0 if untuned)."""
+        p, g, ms = C.c_int(0), C.c_int(0), C.c_double(0)
+        check(lib().dr_chainset_config_get(self.h, C.byref(p), C.byref(g), C.byref(ms)))
+        return dict(path=self.PATHS[p.value], blocks_per_sm=g.value, tuned_ms=ms.value)
 
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))

@@ -499,6 +499,9 @@ struct Chainset {
   int tmp_blocks = 0;
   int NR = 1;
   bool plane = false;           // fused xy-plane update (E0 == E1 <= 128)
+  int path = 0;                 // 0 plane kernel, 1 plane kernel with bulk prefetch, 2 x-line kernel + y passes
+  int grid = 8;                 // kriging-product blocks per SM
+  double tuned_ms = 0.0;        // iteration time of the chosen configuration when it was tuned (0: not tuned)
   bool tma = false;             // ... in the persistent bulk-copy kernel (E0 <= 64, fits shared memory)
   int tma_smem = 0, tma_grid = 0;
 
@@ -721,7 +724,101 @@ static void init_chain_states(Chainset* S) {
   CK(cudaStreamSynchronize(S->stream));
 }
 
-static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) {
+// ---------------------------------------------------------------- autotuning
+// Candidate update paths for an embedding: the fused plane kernel (square x/y
+// planes whose padded layout fits shared memory), the same with bulk prefetch
+// of the state planes, and the x-line kernel with separate y passes (always).
+struct PathOptions {
+  bool plane = false, prefetch = false;
+};
+static PathOptions path_options(const DevVolume& v, int device) {
+  PathOptions po;
+  if (!(v.E0 == v.E1 && v.E0 >= 4 && v.E0 <= 128)) return po;
+  const DeviceTables& dt = device_tables(device);
+  const int elems = v.E0 == 64 ? PlaneGeom<64>::SIZE : (v.E0 == 128 ? PlaneGeom<128>::SIZE : v.E0 * (v.E0 + 1));
+  po.plane = plane_layout(v.E0, elems, false).total <= dt.tma_dyn_max;
+  po.prefetch = po.plane && v.E0 <= 64 && plane_layout(v.E0, elems, true).total <= dt.tma_dyn_max;
+  return po;
+}
+
+struct TuneChoice {
+  int path = 0;      // 0 plane, 1 plane + prefetch, 2 x-line
+  int grid = 8;      // kriging-product blocks per SM
+  double ms = 0.0;   // measured milliseconds per iteration
+};
+
+static bool autotune_enabled() {
+  const char* e = std::getenv("DRB_AUTOTUNE");
+  return !(e && std::string(e) == "0");
+}
+
+struct TuneKey {
+  int dev, E0, E1, E2, bx, by, bz, C, n_h, n_s, L;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, E0, E1, E2, bx, by, bz, C, n_h, n_s, L) <
+           std::tie(o.dev, o.E0, o.E1, o.E2, o.bx, o.by, o.bz, o.C, o.n_h, o.n_s, o.L);
+  }
+};
+static std::mutex g_tune_mtx;
+static std::map<TuneKey, TuneChoice> g_tune;
+
+static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, const TuneChoice* forced = nullptr);
+static void launch_iterations(Chainset* S, int iters);
+static void read_states(Chainset* S, std::vector<ChainState>* st);
+static void write_states(Chainset* S, const std::vector<ChainState>& st);
+
+// Times every candidate (update path x kriging-product grid) on a scratch chain
+// set of the same shape, forced past the step-size search so that all L
+// leapfrog steps run, and keeps the fastest; results are cached per shape.
+static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
+  const DevVolume& v = V->dv;
+  const TuneKey key{V->device, v.E0, v.E1, v.E2, v.bx, v.by, v.bz, C, v.n_h, v.n_s, o->leapfrog};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mtx);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  const PathOptions po = path_options(v, V->device);
+  std::vector<TuneChoice> cand;
+  for (int path : {0, 1, 2}) {
+    if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
+    for (int grid : {8, 4, 2}) cand.push_back(TuneChoice{path, grid, 0.0});
+  }
+  TuneChoice best;
+  best.ms = 1e300;
+  dr_hmc_opts to = *o;
+  to.store_samples = 0;
+  for (TuneChoice& c : cand) {
+    auto T = std::make_unique<Chainset>();
+    chainset_build(T.get(), V, C, &to, &c);
+    std::vector<ChainState> st;
+    read_states(T.get(), &st);
+    for (auto& h : st) {
+      h.eps_start_found = 1;  // integrator_steps() = L from the first iteration
+      h.warmup = 1;
+    }
+    write_states(T.get(), st);
+    launch_iterations(T.get(), 1);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, T->stream));
+    launch_iterations(T.get(), 3);
+    CK(cudaEventRecord(e1, T->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.ms = ms / 3.0;
+    if (c.ms < best.ms) best = c;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mtx);
+  g_tune[key] = best;
+  return best;
+}
+
+static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, const TuneChoice* forced) {
   if (C <= 0 || C > 256) throw Error(DR_ERR_UNSUPPORTED, "n_chains must be in [1, 256]");
   if (!o) throw Error(DR_ERR_INVALID, "opts is NULL");
   if (o->burnin < 0) throw Error(DR_ERR_DOMAIN, "HMCParameters: burnin must be >= 0");
@@ -753,17 +850,26 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   const long long N = v.N;
   ch.U = S->alloc<float2>((size_t)C * 2 * N);
   ch.Q = S->alloc<float2>((size_t)C * N);
-  S->plane = v.E0 == v.E1 && v.E0 >= 4 && v.E0 <= 128 && !std::getenv("DRB_NO_PLANE");
-  if (S->plane) {
-    // the fused plane kernel needs the whole padded plane in shared memory
-    const DeviceTables& dt = device_tables(V->device);
-    const int elems = v.E0 == 64 ? PlaneGeom<64>::SIZE : (v.E0 == 128 ? PlaneGeom<128>::SIZE : v.E0 * (v.E0 + 1));
-    if (plane_layout(v.E0, elems, false).total > dt.tma_dyn_max) S->plane = false;
-    // optional variant with bulk prefetch of the U, q and 1/lambda planes
-    if (S->plane && v.E0 <= 64 && std::getenv("DRB_PLANE_PREFETCH") &&
-        plane_layout(v.E0, elems, true).total <= dt.tma_dyn_max)
-      S->tma = true;
+  const PathOptions po = path_options(v, V->device);
+  int path = po.plane ? 0 : 2, grid = 8;
+  if (forced) {
+    path = forced->path;
+    grid = forced->grid;
+  } else if (std::getenv("DRB_NO_PLANE")) {
+    path = 2;
+  } else if (std::getenv("DRB_PLANE_PREFETCH")) {
+    path = po.prefetch ? 1 : path;
+  } else if (autotune_enabled()) {
+    const TuneChoice t = autotune(V, C, o);
+    path = t.path;
+    grid = t.grid;
+    S->tuned_ms = t.ms;
   }
+  if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) path = po.plane ? 0 : 2;
+  S->path = path;
+  S->grid = grid;
+  S->plane = path != 2;
+  S->tma = path == 1;
   ch.t2_stride = (long long)v.E2 * v.by * v.bx;
   if (S->plane) {
     // T1 is only needed by the initial transforms: borrow the momentum buffer
@@ -779,8 +885,9 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o) 
   ch.gD = S->alloc<float>((size_t)v.n_h * C);
   ch.rs = S->alloc<float>((size_t)std::max(v.n_s, 1) * C);
   ch.nb_x = S->plane ? v.E2 : cdiv_i((long long)v.E1 * v.E2, TILE_LINES);
-  ch.nb_w = std::max(1, std::min(v.n_s, 148 * 8));
-  ch.nb_wt = std::max(1, std::min(cdiv_i(v.n_h, 8), 148 * 8));
+  const int wide = device_tables(V->device).sms * S->grid;
+  ch.nb_w = std::max(1, std::min(v.n_s, wide));
+  ch.nb_wt = std::max(1, std::min(cdiv_i(v.n_h, 8), wide));
   ch.maxblk = std::max(ch.nb_x, std::max(ch.nb_w, ch.nb_wt));
   ch.part = S->alloc<double>((size_t)C * NSLOT * ch.maxblk);
   ch.st = S->alloc<ChainState>(C);
@@ -1098,6 +1205,15 @@ int dr_chainset_create(dr_volume* v, int n_chains, const dr_hmc_opts* opts, dr_c
 }
 
 void dr_chainset_destroy(dr_chainset* s) { delete s; }
+
+int dr_chainset_config_get(const dr_chainset* s, int* path, int* blocks_per_sm, double* tuned_ms) {
+  API_BEGIN
+  if (!s) throw Error(DR_ERR_INVALID, "NULL chain set");
+  if (path) *path = s->path;
+  if (blocks_per_sm) *blocks_per_sm = s->grid;
+  if (tuned_ms) *tuned_ms = s->tuned_ms;
+  API_END
+}
 
 int dr_step(dr_chainset* s, int iterations) {
   API_BEGIN

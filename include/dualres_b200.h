@@ -157,6 +157,14 @@ int dr_samples_get(dr_chainset* cs, int chain, float* samples, int max_saved, in
  * the columns after mu in the --samples stream (gaussian_process_model.h:149-163). */
 int dr_sample_records_get(dr_chainset* cs, int chain, double* rec, int max_saved, int* n_saved);
 void dr_chainset_destroy(dr_chainset* cs);
+/* The configuration the chain set runs (no reference counterpart): update path
+ * (0 fused x/y plane kernel, 1 the same with bulk prefetch of the state planes,
+ * 2 x-line kernel with separate y passes), kriging-product blocks per SM, and the
+ * iteration time measured when the shape was tuned (0 when it was not).  At
+ * creation every eligible (path, blocks) pair is timed on a scratch chain set of
+ * the same shape, and the fastest is kept for the process; DRB_AUTOTUNE=0 turns
+ * this off, DRB_NO_PLANE / DRB_PLANE_PREFETCH force a path. */
+int dr_chainset_config_get(const dr_chainset* cs, int* path, int* blocks_per_sm, double* tuned_ms);
 
 /* ---- fixed-input evaluation (MultiResParameters public API) ------------- */
 /* Sets chain `chain` to mu (2N floats) and sigma^-2 = (s_hr, s_sr). */

@@ -1,0 +1,48 @@
+"""Per-shape autotuning of the chain-set configuration (update path and
+kriging-product grid): a tuned chain set reports one of the candidates and the
+time it measured, a second chain set of the same shape reuses the choice, and
+the switches that turn tuning off or force a path are honoured.  The sampler's
+results on any configuration are covered by the parity tests, which run every
+path against the oracle."""
+import numpy as np
+import pytest
+
+import dualres_b200 as d
+from dualres_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _chains(vol, C, leapfrog):
+    data = d.MultiResData.from_volume(vol)
+    return data, d.MultiResParameters(data, d.HMCParameters(burnin=4, nsave=3, thin=1, leapfrog=leapfrog, seed=2), C)
+
+
+def test_tuned_choice_is_cached_per_shape(monkeypatch):
+    for k in ("DRB_AUTOTUNE", "DRB_NO_PLANE", "DRB_PLANE_PREFETCH"):
+        monkeypatch.delenv(k, raising=False)
+    vol = synth.small_volume(seed=51, dims=(12, 12, 10))
+    data, a = _chains(vol, 3, 7)
+    ca = a.config()
+    assert ca["path"] in d.MultiResParameters.PATHS and ca["blocks_per_sm"] in (2, 4, 8)
+    assert ca["tuned_ms"] > 0
+    b = d.MultiResParameters(data, d.HMCParameters(burnin=4, nsave=3, thin=1, leapfrog=7, seed=9), 3)
+    assert b.config() == ca  # same shape: the cached choice, not a new measurement
+    a.run()
+    st = a.stats()
+    assert all(s["done"] == 1 for s in st)
+    assert np.all(np.isfinite(a.summary(-1)["mean"]))
+    a.close(), b.close(), data.close()
+
+
+def test_switches(monkeypatch):
+    vol = synth.small_volume(seed=52, dims=(12, 12, 10))
+    monkeypatch.setenv("DRB_AUTOTUNE", "0")
+    monkeypatch.delenv("DRB_NO_PLANE", raising=False)
+    monkeypatch.delenv("DRB_PLANE_PREFETCH", raising=False)
+    data, a = _chains(vol, 2, 5)
+    assert a.config() == {"path": "plane", "blocks_per_sm": 8, "tuned_ms": 0.0}
+    monkeypatch.setenv("DRB_NO_PLANE", "1")
+    b = d.MultiResParameters(data, d.HMCParameters(burnin=4, nsave=3, thin=1, leapfrog=5, seed=2), 2)
+    assert b.config()["path"] == "lines"
+    a.close(), b.close(), data.close()

@@ -37,6 +37,7 @@ def update_path(request, monkeypatch):
     and the x-line kernel with separate y passes (every other embedding)."""
     monkeypatch.delenv("DRB_NO_PLANE", raising=False)
     monkeypatch.delenv("DRB_PLANE_PREFETCH", raising=False)
+    monkeypatch.setenv("DRB_AUTOTUNE", "0")  # the path under test, not the tuner's choice
     if request.param == "lines":
         monkeypatch.setenv("DRB_NO_PLANE", "1")
     elif request.param == "prefetch":
