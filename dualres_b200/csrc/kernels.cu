@@ -864,10 +864,12 @@ __global__ void k_base(double2* base, int E0, int E1, int E2, float q00, float q
   const int l = (int)(i % E0), m = (int)((i / E0) % E1), n = (int)(i / ((long long)E0 * E1));
   const float o0 = (float)(l <= E0 / 2 ? l : E0 - l), o1 = (float)(m <= E1 / 2 ? m : E1 - m),
               o2 = (float)(n <= E2 / 2 ? n : E2 - n);
-  const float a = q00 * o0 + q01 * o1 + q02 * o2;
-  const float b = q10 * o0 + q11 * o1 + q12 * o2;
-  const float cc = q20 * o0 + q21 * o1 + q22 * o2;
-  const double d = (double)sqrtf(a * a + b * b + cc * cc);
+  // float arithmetic in source order with every product and sum rounded (no fused multiply-add), so the
+  // distances equal a plain float evaluation of the same expression on the host
+  const float a = __fadd_rn(__fadd_rn(__fmul_rn(q00, o0), __fmul_rn(q01, o1)), __fmul_rn(q02, o2));
+  const float b = __fadd_rn(__fadd_rn(__fmul_rn(q10, o0), __fmul_rn(q11, o1)), __fmul_rn(q12, o2));
+  const float cc = __fadd_rn(__fadd_rn(__fmul_rn(q20, o0), __fmul_rn(q21, o1)), __fmul_rn(q22, o2));
+  const double d = (double)__fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(cc, cc)));
   double val;
   if (covfun == 0)
     val = th0 * exp(-th1 * pow(fabs(d), th2));

@@ -176,6 +176,22 @@ def make_volume(latent_dims=(32, 32, 32), voxel_mm=1.0, theta=(0.806, 0.132, 1.0
                   radius=float(radius), latent=lat_img, name=name)
 
 
+def rotated(vol, quatern=(0.2895, -0.866, -0.2865), voxel=(1.8, 1.8, 2.3), qfac=-1.0, offset=(-90.0, 120.0, -40.0)):
+    """The same images under a scanner-like geometry: the high-res qform becomes a
+    rotation (unit quaternion b, c, d) of anisotropic voxels with qfac, and the
+    std-res qform keeps its index map to the high-res grid (centre of std voxel s
+    at high-res index 2 s + 0.5), so the kriging neighbourhoods are rotated
+    balls of the new voxel geometry."""
+    import dataclasses
+    from .nifti import quatern_to_qform
+    Qh = quatern_to_qform(*quatern, voxel, offset, qfac).astype(np.float64)
+    Qs = None
+    if vol.stdres is not None:
+        M = np.array([[2, 0, 0, 0.5], [0, 2, 0, 0.5], [0, 0, 2, 0.5], [0, 0, 0, 1]], np.float64)
+        Qs = (Qh @ M).astype(np.float32)
+    return dataclasses.replace(vol, qform_hr=Qh.astype(np.float32), qform_sr=Qs, name=vol.name + "_rotated")
+
+
 # The workloads named by the reference's benchmark configurations.
 def config_c1(seed=1):
     """32^3 latent at 1 mm, RBF(0.806, 0.132, 1) -> 64^3 embedding, ellipsoid mask ~60%."""

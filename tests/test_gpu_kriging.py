@@ -18,6 +18,7 @@ CASES = {
     "aniso_1p5": dict(dims=(16, 18, 14), voxel=1.5, theta=(1.0, 0.4, 1.5), radius=6.9),
     "smooth": dict(dims=(18, 16, 16), voxel=1.0, theta=(0.95, 0.05, 2.0), radius=5.0),
     "variance_above_1": dict(dims=(14, 14, 12), voxel=1.0, theta=(1.6, 0.3, 1.0), radius=3.5),
+    "rotated_aniso": dict(dims=(18, 18, 14), voxel=1.0, theta=(0.9, 0.3, 1.2), radius=6.9, rotate=True),
 }
 
 
@@ -25,6 +26,8 @@ CASES = {
 def test_device_kriging_matches_host(name, monkeypatch):
     c = CASES[name]
     vol = synth.make_volume(c["dims"], c["voxel"], c["theta"], 0.5, 0.3, c["radius"], "ellipsoid", 0.65, 9)
+    if c.get("rotate"):
+        vol = synth.rotated(vol)
     monkeypatch.delenv("DRB_HOST_KRIGING", raising=False)
     dv = d.MultiResData.from_volume(vol)
     rp, col, val = dv.W()

@@ -48,6 +48,8 @@ CASES = {
     "single_res_rbf": dict(dual=False, covfun=0, theta=(0.9, 0.35, 1.3)),
     "dual_res_rq": dict(dual=True, covfun=1, theta=(1.1, 0.4, 1.5)),
     "single_res_rq": dict(dual=False, covfun=1, theta=(0.8, 0.25, 1.0)),
+    # scanner-like geometry: rotated qform, 1.8 x 1.8 x 2.3 mm voxels, qfac -1 (std-res at twice the size)
+    "rotated_aniso_rbf": dict(dual=True, covfun=0, theta=(0.9, 0.3, 1.2), rotate=True),
 }
 
 
@@ -57,6 +59,8 @@ def test_variant_matches_oracle(oracle, case, update_path):  # noqa: F811
     from dualres_b200 import synth
     c = CASES[case]
     vol = synth.small_volume(seed=21, theta=c["theta"], dual=c["dual"])
+    if c.get("rotate"):
+        vol = synth.rotated(vol)
     dv, m, prep = _pair(oracle, vol, c["covfun"])
     assert tuple(dv.E) == m.E
     assert dv.n_stdres == (0 if not c["dual"] else dv.n_stdres) and dv.n_highres == len(prep["Yh"])
