@@ -119,6 +119,8 @@ WORKLOADS = {
     "served": dict(chains=1, vol="c4", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
     "served_c1": dict(chains=1, vol="c1", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
     "served_tiny": dict(chains=1, vol="small", burnin=20, nsave=20, thin=1, leapfrog=5, rate=50.0),  # test-sized
+    # config 4: 32 volumes of the uneven size/parameter distribution fitted together (all submitted at once)
+    "uneven32": dict(chains=1, vol="c4", burnin=300, nsave=300, thin=3, leapfrog=25, rate=float("inf"), jobs=32),
 }
 
 
@@ -378,13 +380,15 @@ def run_served(args, dist):
     import dualres_b200 as d
     wl = WORKLOADS[args.workload]
     rate = args.rate if args.rate > 0 else wl["rate"]
+    if "jobs" in wl:
+        args.steps = wl["jobs"]
     hmc = lambda i: d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"],  # noqa: E731
                                     leapfrog=wl["leapfrog"], seed=args.seed + 7919 * dist.rank + i)
     t0 = time.perf_counter()
     vols = [served_volume(wl, i, args.seed + dist.rank * 100003) for i in range(args.warmup + args.steps)]
     gen_s = time.perf_counter() - t0
     rng = np.random.default_rng(args.seed + dist.rank)
-    gaps = rng.exponential(1.0 / rate, size=args.steps)
+    gaps = rng.exponential(1.0 / rate, size=args.steps) if np.isfinite(rate) else np.zeros(args.steps)
     sv = d.Server(device=0, iterations_per_round=8, host_threads=4)
     # warm-up jobs (untimed): library tables, pools, first graphs
     for i in range(args.warmup):

@@ -767,7 +767,8 @@ static void launch_iterations(Chainset* S, int iters);
 static void read_states(Chainset* S, std::vector<ChainState>* st);
 static void write_states(Chainset* S, const std::vector<ChainState>& st);
 
-// Times every candidate (update path x kriging-product grid) on a scratch chain
+// Times every candidate (update path x kriging-product grid; chain sets of 32 or
+// more chains keep 8 blocks/SM) for 2 iterations on a scratch chain
 // set of the same shape, forced past the step-size search so that all L
 // leapfrog steps run, and keeps the fastest; results are cached per shape.
 static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
@@ -782,7 +783,11 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   std::vector<TuneChoice> cand;
   for (int path : {0, 1, 2}) {
     if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
-    for (int grid : {8, 4, 2}) cand.push_back(TuneChoice{path, grid, 0.0});
+    // wide chain sets share each W row across their chains and fill the GPU at 8 blocks/SM; narrower ones
+    // may do better with fewer, longer-lived product blocks
+    if (C >= 32) cand.push_back(TuneChoice{path, 8, 0.0});
+    else
+      for (int grid : {8, 4, 2}) cand.push_back(TuneChoice{path, grid, 0.0});
   }
   TuneChoice best;
   best.ms = 1e300;
@@ -803,14 +808,14 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, T->stream));
-    launch_iterations(T.get(), 3);
+    launch_iterations(T.get(), 2);
     CK(cudaEventRecord(e1, T->stream));
     CK(cudaEventSynchronize(e1));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    c.ms = ms / 3.0;
+    c.ms = ms / 2.0;
     if (c.ms < best.ms) best = c;
   }
   std::lock_guard<std::mutex> lk(g_tune_mtx);

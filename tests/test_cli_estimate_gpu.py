@@ -123,3 +123,25 @@ def test_cli_estimates_covariance_when_absent(tmp_path):
     s = api.mce_summary(vol.stdres, vol.qform_sr)
     th2 = api.fit_rbf_parameters(s["distance"], s["covariance"], s["npairs"])
     assert np.allclose(th, th2, rtol=1e-4)
+
+
+def test_cli_patient_sized_rotated_volume(tmp_path):
+    """A clinical-sized input: 120 x 120 x 72 high-res voxels of 1.8 x 1.8 x 2.3 mm under a rotated qform with
+    qfac -1, std-res at twice the voxel size (256^3 embedding, x-line update path)."""
+    vol = synth.rotated(synth.make_volume((120, 120, 72), 1.0, (1.0, 0.3, 1.5), 0.5, 0.3, 6.9, "ellipsoid", 0.6, 17))
+    tmp = str(tmp_path)
+    nifti.write(os.path.join(tmp, "hr.nii.gz"), vol.highres, pixdim=(1.8, 1.8, 2.3),
+                quatern=(0.2895, -0.866, -0.2865), qoffset=(-90.0, 120.0, -40.0), qfac=-1)
+    _, Qh, _ = nifti.read(os.path.join(tmp, "hr.nii.gz"))
+    assert np.allclose(Qh, vol.qform_hr, atol=1e-5)
+    Qs = vol.qform_sr.astype(np.float64)
+    nifti.write(os.path.join(tmp, "sr.nii.gz"), vol.stdres, pixdim=(3.6, 3.6, 4.6),
+                quatern=(0.2895, -0.866, -0.2865), qoffset=tuple(Qs[:3, 3]), qfac=-1)
+    r = _cli(["--highres", "hr.nii.gz", "--stdres", "sr.nii.gz", "--covariance", "1", "0.3", "1.5",
+              "--burnin", "5", "--nsave", "3", "--thin", "1", "--leapfrog", "3", "--seed", "4", "--output", "big"], tmp)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert "Neighborhood: 6.9 (mm)" in r.stdout
+    mean, Q, _ = nifti.read(os.path.join(tmp, "big_posterior_mean.nii.gz"))
+    assert np.allclose(Q, vol.qform_hr, atol=1e-5)
+    sel = vol.highres != 0
+    assert np.all(np.isfinite(mean[sel])) and np.count_nonzero(mean[sel]) > 0.99 * sel.sum()
