@@ -547,24 +547,57 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
 // ... of [ks, ke): the batch's values and columns are loaded once, coalesced,
 // and broadcast by shuffle, so the X loads of a batch are independent and
 // stay in flight together.
-template <int CG, int NR>
+template <int CG, int NR, int PF>
 __device__ __forceinline__ void csr_batches(const float* __restrict__ val, const int* __restrict__ col, int ks, int ke,
                                             int b0, int bs, const float* const (&x)[NR], int Cp, int lane,
                                             float (&acc)[NR]) {
   constexpr int G = 32 / CG;
   const int grp = lane / CG;
-  for (int base = ks + b0 * 32; base < ke; base += bs * 32) {
-    const int n = min(32, ke - base);
-    const float mv = lane < n ? __ldg(val + base + lane) : 0.f;
-    const int mc = lane < n ? __ldg(col + base + lane) : 0;
+  if constexpr (PF == 1) {
+    for (int base = ks + b0 * 32; base < ke; base += bs * 32) {
+      const int n = min(32, ke - base);
+      const float mv = lane < n ? __ldg(val + base + lane) : 0.f;
+      const int mc = lane < n ? __ldg(col + base + lane) : 0;
 #pragma unroll
-    for (int j0 = 0; j0 < 32; j0 += G) {
-      const int j = j0 + grp;
-      const float w = __shfl_sync(0xffffffffu, mv, j);
-      const long long cidx = (long long)__shfl_sync(0xffffffffu, mc, j) * Cp;
-      if (j < n) {
+      for (int j0 = 0; j0 < 32; j0 += G) {
+        const int j = j0 + grp;
+        const float w = __shfl_sync(0xffffffffu, mv, j);
+        const long long cidx = (long long)__shfl_sync(0xffffffffu, mc, j) * Cp;
+        if (j < n) {
 #pragma unroll
-        for (int r = 0; r < NR; r++) acc[r] = fmaf(w, x[r][cidx], acc[r]);
+          for (int r = 0; r < NR; r++) acc[r] = fmaf(w, x[r][cidx], acc[r]);
+        }
+      }
+    }
+  } else {
+    // PF batches of values and columns are loaded before any is used, so that several 256-byte loads per warp
+    // are in flight while the matrix streams from memory; the batches are then consumed in their usual order.
+    for (int base = ks + b0 * 32; base < ke; base += PF * bs * 32) {
+      float mvp[PF];
+      int mcp[PF], np[PF];
+#pragma unroll
+      for (int p = 0; p < PF; p++) {
+        const int bb = base + p * bs * 32;
+        np[p] = max(0, min(32, ke - bb));
+        mvp[p] = lane < np[p] ? __ldg(val + bb + lane) : 0.f;
+        mcp[p] = lane < np[p] ? __ldg(col + bb + lane) : 0;
+      }
+#pragma unroll
+      for (int p = 0; p < PF; p++) {
+        const int n = np[p];
+        if (n == 0) break;
+        const float mv = mvp[p];
+        const int mc = mcp[p];
+#pragma unroll
+        for (int j0 = 0; j0 < 32; j0 += G) {
+          const int j = j0 + grp;
+          const float w = __shfl_sync(0xffffffffu, mv, j);
+          const long long cidx = (long long)__shfl_sync(0xffffffffu, mc, j) * Cp;
+          if (j < n) {
+#pragma unroll
+            for (int r = 0; r < NR; r++) acc[r] = fmaf(w, x[r][cidx], acc[r]);
+          }
+        }
       }
     }
   }
@@ -598,7 +631,9 @@ __global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, in
     float acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
-    csr_batches<CG, NR>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], warp, 8, x, Cp, lane, acc);
+    // two batches ahead help narrow chain groups; with 32 chains per warp the gathers already overlap
+    csr_batches<CG, NR, (CG == 32 ? 1 : 2)>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], warp, 8, x, Cp,
+                                            lane, acc);
     if (lane < CG) {
 #pragma unroll
       for (int r = 0; r < NR; r++) red[warp][lane + CG * r] = acc[r];
@@ -655,7 +690,8 @@ __global__ void __launch_bounds__(256, 4) k_spmv_wt(DevVolume v, DevChains ch, i
     float acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
-    if (v.n_s > 0) csr_batches<CG, NR>(v.wt_val, v.wt_col, v.wt_rowptr[row], v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc);
+    if (v.n_s > 0)
+      csr_batches<CG, NR, 2>(v.wt_val, v.wt_col, v.wt_rowptr[row], v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc);
     if (lane < CG) {
       const float yh = v.Yh[row];
 #pragma unroll
