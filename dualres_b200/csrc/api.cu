@@ -130,6 +130,8 @@ static DeviceTables& device_tables(int dev) {
     set_plane_attr<16, true>(t.tma_dyn_max); set_plane_attr<32, true>(t.tma_dyn_max);
     set_plane_attr<64, true>(t.tma_dyn_max);
     CK(cudaFuncSetAttribute(k_kriging_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
+    CK(cudaFuncSetAttribute(k_spd_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
+    CK(cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
   }
   t.ready = true;
   return t;
@@ -261,8 +263,53 @@ static std::mutex g_vol_mtx;
 // the host builder (QR).
 static bool device_kriging_enabled() { return std::getenv("DRB_HOST_KRIGING") == nullptr; }
 
+// K^-1 of a kriging plan on the device (one block factors K, then all blocks
+// solve for the rows of K^-1); leaves P.S empty when K is not positive definite.
+static void device_spd_inverse(KrigingPlan& P, int device, cudaStream_t st) {
+  const int m = P.m;
+  DeviceTables& dt = device_tables(device);
+  CK(cudaSetDevice(device));
+  const int grid = std::max(1, std::min(m, 2 * dt.sms));
+  std::vector<void*> bufs;
+  auto dalloc = [&](size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync (K^-1): ") + cudaGetErrorString(e));
+    bufs.push_back(p);
+    return p;
+  };
+  try {
+    double* dM = (double*)dalloc(sizeof(double) * (size_t)m * m);
+    double* dS = (double*)dalloc(sizeof(double) * (size_t)m * m);
+    double* dB = (double*)dalloc(sizeof(double) * (size_t)m * grid);
+    int* dok = (int*)dalloc(sizeof(int));
+    CK(cudaMemcpyAsync(dM, P.K.data(), sizeof(double) * (size_t)m * m, cudaMemcpyHostToDevice, st));
+    k_spd_factor<<<1, KR_NT, sizeof(KrigSmem), st>>>(dM, m, dok);
+    CK_LAUNCH();
+    int ok = 0;
+    CK(cudaMemcpyAsync(&ok, dok, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ok) {
+      k_spd_inverse<<<grid, KR_NT, sizeof(KrigSmem), st>>>(dM, m, dS, dB);
+      CK_LAUNCH();
+      k_symmetrize<<<cdiv_i((long long)m * m, 256), 256, 0, st>>>(dS, m);
+      CK_LAUNCH();
+      P.S.resize((size_t)m * m);
+      CK(cudaMemcpyAsync(P.S.data(), dS, sizeof(double) * (size_t)m * m, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+  } catch (...) {
+    for (void* p : bufs) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    throw;
+  }
+  for (void* p : bufs) cudaFreeAsync(p, st);
+}
+
 static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
   const auto t0 = std::chrono::steady_clock::now();
+  if (hv.kplan.S.empty() && hv.kplan.inverse_wanted && hv.kplan.m > 0) device_spd_inverse(hv.kplan, device, st);
   const KrigingPlan& P = hv.kplan;
   const int m = P.m, nrows = P.nrows;
   const bool have_inv = !P.S.empty();
@@ -794,29 +841,40 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   dr_hmc_opts to = *o;
   to.store_samples = 0;
   for (TuneChoice& c : cand) {
-    auto T = std::make_unique<Chainset>();
-    chainset_build(T.get(), V, C, &to, &c);
-    std::vector<ChainState> st;
-    read_states(T.get(), &st);
-    for (auto& h : st) {
-      h.eps_start_found = 1;  // integrator_steps() = L from the first iteration
-      h.warmup = 1;
+    // a candidate that cannot be built or run (for instance out of device memory beside the caller's other
+    // allocations) is skipped; if none can, the default configuration is used untuned
+    try {
+      auto T = std::make_unique<Chainset>();
+      chainset_build(T.get(), V, C, &to, &c);
+      std::vector<ChainState> st;
+      read_states(T.get(), &st);
+      for (auto& h : st) {
+        h.eps_start_found = 1;  // integrator_steps() = L from the first iteration
+        h.warmup = 1;
+      }
+      write_states(T.get(), st);
+      launch_iterations(T.get(), 1);
+      cudaEvent_t e0, e1;
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      CK(cudaEventRecord(e0, T->stream));
+      launch_iterations(T.get(), 2);
+      CK(cudaEventRecord(e1, T->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      c.ms = ms / 2.0;
+      if (c.ms < best.ms) best = c;
+    } catch (const Error&) {
+      cudaGetLastError();
     }
-    write_states(T.get(), st);
-    launch_iterations(T.get(), 1);
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, T->stream));
-    launch_iterations(T.get(), 2);
-    CK(cudaEventRecord(e1, T->stream));
-    CK(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    c.ms = ms / 2.0;
-    if (c.ms < best.ms) best = c;
+  }
+  if (!(best.ms < 1e300)) {  // nothing could be timed: default, not cached
+    TuneChoice d;
+    d.path = po.plane ? 0 : 2;
+    return d;
   }
   std::lock_guard<std::mutex> lk(g_tune_mtx);
   g_tune[key] = best;

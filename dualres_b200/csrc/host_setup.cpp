@@ -209,7 +209,7 @@ static void mat4_inverse(const double* a, double* inv) {
 
 int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
                  const float* Qsr, const float* theta, float radius, KrigingPlan* plan, int* n_offsets,
-                 std::string* err) {
+                 std::string* err, bool host_inverse) {
   if (radius < 0) { *err = "neighborhood_perturbation: radius cannot be negative"; return DR_ERR_INVALID; }
   std::vector<int> P;
   const int m = neighbourhood(Qhr, radius, &P);
@@ -316,7 +316,8 @@ int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, cons
   std::vector<double>& Sinv = plan->S;
   Sinv.clear();
   bool have_inv = false;
-  if (!std::getenv("DRB_KRIGING_DIRECT")) {
+  plan->inverse_wanted = !std::getenv("DRB_KRIGING_DIRECT");
+  if (plan->inverse_wanted && host_inverse) {
     std::vector<double> Lf(K);
     if (cholesky(Lf.data(), m)) {
       Sinv.assign((size_t)m * m, 0.0);
@@ -623,7 +624,7 @@ int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err, bool
     hv->radius = radius;
     const auto t0 = std::chrono::steady_clock::now();
     const int rc = kriging_plan(hr.data(), nx, ny, nz_, d->qform_hr, sr.data(), d->sx, d->sy, d->sz, d->qform_sr,
-                                d->covariance, radius, &hv->kplan, &hv->n_offsets, err);
+                                d->covariance, radius, &hv->kplan, &hv->n_offsets, err, !defer_kriging);
     if (rc != DR_OK) return rc;
     hv->kriging_plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int c : hv->kplan.col)

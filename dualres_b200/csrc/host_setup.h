@@ -14,7 +14,8 @@ struct KrigingPlan {
   int m = 0;                   // neighbourhood offsets
   int nrows = 0;               // std-res data voxels
   std::vector<double> K;       // m x m covariance of the offsets (unit diagonal)
-  std::vector<double> S;       // K^-1, empty when K is not positive definite
+  std::vector<double> S;       // K^-1, empty when K is not positive definite (or not computed yet)
+  bool inverse_wanted = true;  // the Schur route is allowed (DRB_KRIGING_DIRECT unset)
   std::vector<int> row_start;  // nrows + 1, into pid / col / kp
   std::vector<int> pid;        // offset id of each present neighbour
   std::vector<int> col;        // its high-res data ordinal (the CSR column)
@@ -61,9 +62,10 @@ int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err, bool
 // W^T from W (rows ordered by data voxel, columns ascending).
 void build_transpose(HostVolume* hv);
 
+// host_inverse = false leaves K^-1 to the caller (the device solve computes it).
 int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
                  const float* Qsr, const float* theta, float radius, KrigingPlan* plan, int* n_offsets,
-                 std::string* err);
+                 std::string* err, bool host_inverse = true);
 void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, std::vector<int>* col,
                         std::vector<float>* val);
 // One row by the host route (Schur or Cholesky, QR if not positive definite);

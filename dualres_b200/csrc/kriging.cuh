@@ -267,6 +267,40 @@ __device__ void kr_rows_dot(const double* Mat, int m, const int* rows, int nrows
   }
 }
 
+// K = L L^T in place by one block (M holds K on entry); *ok = 1 when K is positive definite.
+__global__ void __launch_bounds__(KR_NT) k_spd_factor(double* M, int n, int* ok) {
+  extern __shared__ __align__(16) unsigned char kr_smraw[];
+  KrigSmem& sm = *reinterpret_cast<KrigSmem*>(kr_smraw);
+  const bool good = kr_cholesky(M, n, sm);
+  if (threadIdx.x == 0) *ok = good ? 1 : 0;
+}
+
+// Rows of S = K^-1 from the factor: each block solves L L^T x = e_j for its
+// share of j (x in its scratch vector) and stores x as row j of S.
+__global__ void __launch_bounds__(KR_NT) k_spd_inverse(const double* L, int n, double* S, double* scratch) {
+  extern __shared__ __align__(16) unsigned char kr_smraw[];
+  KrigSmem& sm = *reinterpret_cast<KrigSmem*>(kr_smraw);
+  double* b = scratch + (size_t)blockIdx.x * n;
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += KR_NT) b[i] = i == j ? 1.0 : 0.0;
+    __syncthreads();
+    kr_solve(L, n, b, sm);
+    for (int i = threadIdx.x; i < n; i += KR_NT) S[(size_t)j * n + i] = b[i];
+  }
+}
+
+// S = (S + S^T) / 2 (the two triangular solves leave O(eps) asymmetry).
+__global__ void k_symmetrize(double* S, int n) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * n) return;
+  const int i = (int)(e / n), j = (int)(e % n);
+  if (j >= i) return;
+  const double a = 0.5 * (S[(size_t)i * n + j] + S[(size_t)j * n + i]);
+  S[(size_t)i * n + j] = a;
+  S[(size_t)j * n + i] = a;
+}
+
 __global__ void __launch_bounds__(KR_NT) k_kriging_rows(KrigArgs a) {
   extern __shared__ __align__(16) unsigned char kr_smraw[];
   KrigSmem& sm = *reinterpret_cast<KrigSmem*>(kr_smraw);
