@@ -286,6 +286,16 @@ def run_ours(args, dist):
     value = grads_all / t_max
 
     extra = {}
+    # ---- BASELINE B2: the reference algorithm ported plainly to the GPU (four FFTs per step), one chain
+    try:
+        r_plain, ms_plain = plain_gpu_rate(data, wl["leapfrog"], 10)
+        extra["plain_gpu_single_chain"] = {
+            "value": r_plain, "unit": UNIT, "ms_per_iteration": ms_plain,
+            "batched_over_plain": (grads / (ms / 1e3)) / r_plain,
+            "what": "reference algorithm on the GPU: torch.fft (cuFFT) 3D transforms, 4 per leapfrog step, sparse CSR "
+                    "kriging products, host accept each iteration (bench.py PlainGPU)"}
+    except Exception as e:  # the comparator must not break the benchmark line
+        extra["plain_gpu_single_chain"] = {"error": str(e)[:200]}
     # ---- the plain single-chain GPU form on the same volume (same kernels, one chain)
     if C > 1:
         one = d.MultiResParameters(data, d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"],
@@ -363,6 +373,125 @@ def run_ours(args, dist):
     data.close()
     return line
 
+
+
+# ------------------------------------------------------------------ plain single-chain GPU baseline
+class PlainGPU:
+    """The reference's single-chain algorithm ported to the GPU the plain way (BASELINE B2): mu and p kept in real
+    space, four full 3D FFTs per leapfrog step (cuFFT through torch.fft), the kriging products as sparse CSR
+    matrix-vector products, the accept decision read back every iteration.  It follows the restated algorithm of
+    MultiResParameters::update (include/dualres/MultiResParameters.h:337-376, 674-727, 784-859) on the volume the
+    library prepared (its indices, data, kriging matrix and FP64 eigenvalues).  A comparator for the benchmark,
+    not part of the library."""
+
+    def __init__(self, data, device="cuda:0"):
+        import warnings
+
+        import torch
+        warnings.filterwarnings("ignore", message=".*[Ss]parse.*")
+        self.t = torch
+        self.dev = device
+        lam = torch.tensor(data.lambda_re(), dtype=torch.float32, device=device)
+        self.live = lam > 0
+        self.inv_lam = torch.where(self.live, 1.0 / lam, torch.zeros_like(lam))
+        self.N = lam.numel()
+        self.shape = tuple(lam.shape)
+        d_idx, _ = data.indices()
+        self.D = torch.tensor(d_idx.astype(np.int64), device=device)
+        yh, ys = data.data()
+        self.Yh = torch.tensor(yh, device=device)
+        self.Ys = torch.tensor(ys, device=device)
+        self.dual = len(ys) > 0
+        if self.dual:
+            rp, col, val = data.W()
+            W = torch.sparse_csr_tensor(torch.tensor(rp.astype(np.int64)), torch.tensor(col.astype(np.int64)),
+                                        torch.tensor(val), size=(len(ys), len(yh)))
+            self.W = W.to(device)
+            self.WT = W.to_sparse_coo().t().coalesce().to_sparse_csr().to(device)
+
+    def dft_plus(self, x):   # unnormalised inverse transform (FFTW sign +)
+        return self.t.fft.ifftn(x, norm="forward")
+
+    def dft_minus(self, x):  # unnormalised forward transform (FFTW sign -)
+        return self.t.fft.fftn(x, norm="backward")
+
+    def residuals(self, mu):
+        muD = mu.real.reshape(-1)[self.D]
+        rh = self.Yh - muD
+        rs = self.Ys - (self.W @ muD.unsqueeze(1)).squeeze(1) if self.dual else None
+        return rh, rs
+
+    def gradient(self, mu, sh, ss):
+        t = self.t
+        u = self.dft_plus(mu)
+        g = self.dft_minus(t.where(self.live, u * (-self.inv_lam / self.N), t.zeros_like(u)))
+        rh, rs = self.residuals(mu)
+        dg = sh * rh + (ss * (self.WT @ rs.unsqueeze(1)).squeeze(1) if self.dual else 0.0)
+        gr = t.zeros(self.N, dtype=t.float32, device=self.dev)
+        gr.index_add_(0, self.D, dg)
+        return g + gr.reshape(self.shape)
+
+    def log_post(self, mu, sh, ss):
+        t = self.t
+        u = self.dft_plus(mu)
+        lp = -0.5 / self.N * t.sum(t.where(self.live, (u.real ** 2 + u.imag ** 2) * self.inv_lam,
+                                            t.zeros_like(self.inv_lam)), dtype=t.float64)
+        rh, rs = self.residuals(mu)
+        ll = -0.5 * sh * t.sum(rh.double() ** 2)
+        if self.dual:
+            ll = ll - 0.5 * ss * t.sum(rs.double() ** 2)
+        return lp + ll, rh, rs
+
+    def iteration(self, mu, sh, ss, eps, L, gen):
+        t = self.t
+        lam_m = t.where(self.live, self.inv_lam + sh, t.zeros_like(self.inv_lam))
+        inv_lam_m = t.where(self.live, 1.0 / t.where(self.live, lam_m, t.ones_like(lam_m)), t.zeros_like(lam_m))
+        z = t.complex(t.randn(self.shape, generator=gen, device=self.dev), t.randn(self.shape, generator=gen, device=self.dev))
+        e0 = -0.5 * t.sum((z.real ** 2 + z.imag ** 2).double())
+        p = self.dft_minus(t.where(self.live, t.sqrt(lam_m) * self.dft_plus(z) / self.N, t.zeros_like(z)))
+        h0, _, _ = self.log_post(mu, sh, ss)
+        mu1 = mu
+        p = p + 0.5 * eps * self.gradient(mu1, sh, ss)
+        for s in range(1, L + 1):
+            mu1 = mu1 + self.dft_minus(t.where(self.live, self.dft_plus(p) * (eps * inv_lam_m / self.N), t.zeros_like(p)))
+            p = p + (0.5 if s == L else 1.0) * eps * self.gradient(mu1, sh, ss)
+        q = self.dft_plus(p)
+        kin = -0.5 / self.N * t.sum(t.where(self.live, (q.real ** 2 + q.imag ** 2) * inv_lam_m,
+                                           t.zeros_like(inv_lam_m)), dtype=t.float64)
+        h1, rh, rs = self.log_post(mu1, sh, ss)
+        log_r = float(h1 + kin - (e0 + h0))
+        accept = np.log(float(t.rand((), generator=gen, device=self.dev))) < log_r
+        if accept:
+            mu = mu1
+        rh, rs = self.residuals(mu)
+        sh = float(t.distributions.Gamma(len(self.Yh) / 2 + 1, 0.5 * t.sum(rh ** 2)).sample())
+        if self.dual:
+            ss = float(t.distributions.Gamma(len(self.Ys) / 2 + 1, 0.5 * t.sum(rs ** 2)).sample())
+        return mu, sh, ss
+
+
+def plain_gpu_rate(data, L, iters, seed=3):
+    """Gradient evaluations per second of PlainGPU on one chain (CUDA events, after 2 warm-up iterations)."""
+    import torch
+    pg = PlainGPU(data)
+    gen = torch.Generator(device="cuda:0")
+    gen.manual_seed(seed)
+    yh, _ = data.data()
+    mr = torch.zeros(pg.N, dtype=torch.float32, device="cuda:0")
+    mr[pg.D] = torch.tensor(yh, device="cuda:0")
+    mu = torch.complex(mr.reshape(pg.shape), torch.zeros_like(mr).reshape(pg.shape))
+    sh, ss, eps = 2.0, 5.0, 0.02
+    for _ in range(2):
+        mu, sh, ss = pg.iteration(mu, sh, ss, eps, L, gen)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(iters):
+        mu, sh, ss = pg.iteration(mu, sh, ss, eps, L, gen)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return iters * (L + 1) / (ms / 1e3), ms / iters
 
 
 # ------------------------------------------------------------------ served stream
