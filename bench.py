@@ -501,8 +501,7 @@ def served_volume(wl, i, seed):
         return synth.config_c4_volume(i, seed=seed)
     if wl["vol"] == "small":
         return synth.small_volume(seed=seed + i)
-    v = synth.config_c1()
-    return v
+    return synth.config_c1(seed=seed + i)  # each request its own image (same geometry class)
 
 
 def run_served(args, dist):
