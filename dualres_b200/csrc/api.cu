@@ -928,6 +928,9 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     grid = t.grid;
     S->tuned_ms = t.ms;
   }
+  if (!forced) {
+    if (const char* g = std::getenv("DRB_PRODUCT_BLOCKS_PER_SM")) grid = std::max(1, std::min(16, std::atoi(g)));
+  }
   if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) path = po.plane ? 0 : 2;
   S->path = path;
   S->grid = grid;
