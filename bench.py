@@ -241,7 +241,7 @@ def run_ours(args, dist):
     vol = make_volume(wl["vol"])
     d.lib()
     import ctypes
-    dev = 0
+    dev = dist.local  # one process per GPU: the library works on this rank's device
 
     # ---- process warm-up (untimed): CUDA context, module loading, per-device tables
     from dualres_b200 import synth as _synth
@@ -288,7 +288,7 @@ def run_ours(args, dist):
     extra = {}
     # ---- BASELINE B2: the reference algorithm ported plainly to the GPU (four FFTs per step), one chain
     try:
-        r_plain, ms_plain = plain_gpu_rate(data, wl["leapfrog"], 10)
+        r_plain, ms_plain = plain_gpu_rate(data, wl["leapfrog"], 10, device=dev)
         extra["plain_gpu_single_chain"] = {
             "value": r_plain, "unit": UNIT, "ms_per_iteration": ms_plain,
             "batched_over_plain": (grads / (ms / 1e3)) / r_plain,
@@ -470,26 +470,28 @@ class PlainGPU:
         return mu, sh, ss
 
 
-def plain_gpu_rate(data, L, iters, seed=3):
+def plain_gpu_rate(data, L, iters, seed=3, device=0):
     """Gradient evaluations per second of PlainGPU on one chain (CUDA events, after 2 warm-up iterations)."""
     import torch
-    pg = PlainGPU(data)
-    gen = torch.Generator(device="cuda:0")
+    dev = f"cuda:{device}"
+    pg = PlainGPU(data, dev)
+    gen = torch.Generator(device=dev)
     gen.manual_seed(seed)
     yh, _ = data.data()
-    mr = torch.zeros(pg.N, dtype=torch.float32, device="cuda:0")
-    mr[pg.D] = torch.tensor(yh, device="cuda:0")
+    mr = torch.zeros(pg.N, dtype=torch.float32, device=dev)
+    mr[pg.D] = torch.tensor(yh, device=dev)
     mu = torch.complex(mr.reshape(pg.shape), torch.zeros_like(mr).reshape(pg.shape))
     sh, ss, eps = 2.0, 5.0, 0.02
     for _ in range(2):
         mu, sh, ss = pg.iteration(mu, sh, ss, eps, L, gen)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(iters):
-        mu, sh, ss = pg.iteration(mu, sh, ss, eps, L, gen)
-    e1.record()
-    torch.cuda.synchronize()
+    with torch.cuda.device(device):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(iters):
+            mu, sh, ss = pg.iteration(mu, sh, ss, eps, L, gen)
+        e1.record()
+        torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     return iters * (L + 1) / (ms / 1e3), ms / iters
 
@@ -517,7 +519,7 @@ def run_served(args, dist):
     gen_s = time.perf_counter() - t0
     rng = np.random.default_rng(args.seed + dist.rank)
     gaps = rng.exponential(1.0 / rate, size=args.steps) if np.isfinite(rate) else np.zeros(args.steps)
-    sv = d.Server(device=0, iterations_per_round=8, host_threads=4)
+    sv = d.Server(device=dist.local, iterations_per_round=8, host_threads=4)
     # warm-up jobs (untimed): library tables, pools, first graphs
     for i in range(args.warmup):
         sv.submit_volume(vols[i], hmc(i), wl["chains"])
