@@ -135,7 +135,7 @@ def _declare(L):
     L.dr_volume_destroy.argtypes = [vp]
     L.dr_volume_destroy.restype = None
     L.dr_chainset_create.argtypes = [vp, C.c_int, C.POINTER(HmcOpts), C.POINTER(vp)]
-    L.dr_chainset_config_get.argtypes = [vp, _ip, _ip, _dp]
+    L.dr_chainset_config_get.argtypes = [vp, _ip, _ip, _dp, _ip]
     L.dr_chainset_destroy.argtypes = [vp]
     L.dr_chainset_destroy.restype = None
     L.dr_step.argtypes = [vp, C.c_int]
@@ -153,6 +153,7 @@ def _declare(L):
                                     C.c_float, _ip, C.POINTER(C.c_int64), C.POINTER(_ip), C.POINTER(_ip),
                                     C.POINTER(_fp)]
     L.dr_debug_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
+    L.dr_debug_tc_layout.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp]
     L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
@@ -369,10 +370,12 @@ class MultiResParameters:
     PATHS = ("plane", "plane+prefetch", "lines")
 
     def config(self):
-        """The chain set's update path, kriging-product blocks per SM, and tuned iteration time (ms, 0 if untuned)."""
-        p, g, ms = C.c_int(0), C.c_int(0), C.c_double(0)
-        check(lib().dr_chainset_config_get(self.h, C.byref(p), C.byref(g), C.byref(ms)))
-        return dict(path=self.PATHS[p.value], blocks_per_sm=g.value, tuned_ms=ms.value)
+        """The chain set's update path, kriging-product blocks per SM, tuned iteration time (ms, 0 if untuned) and
+        whether the kriging products run on the tensor cores."""
+        p, g, ms, tc = C.c_int(0), C.c_int(0), C.c_double(0), C.c_int(0)
+        check(lib().dr_chainset_config_get(self.h, C.byref(p), C.byref(g), C.byref(ms), C.byref(tc)))
+        return dict(path=self.PATHS[p.value], blocks_per_sm=g.value, tuned_ms=ms.value,
+                    tensor_products=bool(tc.value))
 
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))
@@ -475,6 +478,33 @@ def time_kernel(chains, which, step=1, reps=20):
     b = np.zeros(1, np.float64)
     check(lib().dr_debug_time_kernel(chains.h, which, step, reps, _ptr(ms), _ptr(b)))
     return float(ms[0]), float(b[0])
+
+
+def zorder_keys(ijk):
+    """Z-order keys of integer coordinates (n x 3, 10 bits each), as the tensor-core products order tile rows."""
+    ijk = np.asarray(ijk, np.int64)
+    k = np.zeros(len(ijk), np.uint32)
+    for b in range(10):
+        for a in range(3):
+            k |= (((ijk[:, a] >> b) & 1) << (3 * b + a)).astype(np.uint32)
+    return k
+
+
+def tc_layout(rowptr, col, val, n_cols, keys, g_max):
+    """Host-only check of the tensor-core products' dense-tile layout (dr_debug_tc_layout): the dense matrix read
+    back from the tiles, and the layout's statistics (tiles, chunks, segments, CTAs, chunks covered once, rows
+    covered once, index tables consistent)."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    val = np.ascontiguousarray(val, np.float32)
+    keys = np.ascontiguousarray(keys, np.uint32)
+    n_rows = len(rowptr) - 1
+    dense = np.empty((n_rows, int(n_cols)), np.float32)
+    stats = np.zeros(7, np.int64)
+    check(lib().dr_debug_tc_layout(n_rows, int(n_cols), _ptr(rowptr), _ptr(col), _ptr(val), _ptr(keys), int(g_max),
+                                   _ptr(dense), _ptr(stats)))
+    return dense, dict(zip(("tiles", "chunks", "segments", "ctas", "chunks_once", "rows_once", "consistent"),
+                           (int(x) for x in stats)))
 
 
 def log_posterior_noalloc(data: MultiResData, mu_device_ptr: int, s_hr: float, s_sr: float):

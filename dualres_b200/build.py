@@ -17,8 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libdualres_b200.so")
 SOURCES = ["api.cu", "host_setup.cpp", "estimate.cpp"]
-DEPS = ["api.cu", "kernels.cu", "common.cuh", "fft.cuh", "tma.cuh", "mce.cuh", "drb.h", "host_setup.cpp",
-        "host_setup.h", "estimate.cpp", "estimate.h"]
+DEPS = ["api.cu", "kernels.cu", "common.cuh", "fft.cuh", "tma.cuh", "mce.cuh", "kriging.cuh", "umma.cuh",
+        "tc_products.cuh", "drb.h", "host_setup.cpp", "host_setup.h", "estimate.cpp", "estimate.h"]
 CLI = os.path.join(LIBDIR, "dualgpmf")
 CLI_SOURCES = ["dualgpmf.cpp", "nifti.cpp"]
 CLI_DEPS = CLI_SOURCES + ["nifti.h"]

@@ -22,6 +22,7 @@
 #include "../../include/dualres_b200.h"
 #include "host_setup.h"
 #include "kernels.cu"
+#include "tc_products.cuh"
 #include "mce.cuh"
 #include "kriging.cuh"
 #include "estimate.h"
@@ -62,6 +63,7 @@ struct DeviceTables {
   bool ready = false;
   int sms = 148;
   int tma_dyn_max = 0;  // dynamic shared memory available to the bulk-copy plane kernel
+  bool tc = false;      // the tensor-core kriging products fit this device's shared memory
   const float2* tw_f = nullptr;
   const double2* tw_d = nullptr;
 };
@@ -132,6 +134,13 @@ static DeviceTables& device_tables(int dev) {
     CK(cudaFuncSetAttribute(k_kriging_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
     CK(cudaFuncSetAttribute(k_spd_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
     CK(cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
+    int smax = 0;
+    for (int n = 16; n <= 256; n *= 2) smax = std::max(smax, tc_smem_bytes(n));
+    t.tc = optin >= smax;
+    if (t.tc) {
+      CK(cudaFuncSetAttribute(k_tc_product, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_finish_smem_bytes(256)));
+    }
   }
   t.ready = true;
   return t;
@@ -227,6 +236,13 @@ struct Volume {
   int64_t bytes = 0;
   const float2* tw_f = nullptr;
   const double2* tw_d = nullptr;
+  // Dense-tile form of W and W^T for the tensor-core products, built on first use by a chain set that can use
+  // it (tc_state 0: not built, 1: built, -1: unavailable).
+  std::mutex tc_mtx;
+  int tc_state = 0;
+  DevTcMatrix tc_w{}, tc_wt{};
+  int tc_max_segs = 0;
+  double tc_seconds = 0.0;
 
   template <class T>
   T* alloc(size_t n) {
@@ -549,6 +565,9 @@ struct Chainset {
   int path = 0;                 // 0 plane kernel, 1 plane kernel with bulk prefetch, 2 x-line kernel + y passes
   int grid = 8;                 // kriging-product blocks per SM
   double tuned_ms = 0.0;        // iteration time of the chosen configuration when it was tuned (0: not tuned)
+  bool tcp = false;             // kriging products on the tensor cores (dense tiles of the volume)
+  int tc_N = 0;                 // chains per tensor-core product (power of two >= C)
+  float* tc_partial = nullptr;  // [segments][tc_N][128] partial products
   bool tma = false;             // ... in the persistent bulk-copy kernel (E0 <= 64, fits shared memory)
   int tma_smem = 0, tma_grid = 0;
 
@@ -629,8 +648,27 @@ static void launch_spmv_dc(const DevVolume& v, const DevChains& ch, int NR, int 
   }
 }
 
+// W mu_D (w) or W^T rs on the tensor cores: the tile products into segment partials, then the per-tile sums and
+// the same epilogue as the CSR kernels.
+static void launch_tc(Chainset* S, int step, int sel, int chain_only, bool w) {
+  const Volume* V = S->vol;
+  const DevTcMatrix& M = w ? V->tc_w : V->tc_wt;
+  const int N = S->tc_N;
+  if (M.T > S->dc.maxblk || S->tc_partial == nullptr)
+    throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the tile count");
+  if (M.G > 0) {
+    k_tc_product<<<M.G, TC_THREADS, tc_smem_bytes(N), S->stream>>>(M, S->dc, V->dv.n_h, sel, w ? 0 : 1, N,
+                                                                   S->tc_partial);
+    CK_LAUNCH();
+  }
+  k_tc_finish<<<M.T, 256, tc_finish_smem_bytes(N), S->stream>>>(M, S->tc_partial, N, V->dv, S->dc, step, sel,
+                                                                chain_only, w ? 0 : 1);
+  CK_LAUNCH();
+}
+
 static void launch_spmv(Chainset* S, int step, int sel, int chain_only, bool w) {
-  launch_spmv_dc(S->vol->dv, S->dc, S->NR, step, sel, chain_only, w, S->stream);
+  if (S->tcp) launch_tc(S, step, sel, chain_only, w);
+  else launch_spmv_dc(S->vol->dv, S->dc, S->NR, step, sel, chain_only, w, S->stream);
 }
 
 static void launch_xline(Chainset* S, int step, int flags) {
@@ -775,6 +813,97 @@ static void init_chain_states(Chainset* S) {
 // Candidate update paths for an embedding: the fused plane kernel (square x/y
 // planes whose padded layout fits shared memory), the same with bulk prefetch
 // of the state planes, and the x-line kernel with separate y passes (always).
+// ---------------------------------------------------------------- tensor-core kriging products
+static void tc_upload(Volume* V, const TcPlanHost& P, const float* dval, int nnz, DevTcMatrix* M) {
+  cudaStream_t st = V->stream;
+  M->T = P.T;
+  M->G = P.G;
+  M->n_segs = (int)(P.segs.size() / 4);
+  M->tile_rows = V->upload(P.tile_rows);
+  M->chunk_cols = V->upload(P.chunk_cols);
+  M->segs = reinterpret_cast<const int4*>(V->upload(P.segs));
+  M->cta_seg_ptr = V->upload(P.cta_seg_ptr);
+  M->tile_seg_ptr = V->upload(P.tile_seg_ptr);
+  const size_t nblob = (size_t)P.chunks * 2 * TC_BLK;
+  float* blob = V->alloc<float>(nblob);
+  CK(cudaMemsetAsync(blob, 0, sizeof(float) * std::max<size_t>(nblob, 1), st));
+  if (nnz > 0) {
+    int* dest = nullptr;
+    const cudaError_t e = cudaMallocAsync(&dest, sizeof(int) * nnz, st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, "cudaMallocAsync (tile positions)");
+    CK(cudaMemcpyAsync(dest, P.dest.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+    k_tc_fill<<<cdiv_i(nnz, 256), 256, 0, st>>>(dval, dest, nnz, blob);
+    CK_LAUNCH();
+    CK(cudaFreeAsync(dest, st));
+  }
+  M->blob = blob;
+}
+
+// Builds the volume's dense tiles once; false when the tensor-core products are not available for it (no std-res
+// data, a device without the shared memory, or tiles that would take more than a quarter of the free memory).
+static bool volume_tc(Volume* V) {
+  std::lock_guard<std::mutex> lk(V->tc_mtx);
+  if (V->tc_state != 0) return V->tc_state > 0;
+  V->tc_state = -1;
+  const HostVolume& hv = V->hv;
+  const DevVolume& dv = V->dv;
+  const DeviceTables& dt = device_tables(V->device);
+  if (!dt.tc || dv.n_s == 0 || hv.w_col.empty() || hv.wt_col.empty()) return false;
+  const auto t0 = std::chrono::steady_clock::now();
+  CK(cudaSetDevice(V->device));
+  auto coords = [&](int flat, int* x, int* y, int* z) {
+    *x = flat % hv.E[0];
+    *y = (flat / hv.E[0]) % hv.E[1];
+    *z = flat / (hv.E[0] * hv.E[1]);
+  };
+  // W's rows are ordered by the centroid of the data voxels each std-res voxel is kriged from, W^T's by voxel
+  std::vector<uint32_t> kw(dv.n_s, 0), kt(dv.n_h, 0);
+  for (int r = 0; r < dv.n_s; r++) {
+    double sx = 0, sy = 0, sz = 0;
+    const int n = hv.w_rowptr[r + 1] - hv.w_rowptr[r];
+    for (int k = hv.w_rowptr[r]; k < hv.w_rowptr[r + 1]; k++) {
+      int x, y, z;
+      coords(hv.d_flat[hv.w_col[k]], &x, &y, &z);
+      sx += x;
+      sy += y;
+      sz += z;
+    }
+    if (n > 0) kw[r] = zorder_key((int)std::lround(sx / n), (int)std::lround(sy / n), (int)std::lround(sz / n));
+  }
+  for (int j = 0; j < dv.n_h; j++) {
+    int x, y, z;
+    coords(hv.d_flat[j], &x, &y, &z);
+    kt[j] = zorder_key(x, y, z);
+  }
+  TcPlanHost pw, pt;
+  if (!tc_plan(hv.w_rowptr, hv.w_col, kw, dt.sms, &pw) || !tc_plan(hv.wt_rowptr, hv.wt_col, kt, dt.sms, &pt))
+    return false;
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const double blob_bytes = (double)(pw.chunks + pt.chunks) * 2 * TC_BLK * 4;
+  if (blob_bytes > 0.25 * (double)fr) return false;
+  tc_upload(V, pw, dv.w_val, (int)hv.w_col.size(), &V->tc_w);
+  tc_upload(V, pt, dv.wt_val, (int)hv.wt_col.size(), &V->tc_wt);
+  V->tc_max_segs = std::max(V->tc_w.n_segs, V->tc_wt.n_segs);
+  CK(cudaStreamSynchronize(V->stream));
+  V->tc_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  V->tc_state = 1;
+  return true;
+}
+
+// Chains per tensor-core product: the smallest power of two >= C and >= 16 (0 when C is outside [16, 256]).
+static int tc_chains(int C) {
+  if (C < 16 || C > 256) return 0;
+  int n = 16;
+  while (n < C) n *= 2;
+  return n;
+}
+
+static bool tc_env_off() {
+  const char* e = std::getenv("DRB_TC_PRODUCTS");
+  return e && std::string(e) == "0";
+}
+
 struct PathOptions {
   bool plane = false, prefetch = false;
 };
@@ -790,8 +919,9 @@ static PathOptions path_options(const DevVolume& v, int device) {
 
 struct TuneChoice {
   int path = 0;      // 0 plane, 1 plane + prefetch, 2 x-line
-  int grid = 8;      // kriging-product blocks per SM
+  int grid = 8;      // kriging-product blocks per SM (CSR products)
   double ms = 0.0;   // measured milliseconds per iteration
+  int tc = 0;        // 1: kriging products on the tensor cores
 };
 
 static bool autotune_enabled() {
@@ -827,14 +957,16 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
     if (it != g_tune.end()) return it->second;
   }
   const PathOptions po = path_options(v, V->device);
+  const bool tc = tc_chains(C) > 0 && !tc_env_off() && volume_tc(V);
   std::vector<TuneChoice> cand;
   for (int path : {0, 1, 2}) {
     if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
     // wide chain sets share each W row across their chains and fill the GPU at 8 blocks/SM; narrower ones
     // may do better with fewer, longer-lived product blocks
-    if (C >= 32) cand.push_back(TuneChoice{path, 8, 0.0});
+    if (C >= 32) cand.push_back(TuneChoice{path, 8, 0.0, 0});
     else
-      for (int grid : {8, 4, 2}) cand.push_back(TuneChoice{path, grid, 0.0});
+      for (int grid : {8, 4, 2}) cand.push_back(TuneChoice{path, grid, 0.0, 0});
+    if (tc) cand.push_back(TuneChoice{path, 8, 0.0, 1});
   }
   TuneChoice best;
   best.ms = 1e300;
@@ -915,9 +1047,14 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   ch.Q = S->alloc<float2>((size_t)C * N);
   const PathOptions po = path_options(v, V->device);
   int path = po.plane ? 0 : 2, grid = 8;
+  // tensor-core products by default for 32 or more chains; the tuner, DRB_TC_PRODUCTS=0 / 1 and a forced choice
+  // override the default
+  int tc = C >= 32 ? 1 : 0;
+  if (const char* e = std::getenv("DRB_TC_PRODUCTS")) tc = std::atoi(e) != 0;
   if (forced) {
     path = forced->path;
     grid = forced->grid;
+    tc = forced->tc;
   } else if (std::getenv("DRB_NO_PLANE")) {
     path = 2;
   } else if (std::getenv("DRB_PLANE_PREFETCH")) {
@@ -926,6 +1063,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     const TuneChoice t = autotune(V, C, o);
     path = t.path;
     grid = t.grid;
+    if (!std::getenv("DRB_TC_PRODUCTS")) tc = t.tc;
     S->tuned_ms = t.ms;
   }
   if (!forced) {
@@ -954,6 +1092,13 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   const int wide = device_tables(V->device).sms * S->grid;
   ch.nb_w = std::max(1, std::min(v.n_s, wide));
   ch.nb_wt = std::max(1, std::min(cdiv_i(v.n_h, 8), wide));
+  S->tcp = tc && tc_chains(C) > 0 && volume_tc(V);
+  if (S->tcp) {
+    S->tc_N = tc_chains(C);
+    ch.nb_w = V->tc_w.T;
+    ch.nb_wt = V->tc_wt.T;
+    S->tc_partial = S->alloc<float>((size_t)std::max(V->tc_max_segs, 1) * S->tc_N * TC_M, false);
+  }
   ch.maxblk = std::max(ch.nb_x, std::max(ch.nb_w, ch.nb_wt));
   ch.part = S->alloc<double>((size_t)C * NSLOT * ch.maxblk);
   ch.st = S->alloc<ChainState>(C);
@@ -1034,6 +1179,7 @@ static void check_device_error(Chainset* S) {
   int err = 0;
   CK(cudaMemcpyAsync(&err, S->dc.err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
   CK(cudaStreamSynchronize(S->stream));
+  if (err == 3) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core kriging product pipeline)");
   if (err) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
 }
 
@@ -1272,12 +1418,14 @@ int dr_chainset_create(dr_volume* v, int n_chains, const dr_hmc_opts* opts, dr_c
 
 void dr_chainset_destroy(dr_chainset* s) { delete s; }
 
-int dr_chainset_config_get(const dr_chainset* s, int* path, int* blocks_per_sm, double* tuned_ms) {
+int dr_chainset_config_get(const dr_chainset* s, int* path, int* blocks_per_sm, double* tuned_ms,
+                           int* tensor_products) {
   API_BEGIN
   if (!s) throw Error(DR_ERR_INVALID, "NULL chain set");
   if (path) *path = s->path;
   if (blocks_per_sm) *blocks_per_sm = s->grid;
   if (tuned_ms) *tuned_ms = s->tuned_ms;
+  if (tensor_products) *tensor_products = s->tcp ? 1 : 0;
   API_END
 }
 
@@ -1550,6 +1698,61 @@ int dr_kriging_matrix(const float* hr, int nx, int ny, int nz, const float* Qhr,
 }
 
 void dr_free(void* p) { std::free(p); }
+
+int dr_debug_tc_layout(int n_rows, int n_cols, const int* rowptr, const int* col, const float* val,
+                       const uint32_t* keys, int g_max, float* dense, int64_t* stats) {
+  API_BEGIN
+  if (n_rows < 0 || n_cols < 0 || !rowptr || !keys || !dense || !stats || (rowptr[n_rows] > 0 && (!col || !val)))
+    throw Error(DR_ERR_INVALID, "bad argument");
+  const int nnz = rowptr[n_rows];
+  std::vector<int> rp(rowptr, rowptr + n_rows + 1), cl(col, col + nnz);
+  std::vector<uint32_t> ky(keys, keys + n_rows);
+  TcPlanHost P;
+  if (!tc_plan(rp, cl, ky, g_max, &P)) throw Error(DR_ERR_INVALID, "matrix too large for the tile layout");
+  std::vector<float> blob((size_t)P.chunks * 2 * TC_BLK, 0.f);
+  for (int i = 0; i < nnz; i++) {
+    uint32_t u;
+    std::memcpy(&u, &val[i], 4);
+    u &= 0xFFFFE000u;
+    float h;
+    std::memcpy(&h, &u, 4);
+    blob[P.dest[i]] = h;
+    blob[P.dest[i] + TC_BLK] = val[i] - h;
+  }
+  std::fill(dense, dense + (size_t)n_rows * n_cols, 0.f);
+  const int nseg = (int)(P.segs.size() / 4);
+  std::vector<int> chunk_seen(P.chunks, 0), row_seen(n_rows, 0);
+  for (int g = 0; g < nseg; g++) {
+    const int t = P.segs[4 * g];
+    for (int c = P.segs[4 * g + 1]; c < P.segs[4 * g + 2]; c++) {
+      chunk_seen[c]++;
+      for (int m = 0; m < TC_M; m++) {
+        const int row = P.tile_rows[(size_t)t * TC_M + m];
+        for (int kk = 0; kk < TC_KC; kk++) {
+          const int cc = P.chunk_cols[(size_t)c * TC_KC + kk];
+          const size_t off = (size_t)c * 2 * TC_BLK + (kk / 4) * (TC_M * 4) + m * 4 + kk % 4;
+          if (row >= 0 && cc >= 0) dense[(size_t)row * n_cols + cc] += blob[off] + blob[off + TC_BLK];
+          else if (blob[off] != 0.f || blob[off + TC_BLK] != 0.f) dense[0] = NAN;  // padding must stay zero
+        }
+      }
+    }
+  }
+  for (int r : P.tile_rows)
+    if (r >= 0) row_seen[r]++;
+  bool consistent = P.tile_seg_ptr.size() == (size_t)P.T + 1 && P.tile_seg_ptr[P.T] == nseg &&
+                    P.cta_seg_ptr.size() == (size_t)P.G + 1 && P.cta_seg_ptr[P.G] == nseg;
+  for (int t = 0; consistent && t < P.T; t++)
+    for (int g = P.tile_seg_ptr[t]; g < P.tile_seg_ptr[t + 1]; g++) consistent = consistent && P.segs[4 * g] == t;
+  for (int b = 0; consistent && b < P.G; b++) consistent = P.cta_seg_ptr[b] < P.cta_seg_ptr[b + 1];
+  stats[0] = P.T;
+  stats[1] = P.chunks;
+  stats[2] = nseg;
+  stats[3] = P.G;
+  stats[4] = std::count(chunk_seen.begin(), chunk_seen.end(), 1);
+  stats[5] = std::count(row_seen.begin(), row_seen.end(), 1);
+  stats[6] = consistent ? 1 : 0;
+  API_END
+}
 
 int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* avg_ms, double* algo_bytes) {
   API_BEGIN

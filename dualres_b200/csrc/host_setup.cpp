@@ -514,6 +514,80 @@ void build_transpose(HostVolume* hv) {
     }
 }
 
+uint32_t zorder_key(int x, int y, int z) {
+  uint32_t k = 0;
+  for (int b = 0; b < 10; b++)
+    k |= ((uint32_t)((x >> b) & 1) << (3 * b)) | ((uint32_t)((y >> b) & 1) << (3 * b + 1)) |
+         ((uint32_t)((z >> b) & 1) << (3 * b + 2));
+  return k;
+}
+
+bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const std::vector<uint32_t>& key, int g_max,
+             TcPlanHost* P) {
+  constexpr int M = 128, KC = 32, BLK = M * KC;
+  const int R = (int)rowptr.size() - 1;
+  std::vector<int> order(R);
+  for (int i = 0; i < R; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+  P->T = (R + M - 1) / M;
+  P->tile_rows.assign((size_t)P->T * M, -1);
+  for (int i = 0; i < R; i++) P->tile_rows[i] = order[i];
+  std::vector<long long> chunk_ptr(P->T + 1, 0);
+  std::vector<std::vector<int>> uni(P->T);
+  for (int t = 0; t < P->T; t++) {
+    std::vector<int>& u = uni[t];
+    for (int m = 0; m < M; m++) {
+      const int r = P->tile_rows[(size_t)t * M + m];
+      if (r >= 0) u.insert(u.end(), col.begin() + rowptr[r], col.begin() + rowptr[r + 1]);
+    }
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    chunk_ptr[t + 1] = chunk_ptr[t] + (long long)(u.size() + KC - 1) / KC;
+  }
+  P->chunks = chunk_ptr[P->T];
+  if (P->chunks * 2 * BLK > 0x7fffffffLL) return false;
+  P->chunk_cols.assign((size_t)P->chunks * KC, -1);
+  P->dest.assign(col.size(), -1);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int t = 0; t < P->T; t++) {
+    const std::vector<int>& u = uni[t];
+    std::copy(u.begin(), u.end(), P->chunk_cols.begin() + chunk_ptr[t] * KC);
+    for (int m = 0; m < M; m++) {
+      const int r = P->tile_rows[(size_t)t * M + m];
+      if (r < 0) continue;
+      for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
+        const long long pos = std::lower_bound(u.begin(), u.end(), col[k]) - u.begin();
+        const long long q = chunk_ptr[t] + pos / KC;
+        const int kk = (int)(pos % KC);
+        P->dest[k] = (int)(q * 2 * BLK + (kk / 4) * (M * 4) + m * 4 + kk % 4);
+      }
+    }
+  }
+  const long long Q = P->chunks;
+  P->G = Q == 0 ? 0 : (int)std::min<long long>(Q, std::max(1, g_max));
+  P->segs.clear();
+  P->cta_seg_ptr.assign(P->G + 1, 0);
+  int t = 0;
+  for (int b = 0; b < P->G; b++) {
+    long long c0 = Q * b / P->G;
+    const long long c1 = Q * (b + 1) / P->G;
+    while (c0 < c1) {
+      while (chunk_ptr[t + 1] <= c0) t++;
+      const long long e = std::min(c1, chunk_ptr[t + 1]);
+      P->segs.insert(P->segs.end(), {t, (int)c0, (int)e, 0});
+      c0 = e;
+    }
+    P->cta_seg_ptr[b + 1] = (int)(P->segs.size() / 4);
+  }
+  const int ns = (int)(P->segs.size() / 4);
+  P->tile_seg_ptr.assign(P->T + 1, ns);
+  for (int tt = P->T - 1, g = ns - 1; tt >= 0; tt--) {
+    while (g >= 0 && P->segs[4 * g] >= tt) g--;
+    P->tile_seg_ptr[tt] = g + 1;
+  }
+  return true;
+}
+
 int host_prepare(const dr_volume_desc* d, HostVolume* hv, std::string* err, bool defer_kriging) {
   if (!d || !d->highres || !d->qform_hr || d->nx <= 0 || d->ny <= 0 || d->nz <= 0) {
     *err = "dr_volume_create: highres image and qform are required";

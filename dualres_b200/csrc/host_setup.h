@@ -80,4 +80,23 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
                   const float* Qsr, const float* theta, float radius, std::vector<int>* rowptr, std::vector<int>* col,
                   std::vector<float>* val, int* n_offsets, std::string* err);
 
+// Host part of a dense-tile plan for the tensor-core kriging products: rows
+// ordered along the Z-order curve of their keys (3 x 10-bit coordinates) and
+// cut into tiles of 128; the sorted union of each tile's columns cut into
+// chunks of 32; dest[k] = the blob position of nonzero k's TF32 high part
+// (element (m, kk) of chunk q at q * 8192 + (kk / 4) * 512 + m * 4 + kk % 4,
+// the remainder 4096 floats further).  The chunks are split into at most
+// g_max equal ranges, one per CTA, and the ranges at tile boundaries into
+// segments {tile, first chunk, end chunk, 0}, ordered by chunk.
+struct TcPlanHost {
+  int T = 0, G = 0;
+  long long chunks = 0;
+  std::vector<int> tile_rows, chunk_cols, segs, cta_seg_ptr, tile_seg_ptr, dest;
+};
+// false when the blob would not be addressable with 32-bit positions.
+bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const std::vector<uint32_t>& key, int g_max,
+             TcPlanHost* P);
+// Z-order key of integer voxel coordinates (10 bits each).
+uint32_t zorder_key(int x, int y, int z);
+
 }  // namespace drb

@@ -1,0 +1,296 @@
+// Kriging products on the 5th-generation tensor cores.
+//
+// W mu_D and W^T rs for all chains of a chain set are dense GEMMs once W is cut
+// into tiles of 128 spatially adjacent rows: the union of a tile's columns is a
+// few times its nonzero count (about 6x for W and 3x for W^T on a 32^3 volume
+// at a 6.9 mm neighbourhood), so the tile is stored dense and multiplied on the
+// tensor cores, D[128 x N] = A[128 x K] B[K x N] with N = chains (padded to a
+// power of two >= 16).
+//
+// Precision: each FP32 operand is split as x = hi + lo (hi = the TF32 bits of
+// x, lo = x - hi, exact), and D accumulates hi_A hi_B + hi_A lo_B + lo_A hi_B
+// in FP32 (three kind::tf32 MMAs per K step), which keeps about 21 bits of
+// every product -- the FP32 CSR products' accuracy, not TF32's.  A's split is
+// made once per volume (the blob); B's while it is gathered.
+//
+// k_tc_product: one CTA per SM over a contiguous range of chunks (32 columns
+// of one tile).  Warp roles:
+//   warp 0     one thread bulk-copies the chunk's A blocks (32 KB) into the
+//              stage (mbarrier transaction count);
+//   warp 1     allocates TMEM; one thread issues the MMAs of a chunk when both
+//              its A and B are in, then commits the stage back to the
+//              producers; at a tile boundary it commits the accumulator;
+//   warps 2-5  gather the chunk's chain vectors X[col][chain] (coalesced over
+//              chains), split them and write hi / lo in the K-major layout;
+//   warps 6-9  epilogue: TMEM -> registers -> the segment's partial slot.
+// Every mbarrier wait is bounded; a wait that gives up records 3 in ch.err,
+// the roles drain their copies and MMAs, and TMEM is released.
+//
+// k_tc_finish: one block per tile sums the tile's segment partials in segment
+// order (deterministic), then applies the product's epilogue exactly as the
+// CSR kernels k_spmv_w / k_spmv_wt do: rs = Ys - W mu_D with the ||rs||^2
+// partials, or gD = sigma_h^-2 (Yh - mu_D) + sigma_s^-2 W^T rs with the
+// ||Yh - mu_D||^2 partials (MultiResParameters.h:357-364).
+#pragma once
+
+#include "drb.h"
+#include "umma.cuh"
+
+namespace drb {
+
+constexpr int TC_M = 128;               // tile rows (MMA M)
+constexpr int TC_KC = 32;               // columns per chunk
+constexpr int TC_BLK = TC_M * TC_KC;    // floats in one block (hi or lo) of a chunk
+constexpr int TC_THREADS = 320;
+constexpr int TC_HDR = 4096;            // barriers, TMEM address, chain offsets
+
+__host__ __device__ inline int tc_stages(int N) { return N <= 64 ? 4 : (N <= 128 ? 3 : 2); }
+__host__ __device__ inline int tc_stage_bytes(int N) { return 2 * TC_BLK * 4 + 2 * N * TC_KC * 4; }
+__host__ __device__ inline int tc_smem_bytes(int N) { return TC_HDR + tc_stages(N) * tc_stage_bytes(N); }
+__host__ __device__ inline int tc_finish_smem_bytes(int N) { return N * (TC_M + 1) * 4 + 256 * 8; }
+
+// mode 0: X = mu_D (each chain's accepted half xor sel), mode 1: X = rs.  N: chains, a power of two in [16, 256].
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_product(DevTcMatrix A, DevChains ch, int n_h, int sel, int mode, int N, float* __restrict__ partial) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  uint64_t* fullA = reinterpret_cast<uint64_t*>(tsm);
+  uint64_t* fullB = fullA + 4;
+  uint64_t* empty = fullA + 8;
+  uint64_t* accf = fullA + 12;
+  uint64_t* acce = fullA + 13;
+  uint64_t* done = fullA + 14;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tsm + 128);
+  long long* xoff = reinterpret_cast<long long*>(tsm + 256);
+  unsigned char* stage0 = tsm + TC_HDR;
+  const int stages = tc_stages(N), sbytes = tc_stage_bytes(N);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int seg0 = A.cta_seg_ptr[blockIdx.x], seg1 = A.cta_seg_ptr[blockIdx.x + 1];
+  const uint32_t ncols = N < 32 ? 32 : N;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; s++) {
+      mbar_init(fullA + s, 1);
+      mbar_init(fullB + s, 128);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(accf, 1);
+    mbar_init(acce, 128);
+    mbar_init(done, 1);
+    mbar_fence_init();
+  }
+  for (int n = threadIdx.x; n < N; n += TC_THREADS) {
+    long long o = -1;
+    if (n < ch.C) o = mode == 0 ? (long long)(ch.st[n].acc ^ sel) * n_h * ch.Cp + n : (long long)n;
+    xoff[n] = o;
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, ncols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int q = 0;
+      for (int g = seg0; g < seg1 && ok; g++) {
+        const int4 sg = A.segs[g];
+        for (int c = sg.y; c < sg.z; c++, q++) {
+          const int s = q % stages;
+          if (q >= stages && !mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(fullA + s, 2 * TC_BLK * 4);
+          bulk_g2s(stage0 + s * sbytes, A.blob + (long long)c * 2 * TC_BLK, 2 * TC_BLK * 4, fullA + s);
+        }
+      }
+      // the copies still in flight land before the CTA may exit
+      for (int r = q - stages < 0 ? 0 : q - stages; r < q; r++) mbar_wait_bounded(fullA + r % stages, (r / stages) & 1);
+      if (!ok) atomicExch(ch.err, 3);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_tf32(TC_M, N);
+      const uint32_t lbo_b = 16u * N;
+      int q = 0;
+      for (int g = seg0; g < seg1 && ok; g++) {
+        const int4 sg = A.segs[g];
+        if (g > seg0) {  // the epilogue has read the previous segment's accumulator
+          if (!mbar_wait_bounded(acce, (g - seg0 - 1) & 1)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+        }
+        uint32_t accum = 0;
+        for (int c = sg.y; c < sg.z; c++, q++) {
+          const int s = q % stages;
+          const uint32_t par = (q / stages) & 1;
+          if (!mbar_wait_bounded(fullA + s, par) || !mbar_wait_bounded(fullB + s, par)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a = smem_addr(stage0 + s * sbytes);
+          const uint32_t b = a + 2 * TC_BLK * 4;
+          const uint32_t bl = b + N * TC_KC * 4;
+#pragma unroll
+          for (int ks = 0; ks < TC_KC / 8; ks++) {
+            // A block: element (m, k) at float (k/4)*512 + m*4 + k%4 -> K step ks starts 4096 B further;
+            // LBO (next 4 k) 2048 B, SBO (next 8 rows) 128 B.  B block: (n, k) at (k/4)*4N + n*4 + k%4.
+            const uint64_t ahi = sdesc_kmajor(a + ks * 4096, 2048, 128);
+            const uint64_t alo = sdesc_kmajor(a + TC_BLK * 4 + ks * 4096, 2048, 128);
+            const uint64_t bhi = sdesc_kmajor(b + ks * 32 * N, lbo_b, 128);
+            const uint64_t blo = sdesc_kmajor(bl + ks * 32 * N, lbo_b, 128);
+            umma_tf32(tmem, ahi, bhi, idesc, accum);
+            umma_tf32(tmem, ahi, blo, idesc, 1u);
+            umma_tf32(tmem, alo, bhi, idesc, 1u);
+            accum = 1u;
+          }
+          umma_commit(empty + s);
+        }
+        if (!ok) break;
+        umma_commit(accf);
+      }
+      umma_commit(done);
+      mbar_wait_bounded(done, 0);
+      if (!ok) atomicExch(ch.err, 3);
+    }
+  } else if (warp < 6) {
+    const int t = threadIdx.x - 64;
+    const long long Cp = ch.Cp;
+    const float* __restrict__ X = mode == 0 ? ch.muD : ch.rs;
+    int q = 0;
+    for (int g = seg0; g < seg1 && ok; g++) {
+      const int4 sg = A.segs[g];
+      for (int c = sg.y; c < sg.z; c++, q++) {
+        const int s = q % stages;
+        if (q >= stages && !mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1)) {
+          ok = false;
+          break;
+        }
+        float4* bh = reinterpret_cast<float4*>(stage0 + s * sbytes + 2 * TC_BLK * 4);
+        float4* bl = bh + N * (TC_KC / 4);
+        const int4* cols = reinterpret_cast<const int4*>(A.chunk_cols + (long long)c * TC_KC);
+#pragma unroll 4
+        for (int idx = t; idx < N * (TC_KC / 4); idx += 128) {
+          const int n = idx & (N - 1), kc4 = idx / N;
+          const long long o = xoff[n];
+          const int4 j = cols[kc4];
+          float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
+          if (o >= 0) {
+            if (j.x >= 0) x0 = X[o + j.x * Cp];
+            if (j.y >= 0) x1 = X[o + j.y * Cp];
+            if (j.z >= 0) x2 = X[o + j.z * Cp];
+            if (j.w >= 0) x3 = X[o + j.w * Cp];
+          }
+          const float4 h = make_float4(tf32_hi(x0), tf32_hi(x1), tf32_hi(x2), tf32_hi(x3));
+          bh[kc4 * N + n] = h;
+          bl[kc4 * N + n] = make_float4(x0 - h.x, x1 - h.y, x2 - h.z, x3 - h.w);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(fullB + s);
+      }
+    }
+    if (!ok) atomicExch(ch.err, 3);
+  } else {
+    const int quarter = warp & 3;
+    const int m = 32 * quarter + lane;
+    for (int g = seg0; g < seg1; g++) {
+      // the TMEM loads below are warp-collective: the warp goes on only if every lane saw the accumulator
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(accf, (g - seg0) & 1))) {
+        if (lane == 0) atomicExch(ch.err, 3);
+        break;
+      }
+      tc_fence_after();
+      float* P = partial + (long long)g * N * TC_M + m;
+      for (int cb = 0; cb < N / 16; cb++) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(16 * cb), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; i++) P[(long long)(16 * cb + i) * TC_M] = v[i];
+      }
+      tc_fence_before();
+      mbar_arrive(acce);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, ncols);
+  }
+}
+
+// Sums tile blockIdx.x's segment partials and applies the product's epilogue (mode 0: W, mode 1: W^T).
+__global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* __restrict__ partial, int N, DevVolume v,
+                                                   DevChains ch, int step, int sel, int chain_only, int mode) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  float* S = reinterpret_cast<float*>(fsm);
+  double* red = reinterpret_cast<double*>(fsm + (size_t)N * (TC_M + 1) * 4);
+  const int t = blockIdx.x;
+  const int s0 = A.tile_seg_ptr[t], s1 = A.tile_seg_ptr[t + 1];
+  for (int e = threadIdx.x; e < N * TC_M; e += 256) {
+    float acc = 0.f;
+    for (int g = s0; g < s1; g++) acc += partial[(long long)g * N * TC_M + e];
+    S[(e / TC_M) * (TC_M + 1) + e % TC_M] = acc;
+  }
+  __syncthreads();
+  const int n = threadIdx.x & (N - 1);
+  const int m0 = threadIdx.x / N, dm = 256 / N;
+  bool act = n < ch.C && (chain_only < 0 || n == chain_only);
+  if (act) act = step < 0 || step <= ch.st[n].L_cur;
+  double sq = 0.0;
+  if (act) {
+    const long long Cp = ch.Cp;
+    const float* Sn = S + n * (TC_M + 1);
+    const int* rows = A.tile_rows + (long long)t * TC_M;
+    if (mode == 0) {
+      for (int m = m0; m < TC_M; m += dm) {
+        const int row = rows[m];
+        if (row < 0) continue;
+        const float r = v.Ys[row] - Sn[m];
+        ch.rs[row * Cp + n] = r;
+        sq += (double)r * r;
+      }
+    } else {
+      const ChainState& st = ch.st[n];
+      const float* mu = ch.muD + (long long)(st.acc ^ sel) * v.n_h * Cp + n;
+      const float sh = st.sh, ss = st.ss;
+      for (int m = m0; m < TC_M; m += dm) {
+        const int row = rows[m];
+        if (row < 0) continue;
+        const float rh = v.Yh[row] - mu[row * Cp];
+        ch.gD[row * Cp + n] = sh * rh + ss * Sn[m];
+        sq += (double)rh * rh;
+      }
+    }
+  }
+  red[threadIdx.x] = sq;
+  __syncthreads();
+  if ((int)threadIdx.x < N && act) {
+    double s = 0.0;
+    for (int k = 0; k < dm; k++) s += red[k * N + n];
+    const int L = ch.st[n].L_cur;
+    const int slot = mode == 0 ? (step <= 0 ? SL_RS0 : (step == L ? SL_RSL : SL_SCRATCH))
+                               : (step <= 0 ? SL_RH0 : (step == L ? SL_RHL : SL_SCRATCH));
+    ch.part[((long long)n * NSLOT + slot) * ch.maxblk + t] = s;
+  }
+}
+
+// Builds the dense blob from the CSR values: hi at dest[k], lo at dest[k] + 128 * 32 (the blob is zeroed first).
+__global__ void k_tc_fill(const float* __restrict__ val, const int* __restrict__ dest, int nnz, float* __restrict__ blob) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  const float x = val[k];
+  const float h = tf32_hi(x);
+  blob[dest[k]] = h;
+  blob[dest[k] + TC_BLK] = x - h;
+}
+
+}  // namespace drb
