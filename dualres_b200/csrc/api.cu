@@ -138,8 +138,11 @@ static DeviceTables& device_tables(int dev) {
     for (int n = 16; n <= 256; n *= 2) smax = std::max(smax, tc_smem_bytes(n));
     t.tc = optin >= smax;
     if (t.tc) {
-      CK(cudaFuncSetAttribute(k_tc_product, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-      CK(cudaFuncSetAttribute(k_tc_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_finish_smem_bytes(256)));
+      CK(cudaFuncSetAttribute(k_tc_product<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
     }
   }
   t.ready = true;
@@ -654,15 +657,30 @@ static void launch_tc(Chainset* S, int step, int sel, int chain_only, bool w) {
   const Volume* V = S->vol;
   const DevTcMatrix& M = w ? V->tc_w : V->tc_wt;
   const int N = S->tc_N;
-  if (M.T > S->dc.maxblk || S->tc_partial == nullptr)
-    throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the tile count");
+  const int nfin = tc_finish_blocks(M.T);
+  if (nfin > S->dc.maxblk || S->tc_partial == nullptr)
+    throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the finishing block count");
   if (M.G > 0) {
-    k_tc_product<<<M.G, TC_THREADS, tc_smem_bytes(N), S->stream>>>(M, S->dc, V->dv.n_h, sel, w ? 0 : 1, N,
-                                                                   S->tc_partial);
+    const int n_h = V->dv.n_h, mode = w ? 0 : 1;
+    const size_t sm = tc_smem_bytes(N);
+    switch (N) {
+      case 16: k_tc_product<16><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
+      case 32: k_tc_product<32><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
+      case 64: k_tc_product<64><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
+      case 128: k_tc_product<128><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
+      default: k_tc_product<256><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
+    }
     CK_LAUNCH();
   }
-  k_tc_finish<<<M.T, 256, tc_finish_smem_bytes(N), S->stream>>>(M, S->tc_partial, N, V->dv, S->dc, step, sel,
-                                                                chain_only, w ? 0 : 1);
+  const size_t fs = tc_finish_smem_bytes(N);
+  const int fm = w ? 0 : 1;
+  switch (N) {
+    case 16: k_tc_finish<16><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 32: k_tc_finish<32><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 64: k_tc_finish<64><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 128: k_tc_finish<128><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    default: k_tc_finish<256><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+  }
   CK_LAUNCH();
 }
 
@@ -1095,8 +1113,8 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   S->tcp = tc && tc_chains(C) > 0 && volume_tc(V);
   if (S->tcp) {
     S->tc_N = tc_chains(C);
-    ch.nb_w = V->tc_w.T;
-    ch.nb_wt = V->tc_wt.T;
+    ch.nb_w = tc_finish_blocks(V->tc_w.T);
+    ch.nb_wt = tc_finish_blocks(V->tc_wt.T);
     S->tc_partial = S->alloc<float>((size_t)std::max(V->tc_max_segs, 1) * S->tc_N * TC_M, false);
   }
   ch.maxblk = std::max(ch.nb_x, std::max(ch.nb_w, ch.nb_wt));

@@ -20,14 +20,16 @@
 //   warp 1     allocates TMEM; one thread issues the MMAs of a chunk when both
 //              its A and B are in, then commits the stage back to the
 //              producers; at a tile boundary it commits the accumulator;
-//   warps 2-5  gather the chunk's chain vectors X[col][chain] (coalesced over
-//              chains), split them and write hi / lo in the K-major layout;
-//   warps 6-9  epilogue: TMEM -> registers -> the segment's partial slot.
+//   warps 2-9  two gather groups of 4 warps, each taking every other chunk:
+//              the chunk's chain vectors X[col][chain] (coalesced over
+//              chains) are loaded -- all of a thread's loads before any is
+//              used -- split, and written as hi / lo in the K-major layout;
+//   warps 10-13 epilogue: TMEM -> registers -> the segment's partial slot.
 // Every mbarrier wait is bounded; a wait that gives up records 3 in ch.err,
 // the roles drain their copies and MMAs, and TMEM is released.
 //
-// k_tc_finish: one block per tile sums the tile's segment partials in segment
-// order (deterministic), then applies the product's epilogue exactly as the
+// k_tc_finish: one block per 16 rows of a tile sums the tile's segment
+// partials in segment order (deterministic), then applies the epilogue as the
 // CSR kernels k_spmv_w / k_spmv_wt do: rs = Ys - W mu_D with the ||rs||^2
 // partials, or gD = sigma_h^-2 (Yh - mu_D) + sigma_s^-2 W^T rs with the
 // ||Yh - mu_D||^2 partials (MultiResParameters.h:357-364).
@@ -41,17 +43,18 @@ namespace drb {
 constexpr int TC_M = 128;               // tile rows (MMA M)
 constexpr int TC_KC = 32;               // columns per chunk
 constexpr int TC_BLK = TC_M * TC_KC;    // floats in one block (hi or lo) of a chunk
-constexpr int TC_THREADS = 320;
+constexpr int TC_GROUPS = 2;            // gather groups (chunks in flight in the gather)
+constexpr int TC_THREADS = 32 * (2 + 4 * TC_GROUPS + 4);
 constexpr int TC_HDR = 4096;            // barriers, TMEM address, chain offsets
 
 __host__ __device__ inline int tc_stages(int N) { return N <= 64 ? 4 : (N <= 128 ? 3 : 2); }
 __host__ __device__ inline int tc_stage_bytes(int N) { return 2 * TC_BLK * 4 + 2 * N * TC_KC * 4; }
 __host__ __device__ inline int tc_smem_bytes(int N) { return TC_HDR + tc_stages(N) * tc_stage_bytes(N); }
-__host__ __device__ inline int tc_finish_smem_bytes(int N) { return N * (TC_M + 1) * 4 + 256 * 8; }
 
 // mode 0: X = mu_D (each chain's accepted half xor sel), mode 1: X = rs.  N: chains, a power of two in [16, 256].
+template <int N>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_tc_product(DevTcMatrix A, DevChains ch, int n_h, int sel, int mode, int N, float* __restrict__ partial) {
+    k_tc_product(DevTcMatrix A, DevChains ch, int n_h, int sel, int mode, float* __restrict__ partial) {
   extern __shared__ __align__(1024) unsigned char tsm[];
   uint64_t* fullA = reinterpret_cast<uint64_t*>(tsm);
   uint64_t* fullB = fullA + 4;
@@ -160,14 +163,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       mbar_wait_bounded(done, 0);
       if (!ok) atomicExch(ch.err, 3);
     }
-  } else if (warp < 6) {
-    const int t = threadIdx.x - 64;
+  } else if (warp < 2 + 4 * TC_GROUPS) {
+    constexpr int NI = N * (TC_KC / 4) / 128;  // (chain, 4 columns) pairs per thread and chunk
+    const int grp = (warp - 2) / 4, t = threadIdx.x - 64 - 128 * grp;
     const long long Cp = ch.Cp;
     const float* __restrict__ X = mode == 0 ? ch.muD : ch.rs;
     int q = 0;
     for (int g = seg0; g < seg1 && ok; g++) {
       const int4 sg = A.segs[g];
       for (int c = sg.y; c < sg.z; c++, q++) {
+        if (q % TC_GROUPS != grp) continue;
         const int s = q % stages;
         if (q >= stages && !mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1)) {
           ok = false;
@@ -176,21 +181,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         float4* bh = reinterpret_cast<float4*>(stage0 + s * sbytes + 2 * TC_BLK * 4);
         float4* bl = bh + N * (TC_KC / 4);
         const int4* cols = reinterpret_cast<const int4*>(A.chunk_cols + (long long)c * TC_KC);
-#pragma unroll 4
-        for (int idx = t; idx < N * (TC_KC / 4); idx += 128) {
+        float xv[NI][4];
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+          const int idx = t + 128 * i;
           const int n = idx & (N - 1), kc4 = idx / N;
           const long long o = xoff[n];
-          const int4 j = cols[kc4];
-          float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
-          if (o >= 0) {
-            if (j.x >= 0) x0 = X[o + j.x * Cp];
-            if (j.y >= 0) x1 = X[o + j.y * Cp];
-            if (j.z >= 0) x2 = X[o + j.z * Cp];
-            if (j.w >= 0) x3 = X[o + j.w * Cp];
-          }
-          const float4 h = make_float4(tf32_hi(x0), tf32_hi(x1), tf32_hi(x2), tf32_hi(x3));
+          const int4 j = __ldg(cols + kc4);
+          const bool on = o >= 0;
+          xv[i][0] = (on && j.x >= 0) ? __ldg(X + o + j.x * Cp) : 0.f;
+          xv[i][1] = (on && j.y >= 0) ? __ldg(X + o + j.y * Cp) : 0.f;
+          xv[i][2] = (on && j.z >= 0) ? __ldg(X + o + j.z * Cp) : 0.f;
+          xv[i][3] = (on && j.w >= 0) ? __ldg(X + o + j.w * Cp) : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+          const int idx = t + 128 * i;
+          const int n = idx & (N - 1), kc4 = idx / N;
+          const float4 h = make_float4(tf32_hi(xv[i][0]), tf32_hi(xv[i][1]), tf32_hi(xv[i][2]), tf32_hi(xv[i][3]));
           bh[kc4 * N + n] = h;
-          bl[kc4 * N + n] = make_float4(x0 - h.x, x1 - h.y, x2 - h.z, x3 - h.w);
+          bl[kc4 * N + n] = make_float4(xv[i][0] - h.x, xv[i][1] - h.y, xv[i][2] - h.z, xv[i][3] - h.w);
         }
         fence_proxy_async_smem();
         mbar_arrive(fullB + s);
@@ -227,31 +237,62 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   }
 }
 
-// Sums tile blockIdx.x's segment partials and applies the product's epilogue (mode 0: W, mode 1: W^T).
-__global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* __restrict__ partial, int N, DevVolume v,
+// Sums the segment partials of TC_FR rows of one tile and applies the product's epilogue (mode 0: W, mode 1: W^T).
+// Block (tile t, row group r) = blockIdx.x = t * (128 / TC_FR) + r; its per-chain squared-residual sums go to
+// partial-sum slot blockIdx.x.  Phase 1 reads the partials coalesced along rows (all segment loads of a thread's
+// elements in flight together) and sums them in segment order; phase 2 works along chains, so that mu_D, rs and
+// gD are read and written coalesced.
+constexpr int TC_FR = 16;  // tile rows per finishing block
+__host__ __device__ inline int tc_finish_blocks(int T) { return T * (TC_M / TC_FR); }
+__host__ __device__ inline int tc_finish_smem_bytes(int N) { return N * (TC_FR + 1) * 4 + 256 * 8; }
+
+template <int N>
+__global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* __restrict__ partial, DevVolume v,
                                                    DevChains ch, int step, int sel, int chain_only, int mode) {
+  constexpr int EPT = N * TC_FR / 256;  // elements per thread (N >= 16)
   extern __shared__ __align__(16) unsigned char fsm[];
   float* S = reinterpret_cast<float*>(fsm);
-  double* red = reinterpret_cast<double*>(fsm + (size_t)N * (TC_M + 1) * 4);
-  const int t = blockIdx.x;
+  double* red = reinterpret_cast<double*>(fsm + (size_t)N * (TC_FR + 1) * 4);
+  const int t = blockIdx.x / (TC_M / TC_FR), m0 = (blockIdx.x % (TC_M / TC_FR)) * TC_FR;
   const int s0 = A.tile_seg_ptr[t], s1 = A.tile_seg_ptr[t + 1];
-  for (int e = threadIdx.x; e < N * TC_M; e += 256) {
-    float acc = 0.f;
-    for (int g = s0; g < s1; g++) acc += partial[(long long)g * N * TC_M + e];
-    S[(e / TC_M) * (TC_M + 1) + e % TC_M] = acc;
+  {
+    // element i of this thread: row m0 + mi, chain ni (rows fastest across the warp)
+    const int mi = threadIdx.x % TC_FR, nb = threadIdx.x / TC_FR;
+    float acc[EPT];
+#pragma unroll
+    for (int i = 0; i < EPT; i++) acc[i] = 0.f;
+    const float* P = partial + (long long)s0 * N * TC_M + m0 + mi;
+    int g = s0;
+    for (; g + 1 < s1; g += 2, P += 2LL * N * TC_M) {
+      float x0[EPT], x1[EPT];
+#pragma unroll
+      for (int i = 0; i < EPT; i++) {
+        const int ni = nb + (256 / TC_FR) * i;
+        x0[i] = __ldg(P + (long long)ni * TC_M);
+        x1[i] = __ldg(P + (long long)N * TC_M + (long long)ni * TC_M);
+      }
+#pragma unroll
+      for (int i = 0; i < EPT; i++) acc[i] = (acc[i] + x0[i]) + x1[i];
+    }
+    if (g < s1) {
+#pragma unroll
+      for (int i = 0; i < EPT; i++) acc[i] += __ldg(P + (long long)(nb + (256 / TC_FR) * i) * TC_M);
+    }
+#pragma unroll
+    for (int i = 0; i < EPT; i++) S[(nb + (256 / TC_FR) * i) * (TC_FR + 1) + mi] = acc[i];
   }
   __syncthreads();
   const int n = threadIdx.x & (N - 1);
-  const int m0 = threadIdx.x / N, dm = 256 / N;
+  const int r0 = threadIdx.x / N, dr = 256 / N;
   bool act = n < ch.C && (chain_only < 0 || n == chain_only);
   if (act) act = step < 0 || step <= ch.st[n].L_cur;
   double sq = 0.0;
   if (act) {
     const long long Cp = ch.Cp;
-    const float* Sn = S + n * (TC_M + 1);
-    const int* rows = A.tile_rows + (long long)t * TC_M;
+    const float* Sn = S + n * (TC_FR + 1);
+    const int* rows = A.tile_rows + (long long)t * TC_M + m0;
     if (mode == 0) {
-      for (int m = m0; m < TC_M; m += dm) {
+      for (int m = r0; m < TC_FR; m += dr) {
         const int row = rows[m];
         if (row < 0) continue;
         const float r = v.Ys[row] - Sn[m];
@@ -262,7 +303,7 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
       const ChainState& st = ch.st[n];
       const float* mu = ch.muD + (long long)(st.acc ^ sel) * v.n_h * Cp + n;
       const float sh = st.sh, ss = st.ss;
-      for (int m = m0; m < TC_M; m += dm) {
+      for (int m = r0; m < TC_FR; m += dr) {
         const int row = rows[m];
         if (row < 0) continue;
         const float rh = v.Yh[row] - mu[row * Cp];
@@ -275,11 +316,11 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
   __syncthreads();
   if ((int)threadIdx.x < N && act) {
     double s = 0.0;
-    for (int k = 0; k < dm; k++) s += red[k * N + n];
+    for (int k = 0; k < dr; k++) s += red[k * N + n];
     const int L = ch.st[n].L_cur;
     const int slot = mode == 0 ? (step <= 0 ? SL_RS0 : (step == L ? SL_RSL : SL_SCRATCH))
                                : (step <= 0 ? SL_RH0 : (step == L ? SL_RHL : SL_SCRATCH));
-    ch.part[((long long)n * NSLOT + slot) * ch.maxblk + t] = s;
+    ch.part[((long long)n * NSLOT + slot) * ch.maxblk + blockIdx.x] = s;
   }
 }
 
