@@ -256,13 +256,17 @@ def run_ours(args, dist):
     dist.barrier()
     t0 = time.perf_counter()
     data = d.MultiResData.from_volume(vol, device=dev)
+    t_vol = time.perf_counter()
     chains = d.MultiResParameters(data, hmc, C)
+    t_cs = time.perf_counter()
     stats = None
     for _ in range(args.warmup + args.steps):
         chains.update(1)
         stats = chains.stats()
     summ = chains.summary(-1)
     t_e2e = time.perf_counter() - t0
+    e2e_parts = {"volume": round(t_vol - t0, 4), "chain_set_incl_tuning": round(t_cs - t_vol, 4),
+                 "iterations_and_reads": round(t0 + t_e2e - t_cs, 4)}
     grads_e2e = sum(s["grad_evals"] for s in stats)
     img_bytes = sum(a.nbytes for a in (vol.highres, vol.stdres))
     stat_bytes = C * ctypes.sizeof(d.api.ChainStats)
@@ -365,7 +369,8 @@ def run_ours(args, dist):
                 "h2d_bytes_per_step": int(img_bytes / (args.warmup + args.steps)),
                 "d2h_bytes_per_step": int(stat_bytes),
                 "includes": "in a warm process: volume upload + kriging + FP64 spectrum + chain-set tuning and init "
-                            "+ every iteration (dr_step + d2h chain statistics) + summary d2h"},
+                            "+ every iteration (dr_step + d2h chain statistics) + summary d2h",
+                "seconds_by_part": e2e_parts},
         "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
         "grad_evals_per_step": grads_all / args.steps, **extra,
     }

@@ -837,12 +837,13 @@ static void tc_upload(Volume* V, const TcPlanHost& P, const float* dval, int nnz
   M->T = P.T;
   M->G = P.G;
   M->n_segs = (int)(P.segs.size() / 4);
+  M->chunks = (int)P.chunks;
   M->tile_rows = V->upload(P.tile_rows);
   M->chunk_cols = V->upload(P.chunk_cols);
   M->segs = reinterpret_cast<const int4*>(V->upload(P.segs));
   M->cta_seg_ptr = V->upload(P.cta_seg_ptr);
   M->tile_seg_ptr = V->upload(P.tile_seg_ptr);
-  const size_t nblob = (size_t)P.chunks * 2 * TC_BLK;
+  const size_t nblob = (size_t)P.chunks * TC_BLK;
   float* blob = V->alloc<float>(nblob);
   CK(cudaMemsetAsync(blob, 0, sizeof(float) * std::max<size_t>(nblob, 1), st));
   if (nnz > 0) {
@@ -898,7 +899,7 @@ static bool volume_tc(Volume* V) {
     return false;
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
-  const double blob_bytes = (double)(pw.chunks + pt.chunks) * 2 * TC_BLK * 4;
+  const double blob_bytes = (double)(pw.chunks + pt.chunks) * TC_BLK * 4;
   if (blob_bytes > 0.25 * (double)fr) return false;
   tc_upload(V, pw, dv.w_val, (int)hv.w_col.size(), &V->tc_w);
   tc_upload(V, pt, dv.wt_val, (int)hv.wt_col.size(), &V->tc_wt);
@@ -962,10 +963,13 @@ static void launch_iterations(Chainset* S, int iters);
 static void read_states(Chainset* S, std::vector<ChainState>* st);
 static void write_states(Chainset* S, const std::vector<ChainState>& st);
 
-// Times every candidate (update path x kriging-product grid; chain sets of 32 or
-// more chains keep 8 blocks/SM) for 2 iterations on a scratch chain
-// set of the same shape, forced past the step-size search so that all L
-// leapfrog steps run, and keeps the fastest; results are cached per shape.
+// Tunes in two rounds on scratch chain sets of the same shape, each candidate
+// timed for 2 iterations forced past the step-size search (so that all L
+// leapfrog steps run): first the update paths, with the tensor-core products
+// where the volume and chain count allow them (else CSR products at 8 blocks
+// per SM); then, on the fastest path, the other product choices (CSR at 8
+// blocks/SM, and at 4 and 2 for chain sets of fewer than 32 chains).  The
+// fastest candidate is kept and cached per shape.
 static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   const DevVolume& v = V->dv;
   const TuneKey key{V->device, v.E0, v.E1, v.E2, v.bx, v.by, v.bz, C, v.n_h, v.n_s, o->leapfrog};
@@ -976,21 +980,11 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   }
   const PathOptions po = path_options(v, V->device);
   const bool tc = tc_chains(C) > 0 && !tc_env_off() && volume_tc(V);
-  std::vector<TuneChoice> cand;
-  for (int path : {0, 1, 2}) {
-    if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
-    // wide chain sets share each W row across their chains and fill the GPU at 8 blocks/SM; narrower ones
-    // may do better with fewer, longer-lived product blocks
-    if (C >= 32) cand.push_back(TuneChoice{path, 8, 0.0, 0});
-    else
-      for (int grid : {8, 4, 2}) cand.push_back(TuneChoice{path, grid, 0.0, 0});
-    if (tc) cand.push_back(TuneChoice{path, 8, 0.0, 1});
-  }
   TuneChoice best;
   best.ms = 1e300;
   dr_hmc_opts to = *o;
   to.store_samples = 0;
-  for (TuneChoice& c : cand) {
+  auto try_candidate = [&](TuneChoice c) {
     // a candidate that cannot be built or run (for instance out of device memory beside the caller's other
     // allocations) is skipped; if none can, the default configuration is used untuned
     try {
@@ -1020,6 +1014,17 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
     } catch (const Error&) {
       cudaGetLastError();
     }
+  };
+  for (int path : {0, 1, 2}) {
+    if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
+    try_candidate(TuneChoice{path, 8, 0.0, tc ? 1 : 0});
+  }
+  if (best.ms < 1e300) {
+    const int path = best.path;
+    if (tc) try_candidate(TuneChoice{path, 8, 0.0, 0});
+    // narrower chain sets may do better with fewer, longer-lived CSR product blocks
+    if (C < 32)
+      for (int grid : {4, 2}) try_candidate(TuneChoice{path, grid, 0.0, 0});
   }
   if (!(best.ms < 1e300)) {  // nothing could be timed: default, not cached
     TuneChoice d;
@@ -1727,16 +1732,8 @@ int dr_debug_tc_layout(int n_rows, int n_cols, const int* rowptr, const int* col
   std::vector<uint32_t> ky(keys, keys + n_rows);
   TcPlanHost P;
   if (!tc_plan(rp, cl, ky, g_max, &P)) throw Error(DR_ERR_INVALID, "matrix too large for the tile layout");
-  std::vector<float> blob((size_t)P.chunks * 2 * TC_BLK, 0.f);
-  for (int i = 0; i < nnz; i++) {
-    uint32_t u;
-    std::memcpy(&u, &val[i], 4);
-    u &= 0xFFFFE000u;
-    float h;
-    std::memcpy(&h, &u, 4);
-    blob[P.dest[i]] = h;
-    blob[P.dest[i] + TC_BLK] = val[i] - h;
-  }
+  std::vector<float> blob((size_t)P.chunks * TC_BLK, 0.f);
+  for (int i = 0; i < nnz; i++) blob[P.dest[i]] = val[i];
   std::fill(dense, dense + (size_t)n_rows * n_cols, 0.f);
   const int nseg = (int)(P.segs.size() / 4);
   std::vector<int> chunk_seen(P.chunks, 0), row_seen(n_rows, 0);
@@ -1748,9 +1745,9 @@ int dr_debug_tc_layout(int n_rows, int n_cols, const int* rowptr, const int* col
         const int row = P.tile_rows[(size_t)t * TC_M + m];
         for (int kk = 0; kk < TC_KC; kk++) {
           const int cc = P.chunk_cols[(size_t)c * TC_KC + kk];
-          const size_t off = (size_t)c * 2 * TC_BLK + (kk / 4) * (TC_M * 4) + m * 4 + kk % 4;
-          if (row >= 0 && cc >= 0) dense[(size_t)row * n_cols + cc] += blob[off] + blob[off + TC_BLK];
-          else if (blob[off] != 0.f || blob[off + TC_BLK] != 0.f) dense[0] = NAN;  // padding must stay zero
+          const size_t off = (size_t)c * TC_BLK + (kk / 4) * (TC_M * 4) + m * 4 + kk % 4;
+          if (row >= 0 && cc >= 0) dense[(size_t)row * n_cols + cc] += blob[off];
+          else if (blob[off] != 0.f) dense[0] = NAN;  // padding must stay zero
         }
       }
     }
@@ -1821,6 +1818,13 @@ int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* a
       case 4: b = z * 8 + C * ((double)v.n_s * 4 + 2.0 * v.n_h * 4) + v.n_h * 12.0; break;
       case 5: b = C * ((double)v.n_h * 4 + t2 * 8) + box * 4; break;
       default: b = s->plane ? 0.0 : C * (t2 + t1) * 8; break;
+    }
+    if (s->tcp && (which == 3 || which == 4)) {
+      // tensor-core products: the dense FP32 blob, the chain vectors of every chunk column, the segment partials
+      // written and read back, and the epilogue's operands (rs; or mu_D in and gD out)
+      const DevTcMatrix& M = which == 3 ? s->vol->tc_w : s->vol->tc_wt;
+      b = (double)M.chunks * TC_BLK * 4 + (double)M.chunks * TC_KC * C * 4 +
+          2.0 * M.n_segs * s->tc_N * TC_M * 4 + (which == 3 ? (double)v.n_s * C * 4 : 2.0 * v.n_h * C * 4);
     }
     *algo_bytes = b;
   }

@@ -532,34 +532,51 @@ bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const 
   P->T = (R + M - 1) / M;
   P->tile_rows.assign((size_t)P->T * M, -1);
   for (int i = 0; i < R; i++) P->tile_rows[i] = order[i];
-  std::vector<long long> chunk_ptr(P->T + 1, 0);
+  int n_cols = 0;
+  for (int c : col) n_cols = std::max(n_cols, c + 1);
+  // per tile: the sorted union of its rows' columns (a per-thread stamp array marks columns already taken)
   std::vector<std::vector<int>> uni(P->T);
-  for (int t = 0; t < P->T; t++) {
-    std::vector<int>& u = uni[t];
-    for (int m = 0; m < M; m++) {
-      const int r = P->tile_rows[(size_t)t * M + m];
-      if (r >= 0) u.insert(u.end(), col.begin() + rowptr[r], col.begin() + rowptr[r + 1]);
+#pragma omp parallel
+  {
+    std::vector<int> stamp(n_cols, -1);
+#pragma omp for schedule(dynamic, 1)
+    for (int t = 0; t < P->T; t++) {
+      std::vector<int>& u = uni[t];
+      for (int m = 0; m < M; m++) {
+        const int r = P->tile_rows[(size_t)t * M + m];
+        if (r < 0) continue;
+        for (int k = rowptr[r]; k < rowptr[r + 1]; k++)
+          if (stamp[col[k]] != t) {
+            stamp[col[k]] = t;
+            u.push_back(col[k]);
+          }
+      }
+      std::sort(u.begin(), u.end());
     }
-    std::sort(u.begin(), u.end());
-    u.erase(std::unique(u.begin(), u.end()), u.end());
-    chunk_ptr[t + 1] = chunk_ptr[t] + (long long)(u.size() + KC - 1) / KC;
   }
+  std::vector<long long> chunk_ptr(P->T + 1, 0);
+  for (int t = 0; t < P->T; t++) chunk_ptr[t + 1] = chunk_ptr[t] + (long long)(uni[t].size() + KC - 1) / KC;
   P->chunks = chunk_ptr[P->T];
-  if (P->chunks * 2 * BLK > 0x7fffffffLL) return false;
+  if (P->chunks * BLK > 0x7fffffffLL) return false;
   P->chunk_cols.assign((size_t)P->chunks * KC, -1);
   P->dest.assign(col.size(), -1);
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int t = 0; t < P->T; t++) {
-    const std::vector<int>& u = uni[t];
-    std::copy(u.begin(), u.end(), P->chunk_cols.begin() + chunk_ptr[t] * KC);
-    for (int m = 0; m < M; m++) {
-      const int r = P->tile_rows[(size_t)t * M + m];
-      if (r < 0) continue;
-      for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
-        const long long pos = std::lower_bound(u.begin(), u.end(), col[k]) - u.begin();
-        const long long q = chunk_ptr[t] + pos / KC;
-        const int kk = (int)(pos % KC);
-        P->dest[k] = (int)(q * 2 * BLK + (kk / 4) * (M * 4) + m * 4 + kk % 4);
+#pragma omp parallel
+  {
+    std::vector<int> pos(n_cols, 0);
+#pragma omp for schedule(dynamic, 1)
+    for (int t = 0; t < P->T; t++) {
+      const std::vector<int>& u = uni[t];
+      std::copy(u.begin(), u.end(), P->chunk_cols.begin() + chunk_ptr[t] * KC);
+      for (int i = 0; i < (int)u.size(); i++) pos[u[i]] = i;
+      for (int m = 0; m < M; m++) {
+        const int r = P->tile_rows[(size_t)t * M + m];
+        if (r < 0) continue;
+        for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
+          const long long p = pos[col[k]];
+          const long long q = chunk_ptr[t] + p / KC;
+          const int kk = (int)(p % KC);
+          P->dest[k] = (int)(q * BLK + (kk / 4) * (M * 4) + m * 4 + kk % 4);
+        }
       }
     }
   }

@@ -83,9 +83,8 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
 // Host part of a dense-tile plan for the tensor-core kriging products: rows
 // ordered along the Z-order curve of their keys (3 x 10-bit coordinates) and
 // cut into tiles of 128; the sorted union of each tile's columns cut into
-// chunks of 32; dest[k] = the blob position of nonzero k's TF32 high part
-// (element (m, kk) of chunk q at q * 8192 + (kk / 4) * 512 + m * 4 + kk % 4,
-// the remainder 4096 floats further).  The chunks are split into at most
+// chunks of 32; dest[k] = the blob position of nonzero k (element (m, kk) of
+// chunk q at q * 4096 + (kk / 4) * 512 + m * 4 + kk % 4).  The chunks are split into at most
 // g_max equal ranges, one per CTA, and the ranges at tile boundaries into
 // segments {tile, first chunk, end chunk, 0}, ordered by chunk.
 struct TcPlanHost {

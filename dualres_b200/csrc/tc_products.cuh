@@ -10,21 +10,24 @@
 // Precision: each FP32 operand is split as x = hi + lo (hi = the TF32 bits of
 // x, lo = x - hi, exact), and D accumulates hi_A hi_B + hi_A lo_B + lo_A hi_B
 // in FP32 (three kind::tf32 MMAs per K step), which keeps about 21 bits of
-// every product -- the FP32 CSR products' accuracy, not TF32's.  A's split is
-// made once per volume (the blob); B's while it is gathered.
+// every product -- the FP32 CSR products' accuracy, not TF32's.  The blob holds
+// A in FP32 (16 KB per chunk); both splits are made in shared memory by the
+// gather warps, A's while their B loads are in flight.
 //
 // k_tc_product: one CTA per SM over a contiguous range of chunks (32 columns
 // of one tile).  Warp roles:
-//   warp 0     one thread bulk-copies the chunk's A blocks (32 KB) into the
+//   warp 0     one thread bulk-copies the chunk's A block (16 KB) into the
 //              stage (mbarrier transaction count);
 //   warp 1     allocates TMEM; one thread issues the MMAs of a chunk when both
 //              its A and B are in, then commits the stage back to the
 //              producers; at a tile boundary it commits the accumulator;
-//   warps 2-9  two gather groups of 4 warps, each taking every other chunk:
-//              the chunk's chain vectors X[col][chain] (coalesced over
-//              chains) are loaded -- all of a thread's loads before any is
-//              used -- split, and written as hi / lo in the K-major layout;
-//   warps 10-13 epilogue: TMEM -> registers -> the segment's partial slot.
+//   warps 2-13 three gather groups of 4 warps, taking chunks in turn: the
+//              chunk's chain vectors X[col][chain] are loaded (coalesced over
+//              chains), all of a thread's loads before any is used; meanwhile
+//              the landed A block is split in place into hi and lo; then B is
+//              split and written as hi / lo in the K-major layout, and the
+//              stage is handed to the MMA thread;
+//   warps 14-17 epilogue: TMEM -> registers -> the segment's partial slot.
 // Every mbarrier wait is bounded; a wait that gives up records 3 in ch.err,
 // the roles drain their copies and MMAs, and TMEM is released.
 //
@@ -43,7 +46,7 @@ namespace drb {
 constexpr int TC_M = 128;               // tile rows (MMA M)
 constexpr int TC_KC = 32;               // columns per chunk
 constexpr int TC_BLK = TC_M * TC_KC;    // floats in one block (hi or lo) of a chunk
-constexpr int TC_GROUPS = 2;            // gather groups (chunks in flight in the gather)
+constexpr int TC_GROUPS = 3;            // gather groups (chunks in flight in the gather)
 constexpr int TC_THREADS = 32 * (2 + 4 * TC_GROUPS + 4);
 constexpr int TC_HDR = 4096;            // barriers, TMEM address, chain offsets
 
@@ -107,8 +110,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(fullA + s, 2 * TC_BLK * 4);
-          bulk_g2s(stage0 + s * sbytes, A.blob + (long long)c * 2 * TC_BLK, 2 * TC_BLK * 4, fullA + s);
+          mbar_arrive_expect_tx(fullA + s, TC_BLK * 4);
+          bulk_g2s(stage0 + s * sbytes, A.blob + (long long)c * TC_BLK, TC_BLK * 4, fullA + s);
         }
       }
       // the copies still in flight land before the CTA may exit
@@ -133,7 +136,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int c = sg.y; c < sg.z; c++, q++) {
           const int s = q % stages;
           const uint32_t par = (q / stages) & 1;
-          if (!mbar_wait_bounded(fullA + s, par) || !mbar_wait_bounded(fullB + s, par)) {
+          // the gather group arrives once A is split and B is written
+          if (!mbar_wait_bounded(fullB + s, par)) {
             ok = false;
             break;
           }
@@ -164,6 +168,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if (!ok) atomicExch(ch.err, 3);
     }
   } else if (warp < 2 + 4 * TC_GROUPS) {
+    // Gather group grp takes chunks q = grp (mod TC_GROUPS).  Each chunk waits only for MMAs of earlier chunks,
+    // so the smallest chunk not yet handed over can always proceed, whatever the group and stage counts.
     constexpr int NI = N * (TC_KC / 4) / 128;  // (chain, 4 columns) pairs per thread and chunk
     const int grp = (warp - 2) / 4, t = threadIdx.x - 64 - 128 * grp;
     const long long Cp = ch.Cp;
@@ -181,6 +187,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         float4* bh = reinterpret_cast<float4*>(stage0 + s * sbytes + 2 * TC_BLK * 4);
         float4* bl = bh + N * (TC_KC / 4);
         const int4* cols = reinterpret_cast<const int4*>(A.chunk_cols + (long long)c * TC_KC);
+        // all of this thread's chain-vector loads are issued before any is used (coalesced over chains)
         float xv[NI][4];
 #pragma unroll
         for (int i = 0; i < NI; i++) {
@@ -193,6 +200,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           xv[i][1] = (on && j.y >= 0) ? __ldg(X + o + j.y * Cp) : 0.f;
           xv[i][2] = (on && j.z >= 0) ? __ldg(X + o + j.z * Cp) : 0.f;
           xv[i][3] = (on && j.w >= 0) ? __ldg(X + o + j.w * Cp) : 0.f;
+        }
+        // A: hi in place, lo into the second block, while the loads above are in flight
+        if (!mbar_wait_bounded(fullA + s, (q / stages) & 1)) {
+          ok = false;
+          break;
+        }
+        float4* ah = reinterpret_cast<float4*>(stage0 + s * sbytes);
+        float4* al = ah + TC_BLK / 4;
+#pragma unroll
+        for (int i = 0; i < TC_BLK / 4 / 128; i++) {
+          const float4 a = ah[t + 128 * i];
+          const float4 h = make_float4(tf32_hi(a.x), tf32_hi(a.y), tf32_hi(a.z), tf32_hi(a.w));
+          ah[t + 128 * i] = h;
+          al[t + 128 * i] = make_float4(a.x - h.x, a.y - h.y, a.z - h.z, a.w - h.w);
         }
 #pragma unroll
         for (int i = 0; i < NI; i++) {
@@ -253,49 +274,59 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
   extern __shared__ __align__(16) unsigned char fsm[];
   float* S = reinterpret_cast<float*>(fsm);
   double* red = reinterpret_cast<double*>(fsm + (size_t)N * (TC_FR + 1) * 4);
+  __shared__ int rows[TC_FR];
   const int t = blockIdx.x / (TC_M / TC_FR), m0 = (blockIdx.x % (TC_M / TC_FR)) * TC_FR;
   const int s0 = A.tile_seg_ptr[t], s1 = A.tile_seg_ptr[t + 1];
+  if (threadIdx.x < TC_FR) rows[threadIdx.x] = A.tile_rows[(long long)t * TC_M + m0 + threadIdx.x];
   {
-    // element i of this thread: row m0 + mi, chain ni (rows fastest across the warp)
+    // element i of this thread: row m0 + mi, chain nb + 16 i (rows fastest across the warp); the segments are
+    // summed in order, four segments' loads in flight at a time
     const int mi = threadIdx.x % TC_FR, nb = threadIdx.x / TC_FR;
     float acc[EPT];
 #pragma unroll
     for (int i = 0; i < EPT; i++) acc[i] = 0.f;
-    const float* P = partial + (long long)s0 * N * TC_M + m0 + mi;
+    const long long seg = (long long)N * TC_M;
+    const float* P = partial + (long long)s0 * seg + m0 + mi + (long long)nb * TC_M;
     int g = s0;
-    for (; g + 1 < s1; g += 2, P += 2LL * N * TC_M) {
-      float x0[EPT], x1[EPT];
+    for (; g + 3 < s1; g += 4, P += 4 * seg) {
+      float x[4][EPT];
 #pragma unroll
-      for (int i = 0; i < EPT; i++) {
-        const int ni = nb + (256 / TC_FR) * i;
-        x0[i] = __ldg(P + (long long)ni * TC_M);
-        x1[i] = __ldg(P + (long long)N * TC_M + (long long)ni * TC_M);
-      }
+      for (int u = 0; u < 4; u++)
 #pragma unroll
-      for (int i = 0; i < EPT; i++) acc[i] = (acc[i] + x0[i]) + x1[i];
+        for (int i = 0; i < EPT; i++) x[u][i] = __ldg(P + u * seg + (long long)(256 / TC_FR) * i * TC_M);
+#pragma unroll
+      for (int i = 0; i < EPT; i++) acc[i] = (((acc[i] + x[0][i]) + x[1][i]) + x[2][i]) + x[3][i];
     }
-    if (g < s1) {
+    for (; g < s1; g++, P += seg) {
 #pragma unroll
-      for (int i = 0; i < EPT; i++) acc[i] += __ldg(P + (long long)(nb + (256 / TC_FR) * i) * TC_M);
+      for (int i = 0; i < EPT; i++) acc[i] += __ldg(P + (long long)(256 / TC_FR) * i * TC_M);
     }
 #pragma unroll
     for (int i = 0; i < EPT; i++) S[(nb + (256 / TC_FR) * i) * (TC_FR + 1) + mi] = acc[i];
   }
   __syncthreads();
+  // element j of this thread: row r0 + dr j, chain n (chains fastest)
   const int n = threadIdx.x & (N - 1);
-  const int r0 = threadIdx.x / N, dr = 256 / N;
+  const int r0 = threadIdx.x / N;
+  constexpr int dr = 256 / N;
   bool act = n < ch.C && (chain_only < 0 || n == chain_only);
   if (act) act = step < 0 || step <= ch.st[n].L_cur;
   double sq = 0.0;
   if (act) {
     const long long Cp = ch.Cp;
     const float* Sn = S + n * (TC_FR + 1);
-    const int* rows = A.tile_rows + (long long)t * TC_M + m0;
     if (mode == 0) {
-      for (int m = r0; m < TC_FR; m += dr) {
-        const int row = rows[m];
+      float y[EPT];
+#pragma unroll
+      for (int j = 0; j < EPT; j++) {
+        const int row = rows[r0 + dr * j];
+        y[j] = row >= 0 ? __ldg(v.Ys + row) : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < EPT; j++) {
+        const int row = rows[r0 + dr * j];
         if (row < 0) continue;
-        const float r = v.Ys[row] - Sn[m];
+        const float r = y[j] - Sn[r0 + dr * j];
         ch.rs[row * Cp + n] = r;
         sq += (double)r * r;
       }
@@ -303,11 +334,19 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
       const ChainState& st = ch.st[n];
       const float* mu = ch.muD + (long long)(st.acc ^ sel) * v.n_h * Cp + n;
       const float sh = st.sh, ss = st.ss;
-      for (int m = r0; m < TC_FR; m += dr) {
-        const int row = rows[m];
+      float y[EPT], mv[EPT];
+#pragma unroll
+      for (int j = 0; j < EPT; j++) {
+        const int row = rows[r0 + dr * j];
+        y[j] = row >= 0 ? __ldg(v.Yh + row) : 0.f;
+        mv[j] = row >= 0 ? mu[row * Cp] : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < EPT; j++) {
+        const int row = rows[r0 + dr * j];
         if (row < 0) continue;
-        const float rh = v.Yh[row] - mu[row * Cp];
-        ch.gD[row * Cp + n] = sh * rh + ss * Sn[m];
+        const float rh = y[j] - mv[j];
+        ch.gD[row * Cp + n] = sh * rh + ss * Sn[r0 + dr * j];
         sq += (double)rh * rh;
       }
     }
@@ -324,14 +363,10 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
   }
 }
 
-// Builds the dense blob from the CSR values: hi at dest[k], lo at dest[k] + 128 * 32 (the blob is zeroed first).
+// Scatters the CSR values into the dense blob (zeroed first): value k at dest[k].
 __global__ void k_tc_fill(const float* __restrict__ val, const int* __restrict__ dest, int nnz, float* __restrict__ blob) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nnz) return;
-  const float x = val[k];
-  const float h = tf32_hi(x);
-  blob[dest[k]] = h;
-  blob[dest[k] + TC_BLK] = x - h;
+  if (k < nnz) blob[dest[k]] = val[k];
 }
 
 }  // namespace drb

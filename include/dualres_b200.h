@@ -162,8 +162,9 @@ void dr_chainset_destroy(dr_chainset* cs);
  * 2 x-line kernel with separate y passes), kriging-product blocks per SM, the
  * iteration time measured when the shape was tuned (0 when it was not), and
  * whether the kriging products run on the tensor cores (1) or as CSR products
- * (0).  At creation every eligible (path, blocks, products) choice is timed on a
- * scratch chain set of the same shape, and the fastest is kept for the process;
+ * (0).  At creation the update paths are timed on a scratch chain set of the
+ * same shape (with the tensor-core products where available), then the other
+ * product choices on the fastest path, and the fastest is kept for the process;
  * DRB_AUTOTUNE=0 turns this off, DRB_NO_PLANE / DRB_PLANE_PREFETCH force a
  * path, DRB_TC_PRODUCTS=0 / 1 the products.  Any output may be NULL. */
 int dr_chainset_config_get(const dr_chainset* cs, int* path, int* blocks_per_sm, double* tuned_ms,
@@ -315,10 +316,9 @@ int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starti
 /* Host-only check of the dense-tile layout of the tensor-core kriging products
  * (no GPU): plans the n_rows x n_cols CSR matrix with the given row keys
  * (Z-order keys of 3 x 10-bit coordinates) for at most g_max CTAs, fills the
- * TF32 high / remainder blob as the device does, and writes back the dense
- * matrix read out of the blob through the tiles' row and column maps
- * (dense: n_rows x n_cols floats, hi + lo per element; dense[0] is NaN if a
- * padding position of the blob is not zero) and stats[0..6] = tiles, chunks,
+ * FP32 blob as the device does, and writes back the dense matrix read out of
+ * the blob through the tiles' row and column maps (dense: n_rows x n_cols
+ * floats; dense[0] is NaN if a padding position of the blob is not zero) and stats[0..6] = tiles, chunks,
  * segments, CTAs, chunks covered by the segments exactly once, matrix rows in
  * the tiles exactly once, and 1 if the segment index tables are consistent. */
 int dr_debug_tc_layout(int n_rows, int n_cols, const int* rowptr, const int* col, const float* val,

@@ -3,11 +3,11 @@
 The layout is the tensor-core path's only host-side arithmetic: rows ordered
 along a Z-order curve and cut into tiles of 128, each tile's column union cut
 into chunks of 32, every nonzero placed at its (chunk, row, column) position of
-the K-major core-matrix blocks as a TF32 high part plus an exact remainder, and
-the chunks split into per-CTA ranges and per-tile segments.  Reading the blob
-back through the tile maps must give the kriging matrix exactly (hi + lo == w
-bit for bit), every chunk must be covered by exactly one segment, every row
-must sit in exactly one tile, and the padding must stay zero.
+the K-major core-matrix blocks, and the chunks split into per-CTA ranges and
+per-tile segments.  Reading the blob back through the tile maps must give the
+kriging matrix exactly (bit for bit), every chunk must be covered by exactly
+one segment, every row must sit in exactly one tile, and the padding must stay
+zero.
 """
 import numpy as np
 import pytest
