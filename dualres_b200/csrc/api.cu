@@ -78,6 +78,8 @@ static void set_pass_attrs() {
   if constexpr (sizeof(C) == 8) {
     CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_xline<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   }
 }
@@ -161,12 +163,18 @@ static void launch_pass_n(int dir, int pro, int epi, const PassArgs& a, const De
   else if (dir > 0 && pro == PRO_LOAD && epi == EPI_STORE)
     k_pass<N, +1, PRO_LOAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
   else if constexpr (sizeof(C) == 8) {
-    if (dir > 0 && pro == PRO_DATAGRAD && epi == EPI_STORE)
-      k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
-    else if (dir < 0 && pro == PRO_LOAD && epi == EPI_GATHER)
-      k_pass<N, -1, PRO_LOAD, EPI_GATHER, C><<<grid, block, smem, s>>>(a, v, ch, tw);
-    else
+    // the z passes touch the chain-minor arrays: with 8 or more chains, tiles of 4 lines x 8 chains
+    const bool grouped = a.chain_only < 0 && nch >= 8 && a.B > 1;
+    const dim3 ggrid(cdiv_i((long long)a.A * a.B, TILE_LINES / 8), cdiv_i(nch, 8));
+    if (dir > 0 && pro == PRO_DATAGRAD && epi == EPI_STORE) {
+      if (grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
+      else k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+    } else if (dir < 0 && pro == PRO_LOAD && epi == EPI_GATHER) {
+      if (grouped) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
+      else k_pass<N, -1, PRO_LOAD, EPI_GATHER, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+    } else {
       throw Error(DR_ERR_INVALID, "unsupported pass combination");
+    }
   } else {
     throw Error(DR_ERR_INVALID, "unsupported pass combination");
   }

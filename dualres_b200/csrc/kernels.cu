@@ -95,40 +95,58 @@ __device__ double gamma_draw(double shape, double scale, uint64_t seed, uint32_t
 
 // ----------------------------------------------------------------- pass kernel
 // Batched 1D FFT along the middle axis of [A][n][B] arrays, one tile of 32
-// lines (line = a * B + b) per block, chains on blockIdx.y.
+// lines (line = a * B + b) per block.  CPB = 1: the 32 lines of one chain
+// (blockIdx.y).  CPB = 8: 4 consecutive lines of 8 chains (chain group
+// blockIdx.y), used by the z passes whose epilogue / prologue touch the
+// chain-minor arrays mu_D, mu_O and gD: a warp then reads and writes 8 chains
+// x 4 bytes contiguously there, instead of one 4-byte value per 256-byte row,
+// while its T2 accesses stay whole 32-byte sectors (4 lines x 8 bytes).
 template <int N> struct PassCfg {
   static constexpr int NT = N >= 512 ? 512 : 256;
 };
 
-template <int N, int DIR, int PRO, int EPI, class C>
+template <int N, int DIR, int PRO, int EPI, class C, int CPB = 1>
 __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v, DevChains ch, const C* __restrict__ tw) {
-  constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = PassCfg<N>::NT;
+  constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = PassCfg<N>::NT, LPC = TILE_LINES / CPB;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  const int c = (a.chain_only >= 0) ? a.chain_only : (int)blockIdx.y;
-  if (a.step >= 0 && ch.st != nullptr) {
-    if (a.step > ch.st[c].L_cur) return;
+  __shared__ int s_ok[CPB], s_hsel[CPB], s_wo[CPB];
+  const int cbase = CPB == 1 ? ((a.chain_only >= 0) ? a.chain_only : (int)blockIdx.y) : (int)blockIdx.y * CPB;
+  if (threadIdx.x < CPB) {
+    // per chain of the tile: active at this step, the half of mu_D / mu_O written, whether mu_O is written
+    const int c = cbase + (int)threadIdx.x;
+    int ok = CPB == 1 || c < ch.C;
+    if (ok && a.step >= 0 && ch.st != nullptr && a.step > ch.st[c].L_cur) ok = 0;
+    s_ok[threadIdx.x] = ok;
+    int hs = 0, wo = 0;
+    if (EPI == EPI_GATHER && ok) {
+      hs = (ch.st != nullptr ? ch.st[c].acc : 0) ^ a.sel;
+      wo = a.write_o == 1 || (a.write_o == 2 && ch.st != nullptr && a.step == ch.st[c].L_cur);
+    }
+    s_hsel[threadIdx.x] = hs;
+    s_wo[threadIdx.x] = wo;
   }
+  __syncthreads();
+  if (CPB == 1 && !s_ok[0]) return;
   const long long lines = (long long)a.A * a.B;
-  const long long l0 = (long long)blockIdx.x * TL;
-  const int nl = (int)min((long long)TL, lines - l0);
-  const C* in = reinterpret_cast<const C*>(a.in) + (long long)c * a.in_cs;
-  C* out = reinterpret_cast<C*>(a.out) + (long long)c * a.out_cs;
+  const long long l0 = (long long)blockIdx.x * LPC;
+  const int nl = (int)min((long long)LPC, lines - l0);
   const int B = a.B, n_in = a.n_in, n_out = a.n_out;
-  int hsel = 0;
-  if (EPI == EPI_GATHER) hsel = (ch.st != nullptr ? ch.st[c].acc : 0) ^ a.sel;
-
-  auto in_index = [&](int l, int i) -> long long {
-    const long long lam = l0 + l;
+  // tile line l: chain slot l / LPC of the tile, line l0 + l % LPC
+  auto valid = [&](int l) { return (l % LPC) < nl && s_ok[l / LPC]; };
+  auto chain = [&](int l) { return cbase + l / LPC; };
+  auto line_index = [&](int l, int i, int n) -> long long {
+    const long long lam = l0 + l % LPC;
     const long long aa = lam / B, bb = lam - aa * B;
-    return (aa * n_in + i) * B + bb;
+    return (aa * n + i) * B + bb;
   };
   auto load = [&](int l, int i) -> C {
     C val = mk((decltype(C().x))0, (decltype(C().x))0);
-    if (l < nl && i < n_in) {
-      const long long idx = in_index(l, i);
+    if (valid(l) && i < n_in) {
+      const long long idx = line_index(l, i, n_in);
+      const int c = chain(l);
       if (PRO == PRO_LOAD) {
-        val = in[idx];
+        val = reinterpret_cast<const C*>(a.in)[(long long)c * a.in_cs + idx];
       } else {
         const int j = v.box_to_d[idx];
         if (j >= 0) val.x = ch.gD[(long long)j * ch.Cp + c];
@@ -151,24 +169,20 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
   fft_smem<N, DIR, TL, NT>(sm, 1, P, TL, tw + tw_offset(N));
 
   const auto scale = (decltype(C().x))a.scale;
-  int wo = 0;
-  if (EPI == EPI_GATHER) {
-    wo = a.write_o == 1 || (a.write_o == 2 && ch.st != nullptr && a.step == ch.st[c].L_cur);
-  }
   auto store = [&](int l, int k) {
-    if (l >= nl || k >= n_out) return;
-    const long long lam = l0 + l;
-    const long long aa = lam / B, bb = lam - aa * B;
-    const long long idx = (aa * n_out + k) * B + bb;
+    if (!valid(l) || k >= n_out) return;
+    const long long idx = line_index(l, k, n_out);
+    const int c = chain(l);
     const C val = sm[k * P + l];
     if (EPI == EPI_STORE) {
-      out[idx] = mk(val.x * scale, val.y * scale);
+      reinterpret_cast<C*>(a.out)[(long long)c * a.out_cs + idx] = mk(val.x * scale, val.y * scale);
     } else {
+      const int slot = l / LPC;
       const int j = v.box_to_d[idx];
-      if (j >= 0) ch.muD[((long long)hsel * v.n_h + j) * ch.Cp + c] = (float)(val.x * scale);
-      if (wo) {
+      if (j >= 0) ch.muD[((long long)s_hsel[slot] * v.n_h + j) * ch.Cp + c] = (float)(val.x * scale);
+      if (s_wo[slot]) {
         const int o = v.box_to_o[idx];
-        if (o >= 0) ch.muO[((long long)hsel * v.n_o + o) * ch.Cp + c] = (float)(val.x * scale);
+        if (o >= 0) ch.muO[((long long)s_hsel[slot] * v.n_o + o) * ch.Cp + c] = (float)(val.x * scale);
       }
     }
   };
