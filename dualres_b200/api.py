@@ -154,6 +154,7 @@ def _declare(L):
                                     C.POINTER(_fp)]
     L.dr_debug_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
     L.dr_debug_tc_layout.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp]
+    L.dr_debug_bounded_wait.argtypes = [C.c_int, C.c_double, _ip, _dp]
     L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
@@ -478,6 +479,13 @@ def time_kernel(chains, which, step=1, reps=20):
     b = np.zeros(1, np.float64)
     check(lib().dr_debug_time_kernel(chains.h, which, step, reps, _ptr(ms), _ptr(b)))
     return float(ms[0]), float(b[0])
+
+
+def bounded_wait(limit_ms=200.0, device=0):
+    """One device wait that nothing completes (dr_debug_bounded_wait): (gave_up, waited_ms)."""
+    g, w = C.c_int(-1), C.c_double(0)
+    check(lib().dr_debug_bounded_wait(device, float(limit_ms), C.byref(g), C.byref(w)))
+    return bool(g.value == 1), w.value
 
 
 def zorder_keys(ijk):

@@ -1839,6 +1839,33 @@ int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* a
   API_END
 }
 
+int dr_debug_bounded_wait(int device, double limit_ms, int* gave_up, double* waited_ms) {
+  API_BEGIN
+  if (!gave_up || !waited_ms || !(limit_ms > 0 && limit_ms <= 10000)) throw Error(DR_ERR_INVALID, "bad argument");
+  device_tables(device);
+  CK(cudaSetDevice(device));
+  int* d_flag = nullptr;
+  unsigned long long* d_ns = nullptr;
+  CK(cudaMalloc(&d_flag, sizeof(int)));
+  const cudaError_t e = cudaMalloc(&d_ns, sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    cudaFree(d_flag);
+    throw Error(DR_ERR_NOMEM, "cudaMalloc");
+  }
+  k_debug_bounded_wait<<<1, 32>>>((uint64_t)(limit_ms * 1e6), d_flag, d_ns);
+  const cudaError_t le = cudaGetLastError();
+  unsigned long long ns = 0;
+  int flag = -1;
+  const cudaError_t c1 = le == cudaSuccess ? cudaMemcpy(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost) : le;
+  const cudaError_t c2 = c1 == cudaSuccess ? cudaMemcpy(&ns, d_ns, sizeof(ns), cudaMemcpyDeviceToHost) : c1;
+  cudaFree(d_flag);
+  cudaFree(d_ns);
+  CK(c2);
+  *gave_up = flag;
+  *waited_ms = (double)ns * 1e-6;
+  API_END
+}
+
 int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starting_eps, float mhtarget, int n,
                             const float* rates, double* eps_out, int* steps_out, int device) {
   API_BEGIN
@@ -1921,6 +1948,12 @@ static int64_t estimate_bytes(const HostVolume& hv, int C, const dr_hmc_opts& o)
   double cs = C * (3 * N * 8 + t2 * 8 + (hv.E[0] == hv.E[1] ? 0.0 : (double)hv.E[2] * hv.E[1] * hv.box[0] * 8)) +
               C * (2 * (nh + no) * 4 + (nh + ns) * 4 + no * 24) + N * 8 + (double)C * 9 * 2048 * 8;
   if (o.store_samples) cs += (double)std::max(o.nsave, 1) * (no * 4 + 24) * C;
+  if (tc_chains(C) > 0 && ns > 0) {
+    // dense tiles of W and W^T for the tensor-core products (their column unions are a few times the nonzeros:
+    // 5.8x and 3.1x on a 32^3 volume; 10x each is budgeted), index tables, and the segment partials
+    vol += 2 * nnz * 10 * 4 + (nh + ns) * 8;
+    cs += (double)((ns + nh) / TC_M + 2 + 2 * 148) * tc_chains(C) * TC_M * 4;
+  }
   return (int64_t)(1.10 * (vol + cs)) + (16 << 20);
 }
 

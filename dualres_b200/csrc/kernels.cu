@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(ch.err, 1);
-        mbar_wait_bounded(bar, 0, 1 << 20);
+        mbar_wait_bounded(bar, 0, 500000000ull);
       }
       return;
     }
@@ -984,6 +984,19 @@ __global__ void k_scale(float2* u, long long N, float f) {
 }
 
 // Device restatement of HMCParameters::update over a given MH-rate sequence (diagnostics).
+// A wait that runs out: an mbarrier that nothing arrives on, waited for with a limit of limit_ms (the bounded-wait
+// path every pipeline in this library takes when a copy or an MMA does not complete).
+__global__ void k_debug_bounded_wait(uint64_t limit_ns, int* gave_up, unsigned long long* waited_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  mbar_fence_init();
+  const uint64_t t0 = globaltimer_ns();
+  const bool ok = mbar_wait_bounded(&bar, 0, limit_ns);
+  *waited_ns = globaltimer_ns() - t0;
+  *gave_up = ok ? 0 : 1;
+}
+
 __global__ void k_debug_dual_averaging(ChainState st, int n, const float* rates, double* eps_out, int* steps_out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int i = 0; i < n; i++) {

@@ -313,6 +313,12 @@ int dr_debug_dual_averaging(int burnin, int nsave, int thin, int L, float starti
  * 6 inverse y pass.  The kernels run on the live chain state, which they
  * change: call it only when the chains are no longer needed.  algo_bytes
  * receives the kernel's algorithmic bytes per launch (may be NULL). */
+/* Runs one bounded mbarrier wait that nothing completes (the time-out path of
+ * the library's bulk-copy and tensor-core pipelines): *gave_up = 1 when the
+ * wait returned after about limit_ms (0 < limit_ms <= 10000) with the time it
+ * waited in *waited_ms; the device stays usable. */
+int dr_debug_bounded_wait(int device, double limit_ms, int* gave_up, double* waited_ms);
+
 /* Host-only check of the dense-tile layout of the tensor-core kriging products
  * (no GPU): plans the n_rows x n_cols CSR matrix with the given row keys
  * (Z-order keys of 3 x 10-bit coordinates) for at most g_max CTAs, fills the
