@@ -376,7 +376,7 @@ class MultiResParameters:
         p, g, ms, tc = C.c_int(0), C.c_int(0), C.c_double(0), C.c_int(0)
         check(lib().dr_chainset_config_get(self.h, C.byref(p), C.byref(g), C.byref(ms), C.byref(tc)))
         return dict(path=self.PATHS[p.value], blocks_per_sm=g.value, tuned_ms=ms.value,
-                    tensor_products=bool(tc.value))
+                    tensor_products=bool(tc.value), tma_row_gather=tc.value == 2)
 
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))

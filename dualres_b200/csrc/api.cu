@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/dualres_b200.h"
 #include "host_setup.h"
 #include "kernels.cu"
@@ -140,11 +142,16 @@ static DeviceTables& device_tables(int dev) {
     for (int n = 16; n <= 256; n *= 2) smax = std::max(smax, tc_smem_bytes(n));
     t.tc = optin >= smax;
     if (t.tc) {
-      CK(cudaFuncSetAttribute(k_tc_product<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-      CK(cudaFuncSetAttribute(k_tc_product<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-      CK(cudaFuncSetAttribute(k_tc_product<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-      CK(cudaFuncSetAttribute(k_tc_product<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-      CK(cudaFuncSetAttribute(k_tc_product<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+      CK(cudaFuncSetAttribute(k_tc_product<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
     }
   }
   t.ready = true;
@@ -579,6 +586,8 @@ struct Chainset {
   bool tcp = false;             // kriging products on the tensor cores (dense tiles of the volume)
   int tc_N = 0;                 // chains per tensor-core product (power of two >= C)
   float* tc_partial = nullptr;  // [segments][tc_N][128] partial products
+  bool tc_tg = false;           // W^T rs: the chain vectors arrive by TMA row gathers over tc_map_wt
+  CUtensorMap tc_map_w{}, tc_map_wt{};  // (tc_map_w unused: W mu_D gathers with its threads); rs as [n_s] rows
   bool tma = false;             // ... in the persistent bulk-copy kernel (E0 <= 64, fits shared memory)
   int tma_smem = 0, tma_grid = 0;
 
@@ -671,13 +680,22 @@ static void launch_tc(Chainset* S, int step, int sel, int chain_only, bool w) {
   if (M.G > 0) {
     const int n_h = V->dv.n_h, mode = w ? 0 : 1;
     const size_t sm = tc_smem_bytes(N);
+    const CUtensorMap& xm = w ? S->tc_map_w : S->tc_map_wt;
+    float* P = S->tc_partial;
+    // TMA row gathers for W^T rs (one row set per chunk); W mu_D would need both halves of mu_D per chunk, twice
+    // the gathered bytes in twice the operations, and measured faster with the threads' own loads
+    const bool tg = S->tc_tg && !w;
+#define DRB_TC_LAUNCH(NN)                                                                                 \
+  if (tg) k_tc_product<NN, true><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, P, xm); \
+  else k_tc_product<NN, false><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, P, xm);
     switch (N) {
-      case 16: k_tc_product<16><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
-      case 32: k_tc_product<32><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
-      case 64: k_tc_product<64><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
-      case 128: k_tc_product<128><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
-      default: k_tc_product<256><<<M.G, TC_THREADS, sm, S->stream>>>(M, S->dc, n_h, sel, mode, S->tc_partial); break;
+      case 16: DRB_TC_LAUNCH(16) break;
+      case 32: DRB_TC_LAUNCH(32) break;
+      case 64: DRB_TC_LAUNCH(64) break;
+      case 128: DRB_TC_LAUNCH(128) break;
+      default: DRB_TC_LAUNCH(256) break;
     }
+#undef DRB_TC_LAUNCH
     CK_LAUNCH();
   }
   const size_t fs = tc_finish_smem_bytes(N);
@@ -918,6 +936,35 @@ static bool volume_tc(Volume* V) {
   return true;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (null when the driver does not provide it).
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// A 2D map of a chain-minor array (rows of Cp floats) whose box is one row of N chains, for tile::gather4 row
+// gathers; false when the driver cannot encode it (the products then gather with their threads).
+static bool encode_row_map(CUtensorMap* m, const float* base, int Cp, long long rows, int N) {
+  const PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+  if (!fn || rows <= 0 || rows > 0x7fffffffLL || (Cp * 4) % 16 != 0 || N > 256) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)Cp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Cp * 4};
+  const cuuint32_t box[2] = {(cuuint32_t)N, 1};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Chains per tensor-core product: the smallest power of two >= C and >= 16 (0 when C is outside [16, 256]).
 static int tc_chains(int C) {
   if (C < 16 || C > 256) return 0;
@@ -1129,6 +1176,8 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     ch.nb_w = tc_finish_blocks(V->tc_w.T);
     ch.nb_wt = tc_finish_blocks(V->tc_wt.T);
     S->tc_partial = S->alloc<float>((size_t)std::max(V->tc_max_segs, 1) * S->tc_N * TC_M, false);
+    const char* tg = std::getenv("DRB_TC_TMA_GATHER");
+    S->tc_tg = !(tg && std::string(tg) == "0") && encode_row_map(&S->tc_map_wt, ch.rs, ch.Cp, (long long)v.n_s, S->tc_N);
   }
   ch.maxblk = std::max(ch.nb_x, std::max(ch.nb_w, ch.nb_wt));
   ch.part = S->alloc<double>((size_t)C * NSLOT * ch.maxblk);
@@ -1456,7 +1505,7 @@ int dr_chainset_config_get(const dr_chainset* s, int* path, int* blocks_per_sm, 
   if (path) *path = s->path;
   if (blocks_per_sm) *blocks_per_sm = s->grid;
   if (tuned_ms) *tuned_ms = s->tuned_ms;
-  if (tensor_products) *tensor_products = s->tcp ? 1 : 0;
+  if (tensor_products) *tensor_products = s->tcp ? (s->tc_tg ? 2 : 1) : 0;
   API_END
 }
 

@@ -23,10 +23,11 @@
 //              producers; at a tile boundary it commits the accumulator;
 //   warps 2-13 three gather groups of 4 warps, taking chunks in turn: the
 //              chunk's chain vectors X[col][chain] are loaded (coalesced over
-//              chains), all of a thread's loads before any is used; meanwhile
-//              the landed A block is split in place into hi and lo; then B is
-//              split and written as hi / lo in the K-major layout, and the
-//              stage is handed to the MMA thread;
+//              chains), all of a thread's loads before any is used -- or, for
+//              W^T rs, taken from shared memory where warp 0's TMA row gathers
+//              (tile::gather4) put them; meanwhile the landed A block is split
+//              in place into hi and lo; then B is split and written as hi / lo
+//              in the K-major layout, and the stage is handed to the MMA thread;
 //   warps 14-17 epilogue: TMEM -> registers -> the segment's partial slot.
 // Every mbarrier wait is bounded; a wait that gives up records 3 in ch.err,
 // the roles drain their copies and MMAs, and TMEM is released.
@@ -37,6 +38,8 @@
 // partials, or gD = sigma_h^-2 (Yh - mu_D) + sigma_s^-2 W^T rs with the
 // ||Yh - mu_D||^2 partials (MultiResParameters.h:357-364).
 #pragma once
+
+#include <cuda.h>
 
 #include "drb.h"
 #include "umma.cuh"
@@ -50,14 +53,34 @@ constexpr int TC_GROUPS = 3;            // gather groups (chunks in flight in th
 constexpr int TC_THREADS = 32 * (2 + 4 * TC_GROUPS + 4);
 constexpr int TC_HDR = 4096;            // barriers, TMEM address, chain offsets
 
+// Barrier of the nthreads threads (whole warps) that use barrier id, returning the AND of their v: every thread of
+// the group reaches it once per chunk, so a wait that gave up in one warp ends the group's loop in all of them.
+__device__ __forceinline__ bool group_all(bool v, int id, int nthreads) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
 __host__ __device__ inline int tc_stages(int N) { return N <= 64 ? 4 : (N <= 128 ? 3 : 2); }
 __host__ __device__ inline int tc_stage_bytes(int N) { return 2 * TC_BLK * 4 + 2 * N * TC_KC * 4; }
 __host__ __device__ inline int tc_smem_bytes(int N) { return TC_HDR + tc_stages(N) * tc_stage_bytes(N); }
 
 // mode 0: X = mu_D (each chain's accepted half xor sel), mode 1: X = rs.  N: chains, a power of two in [16, 256].
-template <int N>
+// TG: the chain vectors of a chunk's columns arrive by TMA row gathers (tile::gather4 over xmap, a 2D map of X with
+// rows of Cp chains and a one-row box of N chains) issued by warp 0 into the stage's B blocks -- for mu_D both
+// halves, half 0 into the hi block and half 1 into the lo block; padding columns fetch row 0, which meets zero
+// columns of A -- and the gather groups only read them from shared memory.  Without TG the gather groups load them.
+template <int N, bool TG>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_tc_product(DevTcMatrix A, DevChains ch, int n_h, int sel, int mode, float* __restrict__ partial) {
+    k_tc_product(DevTcMatrix A, DevChains ch, int n_h, int sel, int mode, float* __restrict__ partial,
+                 const __grid_constant__ CUtensorMap xmap) {
   extern __shared__ __align__(1024) unsigned char tsm[];
   uint64_t* fullA = reinterpret_cast<uint64_t*>(tsm);
   uint64_t* fullB = fullA + 4;
@@ -67,6 +90,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   uint64_t* done = fullA + 14;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tsm + 128);
   long long* xoff = reinterpret_cast<long long*>(tsm + 256);
+  int* xhalf = reinterpret_cast<int*>(tsm + 2304);
   unsigned char* stage0 = tsm + TC_HDR;
   const int stages = tc_stages(N), sbytes = tc_stage_bytes(N);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -86,8 +110,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   }
   for (int n = threadIdx.x; n < N; n += TC_THREADS) {
     long long o = -1;
-    if (n < ch.C) o = mode == 0 ? (long long)(ch.st[n].acc ^ sel) * n_h * ch.Cp + n : (long long)n;
+    int h = -1;
+    if (n < ch.C) {
+      h = mode == 0 ? (ch.st[n].acc ^ sel) : 0;
+      o = (long long)h * n_h * ch.Cp + n;
+    }
     xoff[n] = o;
+    xhalf[n] = h;
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, ncols);
@@ -100,24 +129,48 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   bool ok = true;
 
   if (warp == 0) {
-    if (lane == 0) {
-      int q = 0;
-      for (int g = seg0; g < seg1 && ok; g++) {
-        const int4 sg = A.segs[g];
-        for (int c = sg.y; c < sg.z; c++, q++) {
-          const int s = q % stages;
-          if (q >= stages && !mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1)) {
-            ok = false;
-            break;
-          }
-          mbar_arrive_expect_tx(fullA + s, TC_BLK * 4);
-          bulk_g2s(stage0 + s * sbytes, A.blob + (long long)c * TC_BLK, TC_BLK * 4, fullA + s);
+    // the whole warp: lane 0 bulk-copies A, lanes 0-7 (and 8-15 for the second half of mu_D) gather 4 rows each.
+    // A CTA's chunks are one contiguous range (its segments in order), and the column indices of the next chunk
+    // are loaded while the current one is issued.
+    const int halves = mode == 0 ? 2 : 1;
+    const uint32_t xbytes = TG ? (uint32_t)halves * TC_KC * N * 4 : 0u;
+    const int c_begin = seg0 < seg1 ? A.segs[seg0].y : 0, c_end = seg0 < seg1 ? A.segs[seg1 - 1].z : 0;
+    int jn = 0;
+    if constexpr (TG) {
+      if (c_begin < c_end) jn = __ldg(A.chunk_cols + (long long)c_begin * TC_KC + lane);
+    }
+    int q = 0;
+    for (int c = c_begin; c < c_end; c++, q++) {
+      const int s = q % stages;
+      int j = jn;
+      if constexpr (TG) {
+        if (c + 1 < c_end) jn = __ldg(A.chunk_cols + (long long)(c + 1) * TC_KC + lane);
+        if (j < 0) j = 0;
+      }
+      if (!__all_sync(0xffffffffu, q < stages || mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1))) {
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
+        mbar_arrive_expect_tx(fullA + s, TC_BLK * 4 + xbytes);
+        bulk_g2s(stage0 + s * sbytes, A.blob + (long long)c * TC_BLK, TC_BLK * 4, fullA + s);
+      }
+      if constexpr (TG) {
+        __syncwarp();
+        const int h = lane >> 3, r4 = (lane & 7) * 4;
+        const int y0 = __shfl_sync(0xffffffffu, j, r4), y1 = __shfl_sync(0xffffffffu, j, r4 + 1);
+        const int y2 = __shfl_sync(0xffffffffu, j, r4 + 2), y3 = __shfl_sync(0xffffffffu, j, r4 + 3);
+        if (h < halves) {
+          const int ro = h * n_h;
+          unsigned char* dst = stage0 + s * sbytes + 2 * TC_BLK * 4 + h * N * TC_KC * 4 + r4 * N * 4;
+          tma_gather4(dst, &xmap, 0, y0 + ro, y1 + ro, y2 + ro, y3 + ro, fullA + s);
         }
       }
-      // the copies still in flight land before the CTA may exit
-      for (int r = q - stages < 0 ? 0 : q - stages; r < q; r++) mbar_wait_bounded(fullA + r % stages, (r / stages) & 1);
-      if (!ok) atomicExch(ch.err, 3);
     }
+    // the copies still in flight land before the CTA may exit
+    if (lane == 0)
+      for (int r = q - stages < 0 ? 0 : q - stages; r < q; r++) mbar_wait_bounded(fullA + r % stages, (r / stages) & 1);
+    if (!ok && lane == 0) atomicExch(ch.err, 3);
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_tf32(TC_M, N);
@@ -180,31 +233,55 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       for (int c = sg.y; c < sg.z; c++, q++) {
         if (q % TC_GROUPS != grp) continue;
         const int s = q % stages;
-        if (q >= stages && !mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1)) {
-          ok = false;
-          break;
-        }
+        bool got = q < stages || mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1);
         float4* bh = reinterpret_cast<float4*>(stage0 + s * sbytes + 2 * TC_BLK * 4);
         float4* bl = bh + N * (TC_KC / 4);
-        const int4* cols = reinterpret_cast<const int4*>(A.chunk_cols + (long long)c * TC_KC);
-        // all of this thread's chain-vector loads are issued before any is used (coalesced over chains)
         float xv[NI][4];
+        if constexpr (TG) {
+          // A and the gathered rows have landed: row k of half h at float h * 32N + k * N of the B blocks
+          got = got && mbar_wait_bounded(fullA + s, (q / stages) & 1);
+          if (got) {
+            const float* xs = reinterpret_cast<const float*>(bh);
 #pragma unroll
-        for (int i = 0; i < NI; i++) {
-          const int idx = t + 128 * i;
-          const int n = idx & (N - 1), kc4 = idx / N;
-          const long long o = xoff[n];
-          const int4 j = __ldg(cols + kc4);
-          const bool on = o >= 0;
-          xv[i][0] = (on && j.x >= 0) ? __ldg(X + o + j.x * Cp) : 0.f;
-          xv[i][1] = (on && j.y >= 0) ? __ldg(X + o + j.y * Cp) : 0.f;
-          xv[i][2] = (on && j.z >= 0) ? __ldg(X + o + j.z * Cp) : 0.f;
-          xv[i][3] = (on && j.w >= 0) ? __ldg(X + o + j.w * Cp) : 0.f;
-        }
-        // A: hi in place, lo into the second block, while the loads above are in flight
-        if (!mbar_wait_bounded(fullA + s, (q / stages) & 1)) {
-          ok = false;
-          break;
+            for (int i = 0; i < NI; i++) {
+              const int idx = t + 128 * i;
+              const int n = idx & (N - 1), kc4 = idx / N;
+              const int h = xhalf[n];
+              const float* r = xs + (h > 0 ? h : 0) * N * TC_KC + 4 * kc4 * N + n;
+#pragma unroll
+              for (int kk = 0; kk < 4; kk++) xv[i][kk] = h >= 0 ? r[kk * N] : 0.f;
+            }
+          }
+          // every thread of the group has read the staged rows before the blocks are overwritten, and the group
+          // goes on only if every thread's waits succeeded
+          if (!group_all(got, 1 + grp, 128)) {
+            ok = false;
+            break;
+          }
+        } else {
+          if (!got) {
+            ok = false;
+            break;
+          }
+          const int4* cols = reinterpret_cast<const int4*>(A.chunk_cols + (long long)c * TC_KC);
+          // all of this thread's chain-vector loads are issued before any is used (coalesced over chains)
+#pragma unroll
+          for (int i = 0; i < NI; i++) {
+            const int idx = t + 128 * i;
+            const int n = idx & (N - 1), kc4 = idx / N;
+            const long long o = xoff[n];
+            const int4 j = __ldg(cols + kc4);
+            const bool on = o >= 0;
+            xv[i][0] = (on && j.x >= 0) ? __ldg(X + o + j.x * Cp) : 0.f;
+            xv[i][1] = (on && j.y >= 0) ? __ldg(X + o + j.y * Cp) : 0.f;
+            xv[i][2] = (on && j.z >= 0) ? __ldg(X + o + j.z * Cp) : 0.f;
+            xv[i][3] = (on && j.w >= 0) ? __ldg(X + o + j.w * Cp) : 0.f;
+          }
+          // A: hi in place, lo into the second block, while the loads above are in flight
+          if (!mbar_wait_bounded(fullA + s, (q / stages) & 1)) {
+            ok = false;
+            break;
+          }
         }
         float4* ah = reinterpret_cast<float4*>(stage0 + s * sbytes);
         float4* al = ah + TC_BLK / 4;

@@ -65,6 +65,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// Row gather (tensor TMA, tile::gather4): rows y0..y3 of a 2D tensor map whose box is one row high, x the first
+// column, into 4 consecutive box rows at dst; completes on *bar (transaction bytes).  CTA-local, no multicast.
+__device__ __forceinline__ void tma_gather4(void* dst, const void* tmap, int x, int y0, int y1, int y2, int y3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+      "%4, %5, %6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"(tmap), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3), "r"(smem_addr(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
                "r"(bytes)

@@ -161,8 +161,8 @@ void dr_chainset_destroy(dr_chainset* cs);
  * (0 fused x/y plane kernel, 1 the same with bulk prefetch of the state planes,
  * 2 x-line kernel with separate y passes), kriging-product blocks per SM, the
  * iteration time measured when the shape was tuned (0 when it was not), and
- * whether the kriging products run on the tensor cores (1) or as CSR products
- * (0).  At creation the update paths are timed on a scratch chain set of the
+ * whether the kriging products run on the tensor cores (1; 2 when W^T's chain
+ * vectors arrive by TMA row gathers) or as CSR products (0).  At creation the update paths are timed on a scratch chain set of the
  * same shape (with the tensor-core products where available), then the other
  * product choices on the fastest path, and the fastest is kept for the process;
  * DRB_AUTOTUNE=0 turns this off, DRB_NO_PLANE / DRB_PLANE_PREFETCH force a

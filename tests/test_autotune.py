@@ -41,7 +41,8 @@ def test_switches(monkeypatch):
     monkeypatch.delenv("DRB_NO_PLANE", raising=False)
     monkeypatch.delenv("DRB_PLANE_PREFETCH", raising=False)
     data, a = _chains(vol, 2, 5)
-    assert a.config() == {"path": "plane", "blocks_per_sm": 8, "tuned_ms": 0.0, "tensor_products": False}
+    assert a.config() == {"path": "plane", "blocks_per_sm": 8, "tuned_ms": 0.0, "tensor_products": False,
+                          "tma_row_gather": False}
     monkeypatch.setenv("DRB_NO_PLANE", "1")
     b = d.MultiResParameters(data, d.HMCParameters(burnin=4, nsave=3, thin=1, leapfrog=5, seed=2), 2)
     assert b.config()["path"] == "lines"

@@ -101,6 +101,29 @@ def test_c1_tensor_products_match_csr(products):
     a.close(), b.close(), data.close()
 
 
+def test_tma_row_gathers_equal_thread_gathers(products, monkeypatch):
+    """W^T rs with the chain vectors brought in by TMA row gathers (tile::gather4) and with the gather warps' own
+    loads: the MMA operands are the same, so the gradients are bit-identical."""
+    import dualres_b200 as d
+    from dualres_b200 import synth
+    vol = synth.small_volume(seed=63, dims=(16, 15, 13), radius=4.2)
+    data = d.MultiResData.from_volume(vol)
+    rng = np.random.default_rng(9)
+    mus = [_field(data.shape, rng, 0.3) for _ in range(3)]
+    grads = {}
+    for tg in ("1", "0"):
+        monkeypatch.setenv("DRB_TC_TMA_GATHER", tg)
+        ch = products(data, 64, True)
+        assert ch.config()["tma_row_gather"] == (tg == "1")
+        for c, mu in zip((0, 20, 63), mus):
+            ch.set_state(c, mu, (1.3, 2.9))
+        grads[tg] = [ch.gradient(c, mu) for c, mu in zip((0, 20, 63), mus)]
+        ch.close()
+    for a, b in zip(grads["1"], grads["0"]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    data.close()
+
+
 def test_full_run_matches_csr_run(products):
     import dualres_b200 as d
     from dualres_b200 import synth
