@@ -1025,6 +1025,26 @@ static void write_states(Chainset* S, const std::vector<ChainState>& st);
 // per SM); then, on the fastest path, the other product choices (CSR at 8
 // blocks/SM, and at 4 and 2 for chain sets of fewer than 32 chains).  The
 // fastest candidate is kept and cached per shape.
+// Keeps freed device memory in the device's default pool for its scope (the process's pool attribute, restored at
+// the end), so that the tuner's scratch chain sets reuse one another's memory.
+struct PoolKeep {
+  cudaMemPool_t pool{};
+  uint64_t old = 0;
+  bool ok = false;
+  explicit PoolKeep(int dev) {
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &old) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      ok = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
+    }
+    cudaGetLastError();
+  }
+  ~PoolKeep() {
+    if (ok) cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &old);
+    cudaGetLastError();
+  }
+};
+
 static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   const DevVolume& v = V->dv;
   const TuneKey key{V->device, v.E0, v.E1, v.E2, v.bx, v.by, v.bz, C, v.n_h, v.n_s, o->leapfrog};
@@ -1035,6 +1055,7 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   }
   const PathOptions po = path_options(v, V->device);
   const bool tc = tc_chains(C) > 0 && !tc_env_off() && volume_tc(V);
+  const PoolKeep keep(V->device);
   TuneChoice best;
   best.ms = 1e300;
   dr_hmc_opts to = *o;

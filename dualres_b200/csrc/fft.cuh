@@ -266,9 +266,11 @@ struct Plan2 {
   static constexpr int NBM = NB1 > NB2 ? NB1 : NB2;
 };
 
+// Line elements at or beyond rlim are read as zero (they are never loaded), and elements at or beyond wlim are not
+// written (nothing reads them): the pruned input of the first stage and the pruned output of the last.
 template <int N, int R, int P, int DIR, int PER_LANE, class Idx>
 __device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)[PER_LANE], bool on,
-                                            const float2* __restrict__ tw) {
+                                            const float2* __restrict__ tw, int rlim = N, int wlim = N) {
   constexpr int M = N / P, Mn = M / R, NB = N / R;
   float2 x[PER_LANE][R];
 #pragma unroll
@@ -277,7 +279,10 @@ __device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)
     if (on && b < NB) {
       const int p = b / Mn, t = b % Mn;
 #pragma unroll
-      for (int j = 0; j < R; j++) x[q][j] = sm[idx(p * M + t + Mn * j)];
+      for (int j = 0; j < R; j++) {
+        const int i = p * M + t + Mn * j;
+        x[q][j] = i < rlim ? sm[idx(i)] : make_float2(0.f, 0.f);
+      }
       reg_fft<R, DIR>(x[q]);
       if (Mn > 1) {
 #pragma unroll
@@ -296,15 +301,19 @@ __device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)
     if (on && b < NB) {
       const int p = b / Mn, t = b % Mn;
 #pragma unroll
-      for (int k = 0; k < R; k++) sm[idx((p + P * k) * Mn + t)] = x[q][k];
+      for (int k = 0; k < R; k++) {
+        const int i = (p + P * k) * Mn + t;
+        if (i < wlim) sm[idx(i)] = x[q][k];
+      }
     }
   }
   __syncwarp();
 }
 
-// Row FFTs (lines = y rows, elements along x) of a padded plane, all E rows.
+// Row FFTs (lines = y rows, elements along x) of a padded plane, all E rows; x >= rlim read as zero, x >= wlim not
+// written.
 template <int E, int R1, int R2, int DIR>
-__device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict__ tw) {
+__device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict__ tw, int rlim = E, int wlim = E) {
   using PL = PaddedPlane<E>;
   constexpr int NBM = Plan2<E, R1, R2>::NBM, LPW = 32 / NBM;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -315,15 +324,17 @@ __device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict_
     const bool on = li < LPW && y < E;
     const int row = on ? (y + (y >> 3)) * PL::RP : 0;
     auto idx = [row](int i) { return row + i + (i >> 3); };
-    plane_stage<E, R1, 1, DIR, 1>(sm, idx, bl, on, tw);
-    plane_stage<E, R2, R1, DIR, 1>(sm, idx, bl, on, tw);
+    plane_stage<E, R1, 1, DIR, 1>(sm, idx, bl, on, tw, rlim, E);
+    plane_stage<E, R2, R1, DIR, 1>(sm, idx, bl, on, tw, E, wlim);
   }
   __syncthreads();
 }
 
-// Column FFTs (lines = x columns, elements along y) of the first ncols columns.
+// Column FFTs (lines = x columns, elements along y) of the first ncols columns; y >= rlim read as zero, y >= wlim
+// not written.
 template <int E, int R1, int R2, int DIR>
-__device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* __restrict__ tw) {
+__device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* __restrict__ tw, int rlim = E,
+                                           int wlim = E) {
   using PL = PaddedPlane<E>;
   constexpr int NBM = Plan2<E, R1, R2>::NBM, PL_LANE = NBM / 4;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -336,8 +347,8 @@ __device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* 
     const bool on = x < ncols;
     const int col = on ? x + (x >> 3) : 0;
     auto idx = [col](int i) { return (i + (i >> 3)) * PL::RP + col; };
-    plane_stage<E, R1, 1, DIR, PL_LANE>(sm, idx, bl, on, tw);
-    plane_stage<E, R2, R1, DIR, PL_LANE>(sm, idx, bl, on, tw);
+    plane_stage<E, R1, 1, DIR, PL_LANE>(sm, idx, bl, on, tw, rlim, E);
+    plane_stage<E, R2, R1, DIR, PL_LANE>(sm, idx, bl, on, tw, E, wlim);
   }
   __syncthreads();
 }

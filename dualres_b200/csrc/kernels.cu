@@ -363,16 +363,18 @@ __host__ __device__ inline PlaneLayout plane_layout(int E, int plane_elems, bool
   return L;
 }
 
+// The padded planes prune both transforms to the box (ncols x nrows of T2): the inverse transforms read only the
+// box (everything else is zero and is never stored), and the forward transforms write only what lands in it.
 template <int E, bool PREFETCH>
-__device__ __forceinline__ void plane_fft(float2* sm, int ncols, bool rows_first, int dir, const float2* tw) {
+__device__ __forceinline__ void plane_fft(float2* sm, int ncols, int nrows, int dir, const float2* tw) {
   using G = PlaneGeom<E>;
   if constexpr (G::PADDED) {
     if (dir > 0) {
-      plane_cols<E, G::R1, G::R2, +1>(sm, ncols, tw);
-      plane_rows<E, G::R1, G::R2, +1>(sm, tw);
+      plane_cols<E, G::R1, G::R2, +1>(sm, ncols, tw, nrows, E);
+      plane_rows<E, G::R1, G::R2, +1>(sm, tw, ncols, E);
     } else {
-      plane_rows<E, G::R1, G::R2, -1>(sm, tw);
-      plane_cols<E, G::R1, G::R2, -1>(sm, ncols, tw);
+      plane_rows<E, G::R1, G::R2, -1>(sm, tw, E, ncols);
+      plane_cols<E, G::R1, G::R2, -1>(sm, ncols, tw, E, nrows);
     }
   } else {
     if (dir > 0) {
@@ -431,12 +433,20 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
       bulk_g2s(smraw + Ly.s_off, Sg, bs, bar);
     }
   }
-  for (int e = tid; e < E * E; e += NT) {
-    const int y = e / E, x = e % E;
-    sm[G::at(y, x)] = (y < by && x < bx) ? T[y * bx + x] : make_float2(0.f, 0.f);
+  if constexpr (G::PADDED) {
+    // only the box: the pruned inverse transforms read nothing outside it
+    for (int e = tid; e < by * bx; e += NT) {
+      const int y = e / bx, x = e % bx;
+      sm[G::at(y, x)] = T[e];
+    }
+  } else {
+    for (int e = tid; e < E * E; e += NT) {
+      const int y = e / E, x = e % E;
+      sm[G::at(y, x)] = (y < by && x < bx) ? T[y * bx + x] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
-  plane_fft<E, PREFETCH>(sm, bx, false, +1, twE);
+  plane_fft<E, PREFETCH>(sm, bx, by, +1, twE);
   if constexpr (PREFETCH) {
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
@@ -546,7 +556,7 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   }
   if (last) return;
   __syncthreads();
-  plane_fft<E, PREFETCH>(sm, bx, true, -1, twE);
+  plane_fft<E, PREFETCH>(sm, bx, by, -1, twE);
   for (int e = tid; e < by * bx; e += NT) {
     const int y = e / bx, x = e % bx;
     T[y * bx + x] = sm[G::at(y, x)];
