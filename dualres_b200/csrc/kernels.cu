@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   __shared__ int s_ok[CPB], s_hsel[CPB], s_wo[CPB];
+  __shared__ long long s_in0[TL], s_out0[TL];  // per tile line: index of its element 0 in the input / output
   const int cbase = CPB == 1 ? ((a.chain_only >= 0) ? a.chain_only : (int)blockIdx.y) : (int)blockIdx.y * CPB;
   if (threadIdx.x < CPB) {
     // per chain of the tile: active at this step, the half of mu_D / mu_O written, whether mu_O is written
@@ -126,24 +127,28 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
     s_hsel[threadIdx.x] = hs;
     s_wo[threadIdx.x] = wo;
   }
-  __syncthreads();
-  if (CPB == 1 && !s_ok[0]) return;
   const long long lines = (long long)a.A * a.B;
   const long long l0 = (long long)blockIdx.x * LPC;
-  const int nl = (int)min((long long)LPC, lines - l0);
   const int B = a.B, n_in = a.n_in, n_out = a.n_out;
+  if (threadIdx.x < TL) {
+    // line lam = a * B + b starts at (a * n) * B + b; computed once per line rather than per element
+    const long long lam = l0 + threadIdx.x % LPC;
+    const long long aa = lam / B, bb = lam - aa * B;
+    s_in0[threadIdx.x] = aa * n_in * B + bb;
+    s_out0[threadIdx.x] = aa * n_out * B + bb;
+  }
+  __syncthreads();
+  if (CPB == 1 && !s_ok[0]) return;
+  const int nl = (int)min((long long)LPC, lines - l0);
   // tile line l: chain slot l / LPC of the tile, line l0 + l % LPC
   auto valid = [&](int l) { return (l % LPC) < nl && s_ok[l / LPC]; };
   auto chain = [&](int l) { return cbase + l / LPC; };
-  auto line_index = [&](int l, int i, int n) -> long long {
-    const long long lam = l0 + l % LPC;
-    const long long aa = lam / B, bb = lam - aa * B;
-    return (aa * n + i) * B + bb;
-  };
+  auto in_index = [&](int l, int i) -> long long { return s_in0[l] + (long long)i * B; };
+  auto out_index = [&](int l, int k) -> long long { return s_out0[l] + (long long)k * B; };
   auto load = [&](int l, int i) -> C {
     C val = mk((decltype(C().x))0, (decltype(C().x))0);
     if (valid(l) && i < n_in) {
-      const long long idx = line_index(l, i, n_in);
+      const long long idx = in_index(l, i);
       const int c = chain(l);
       if (PRO == PRO_LOAD) {
         val = reinterpret_cast<const C*>(a.in)[(long long)c * a.in_cs + idx];
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
   const auto scale = (decltype(C().x))a.scale;
   auto store = [&](int l, int k) {
     if (!valid(l) || k >= n_out) return;
-    const long long idx = line_index(l, k, n_out);
+    const long long idx = out_index(l, k);
     const int c = chain(l);
     const C val = sm[k * P + l];
     if (EPI == EPI_STORE) {
