@@ -222,10 +222,10 @@ def ess_geyer(x):
     pairs = rho[0:2 * m:2] + rho[1:2 * m:2]           # Gamma_k = rho_2k + rho_2k+1
     pos = pairs > 0
     first_neg = np.where(pos.all(axis=0), m, np.argmin(pos, axis=0))
-    idx = np.arange(m)[:, None]
-    pairs = np.where(idx < first_neg[None, :], pairs, 0.0)
-    pairs = np.minimum.accumulate(np.where(pairs > 0, pairs, np.inf), axis=0)
-    pairs = np.where(np.isfinite(pairs), pairs, 0.0)
+    keep = np.arange(m)[:, None] < first_neg[None, :]   # initial positive sequence
+    # initial monotone sequence: running minimum over the kept pairs; pairs past the truncation count zero
+    pairs = np.minimum.accumulate(np.where(keep, pairs, np.inf), axis=0)
+    pairs = np.where(keep, pairs, 0.0)
     tau = -1.0 + 2.0 * pairs.sum(axis=0)
     tau = np.maximum(tau, 1.0 / np.log10(max(n, 10)))
     return np.where(ok, n / tau, 0.0)

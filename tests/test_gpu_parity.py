@@ -2,12 +2,12 @@
 
 Tolerances (stated per check):
   * eigenvalues: FP64 on both sides, rel 1e-10;
-  * log prior / log likelihood at identical inputs: rel 1e-5 (north-star bar);
+  * log prior / log likelihood at identical inputs: rel 1e-5 (the accuracy bar for this path);
   * gradient: norm-wise rel 1e-5 on well-conditioned spectra; on the fixture
     with 1940/4096 non-positive modes (g2) the bar is 1e-3, because FP32
     rounding of u = IFFT(mu) is amplified by 1/lambda_min (the reference's FP32
     build has the same amplification);
-  * fixed-momentum leapfrog: norm-wise rel 1e-4 (north-star bar);
+  * fixed-momentum leapfrog: norm-wise rel 1e-4 (the trajectory bar for this path);
   * kriging sparsity: bit-exact; weights abs 1e-6.
 """
 import os
