@@ -141,6 +141,10 @@ typedef struct orc_model_f orc_model_f;
    * proposed_energy, 0}; norms[0..1] = squared residual norms at the kept mu. */  \
   double orc_transition##SFX(orc_model##SFX* m, const REAL* z, double u, REAL eps,  \
                              int L, double* out, double* norms);                    \
+  /* The momentum draw alone (MultiResParameters.h:784-815) from injected       \
+   * normals z (as orc_transition): writes p (N complex, re/im interleaved) and   \
+   * returns E0 = -1/2 sum |z|^2.  Uses the current sigma for the mass matrix. */ \
+  double orc_momentum##SFX(orc_model##SFX* m, const REAL* z, REAL* p);              \
   /* Full fit_model loop (gaussian_process_model.h:88-177) with the oracle's own  \
    * RNG.  Outputs (n_o each): mean, var, activation; stats[0..3] = {mh rate,    \
    * final eps, gradient evaluations, iterations}. */                            \

@@ -398,7 +398,7 @@ int64_t orc_kriging_build(const float* hr, int nx, int ny, int nz, const float* 
           continue; /* filled from the shared solution below */
         if (r >= 0 && r == full_ref) continue; /* solved by the r = -1 pass */
         const int cnt = rcnt[rr];
-        if (cnt == 0) continue;
+        if (cnt <= 0) continue;
         for (int a = 0; a < cnt; a++)
           for (int c = 0; c < cnt; c++) A[(long)a * cnt + c] = K[(long)rpid[rr][a] * m + rpid[rr][c]];
         double* w = (double*)malloc(sizeof(double) * cnt);

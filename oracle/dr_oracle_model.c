@@ -470,6 +470,13 @@ double SFX(orc_transition)(MODEL* m, const real* z, double u, real eps, int L, d
   return transition_impl(m, z, u, eps, L, out, norms);
 }
 
+double SFX(orc_momentum)(MODEL* m, const real* z, real* p) {
+  mass_matrix(m);
+  const double E0 = sample_momentum_injected(m, z);
+  memcpy(p, m->momentum, sizeof(cplx) * m->N);
+  return E0;
+}
+
 /* --------------------------- oracle RNG ---------------------------------- */
 /* xoshiro256** seeded by splitmix64; Box-Muller normals; Marsaglia-Tsang gamma. */
 typedef struct { uint64_t s[4]; int have; double cached; } orng;

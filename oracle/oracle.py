@@ -82,6 +82,8 @@ def _declare(L):
         g("orc_leapfrog").argtypes = [C.c_void_p, rp, rp, rt, C.c_int]
         g("orc_transition").argtypes = [C.c_void_p, rp, C.c_double, rt, C.c_int, _f64p, _f64p]
         g("orc_transition").restype = C.c_double
+        g("orc_momentum").argtypes = [C.c_void_p, rp, rp]
+        g("orc_momentum").restype = C.c_double
         g("orc_fit").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64,
                                  _f64p, _f64p, _f64p, _f64p]
         g("orc_fit").restype = C.c_int
@@ -250,6 +252,12 @@ class Model:
         norms = np.zeros(2)
         r = self._f("orc_transition")(self.h, np.ascontiguousarray(z, self.rdt).ravel(), u, eps, L, out, norms)
         return r, out, norms
+
+    def momentum(self, z):
+        """p and E0 from injected normals z (2N reals), as transition() draws them."""
+        out = np.zeros(2 * self.N, self.rdt)
+        e0 = self._f("orc_momentum")(self.h, np.ascontiguousarray(z, self.rdt).ravel(), out)
+        return self._back(out), e0
 
     def fit(self, burnin, n_save, thin, L, mh_target, seed, n_out):
         mean = np.zeros(n_out)
