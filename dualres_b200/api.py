@@ -469,7 +469,8 @@ def debug_dual_averaging(burnin, nsave, thin, L, starting_eps, mhtarget, rates, 
 
 
 KERNEL_NAMES = ["state update (k_xyplane when E0 == E1 <= 128, else k_xline)", "forward y pass (k_pass)", "forward z pass + gather (k_pass)",
-                "W product (k_spmv_w)", "W^T product (k_spmv_wt)", "inverse z pass (k_pass)",
+                "W product (k_tc_product + k_tc_finish from 16 chains, else k_spmv_w)",
+                "W^T product (k_tc_product + k_tc_finish from 16 chains, else k_spmv_wt)", "inverse z pass (k_pass)",
                 "inverse y pass (k_pass)"]
 
 
