@@ -55,3 +55,48 @@ def test_ctypes_mirror_matches_header(c_layout, cname):
     assert c_layout[(cname, "sizeof")] == ctypes.sizeof(cls), cname
     for f, _ in cls._fields_:
         assert c_layout[(cname, f)] == getattr(cls, f).offset, (cname, f)
+
+
+def _header_prototypes():
+    import re
+    src = open(os.path.join(ROOT, "include", "dualres_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for ret, name, args in re.findall(r"\b([A-Za-z_][\w\s\*]*?)\b(dr_\w+)\s*\(([^;{]*?)\)\s*;", src, flags=re.S):
+        args = " ".join(args.split())
+        out[name] = (ret.strip(), [] if args in ("", "void") else [a.strip() for a in args.split(",")])
+    return out
+
+
+def _c_kind(decl):
+    """Coarse kind of one C parameter declaration."""
+    if "*" in decl:
+        return "ptr"
+    t = decl.split()[:-1] if len(decl.split()) > 1 else decl.split()
+    t = " ".join(w for w in t if w != "const")
+    return {"int": "i32", "int64_t": "i64", "uint64_t": "u64", "float": "f32", "double": "f64"}.get(t, t)
+
+
+def _ctypes_kind(t):
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(t, type) and issubclass(t, ctypes._Pointer)):
+        return "ptr"
+    for kind, ct in (("i32", ctypes.c_int), ("i64", ctypes.c_int64), ("u64", ctypes.c_uint64),
+                     ("f32", ctypes.c_float), ("f64", ctypes.c_double)):
+        if t is ct:
+            return kind
+    return repr(t)
+
+
+def test_ctypes_signatures_match_header_prototypes():
+    protos = _header_prototypes()
+    L = api.lib(build_if_missing=False)
+    checked = 0
+    for name, (_, params) in sorted(protos.items()):
+        fn = getattr(L, name, None)
+        if fn is None or fn.argtypes is None:
+            continue
+        assert len(fn.argtypes) == len(params), (name, params, fn.argtypes)
+        for decl, t in zip(params, fn.argtypes):
+            assert _c_kind(decl) == _ctypes_kind(t), (name, decl, t)
+        checked += 1
+    assert checked >= 30, checked
