@@ -81,25 +81,64 @@ struct MODEL {
 
 /* ------------------------------ FFT -------------------------------------- */
 /* Unnormalised DFT, forward exp(-2 pi i jk/n), inverse exp(+2 pi i jk/n)
- * (FFTW convention, sized_fft.h:138-214).  Iterative radix-2. */
+ * (FFTW convention, sized_fft.h:138-214), n a power of two.  Stockham
+ * autosort (C. Van Loan, "Computational Frameworks for the Fast Fourier
+ * Transform", 1992, sec. 1.7) in radix-4 stages, with one radix-2 stage first
+ * when log2 n is odd: each stage reads one buffer and writes the other in
+ * natural order, so no bit reversal is needed and the inner loops run over
+ * contiguous elements.  tw[k] = exp(-2 pi i k / n), k < n/2. */
+static inline cplx tw_at(const cplx* tw, int n, long k, int inverse) {
+  /* exp(-+2 pi i k / n) for 0 <= k < n from the half table (W^(k + n/2) = -W^k) */
+  const cplx w = k < n / 2 ? tw[k] : -tw[k - n / 2];
+  return inverse ? CONJ(w) : w;
+}
+
 static void fft_line(cplx* a, int n, const cplx* tw, int inverse) {
-  for (int i = 1, j = 0; i < n; i++) {
-    int bit = n >> 1;
-    for (; j & bit; bit >>= 1) j ^= bit;
-    j ^= bit;
-    if (i < j) { cplx t = a[i]; a[i] = a[j]; a[j] = t; }
+  if (n < 2) return;
+  cplx work[n];
+  cplx *x = a, *y = work;
+  int m = 1;
+  int lg = 0;
+  while ((1 << lg) < n) lg++;
+  if (lg & 1) {
+    /* one radix-2 stage: y[2j + q] = W_n^(jq) sum_p x[j + p n/2] (-1)^(pq) */
+    const int l = n / 2;
+    for (int j = 0; j < l; j++) {
+      const cplx c0 = x[j], c1 = x[j + l];
+      y[2 * j] = c0 + c1;
+      y[2 * j + 1] = tw_at(tw, n, j, inverse) * (c0 - c1);
+    }
+    cplx* t = x;
+    x = y;
+    y = t;
+    m = 2;
   }
-  for (int len = 2; len <= n; len <<= 1) {
-    const int half = len >> 1, step = n / len;
-    for (int i = 0; i < n; i += len)
-      for (int k = 0; k < half; k++) {
-        cplx w = tw[k * step];
-        if (inverse) w = CONJ(w);
-        const cplx u = a[i + k], v = a[i + k + half] * w;
-        a[i + k] = u + v;
-        a[i + k + half] = u - v;
+  /* radix-4 stages: y[k + 4jm + qm] = W_(4l)^(jq) sum_p x[k + jm + plm] W_4^(pq), l = n / (4m) */
+  for (; m < n; m *= 4) {
+    const int l = n / (4 * m);
+    const long step = n / (4 * l);
+    for (int j = 0; j < l; j++) {
+      const cplx w1 = tw_at(tw, n, j * step, inverse), w2 = tw_at(tw, n, 2 * j * step, inverse),
+                 w3 = tw_at(tw, n, 3 * j * step, inverse);
+      const cplx* x0 = x + (long)j * m;
+      cplx* y0 = y + 4L * j * m;
+      const long lm = (long)l * m;
+      for (int k = 0; k < m; k++) {
+        const cplx a0 = x0[k], a1 = x0[k + lm], a2 = x0[k + 2 * lm], a3 = x0[k + 3 * lm];
+        const cplx b0 = a0 + a2, b1 = a0 - a2, b2 = a1 + a3, d = a1 - a3;
+        /* (a1 - a3) W_4 with W_4 = -i (forward) or +i (inverse) */
+        const cplx b3 = inverse ? (-CIM(d) + CRE(d) * I) : (CIM(d) - CRE(d) * I);
+        y0[k] = b0 + b2;
+        y0[k + m] = w1 * (b1 + b3);
+        y0[k + 2 * m] = w2 * (b0 - b2);
+        y0[k + 3 * m] = w3 * (b1 - b3);
       }
+    }
+    cplx* t = x;
+    x = y;
+    y = t;
   }
+  if (x != a) memcpy(a, x, sizeof(cplx) * n);
 }
 
 static cplx* make_twiddles(int n) {
@@ -111,42 +150,114 @@ static cplx* make_twiddles(int n) {
   return t;
 }
 
+/* FFT_W lines at a time, stored split and line-fastest: element k of line v is
+ * (re[k FFT_W + v], im[k FFT_W + v]).  The stages are fft_line's, with every
+ * butterfly applied to the FFT_W lines in one contiguous (vectorisable) loop. */
+#define FFT_W 16
+static void fft_lines_soa(real* re, real* im, real* wre, real* wim, int n, const cplx* tw, int inverse) {
+  real *xr = re, *xi = im, *yr = wre, *yi = wim, *t;
+  const real sgn = inverse ? (real)1 : (real)-1; /* W_4 = sgn i */
+  int m = 1, lg = 0;
+  while ((1 << lg) < n) lg++;
+  if (lg & 1) {
+    const int l = n / 2;
+    for (int j = 0; j < l; j++) {
+      const cplx w = tw_at(tw, n, j, inverse);
+      const real wr = CRE(w), wi = CIM(w);
+      const real *restrict ar = xr + (long)j * FFT_W, *restrict ai = xi + (long)j * FFT_W;
+      const real *restrict br = ar + (long)l * FFT_W, *restrict bi = ai + (long)l * FFT_W;
+      real *restrict o0r = yr + 2L * j * FFT_W, *restrict o0i = yi + 2L * j * FFT_W;
+      real *restrict o1r = o0r + FFT_W, *restrict o1i = o0i + FFT_W;
+      for (int v = 0; v < FFT_W; v++) {
+        const real dr = ar[v] - br[v], di = ai[v] - bi[v];
+        o0r[v] = ar[v] + br[v];
+        o0i[v] = ai[v] + bi[v];
+        o1r[v] = wr * dr - wi * di;
+        o1i[v] = wr * di + wi * dr;
+      }
+    }
+    t = xr; xr = yr; yr = t;
+    t = xi; xi = yi; yi = t;
+    m = 2;
+  }
+  for (; m < n; m *= 4) {
+    const int l = n / (4 * m);
+    const long lm = (long)l * m * FFT_W;
+    for (int j = 0; j < l; j++) {
+      const cplx w1 = tw_at(tw, n, (long)j * m, inverse), w2 = tw_at(tw, n, 2L * j * m, inverse),
+                 w3 = tw_at(tw, n, 3L * j * m, inverse);
+      const real w1r = CRE(w1), w1i = CIM(w1), w2r = CRE(w2), w2i = CIM(w2), w3r = CRE(w3), w3i = CIM(w3);
+      for (int k = 0; k < m; k++) {
+        const long in = ((long)j * m + k) * FFT_W, out = (4L * j * m + k) * FFT_W, om = (long)m * FFT_W;
+        const real *restrict a0r = xr + in, *restrict a0i = xi + in;
+        real *restrict y0r = yr + out, *restrict y0i = yi + out;
+        for (int v = 0; v < FFT_W; v++) {
+          const real a0x = a0r[v], a0y = a0i[v], a1x = a0r[v + lm], a1y = a0i[v + lm];
+          const real a2x = a0r[v + 2 * lm], a2y = a0i[v + 2 * lm], a3x = a0r[v + 3 * lm], a3y = a0i[v + 3 * lm];
+          const real b0x = a0x + a2x, b0y = a0y + a2y, b1x = a0x - a2x, b1y = a0y - a2y;
+          const real b2x = a1x + a3x, b2y = a1y + a3y, dx = a1x - a3x, dy = a1y - a3y;
+          const real b3x = -sgn * dy, b3y = sgn * dx;
+          const real c1x = b1x + b3x, c1y = b1y + b3y, c2x = b0x - b2x, c2y = b0y - b2y;
+          const real c3x = b1x - b3x, c3y = b1y - b3y;
+          y0r[v] = b0x + b2x;
+          y0i[v] = b0y + b2y;
+          y0r[v + om] = w1r * c1x - w1i * c1y;
+          y0i[v + om] = w1r * c1y + w1i * c1x;
+          y0r[v + 2 * om] = w2r * c2x - w2i * c2y;
+          y0i[v + 2 * om] = w2r * c2y + w2i * c2x;
+          y0r[v + 3 * om] = w3r * c3x - w3i * c3y;
+          y0i[v + 3 * om] = w3r * c3y + w3i * c3x;
+        }
+      }
+    }
+    t = xr; xr = yr; yr = t;
+    t = xi; xi = yi; yi = t;
+  }
+  if (xr != re) {
+    memcpy(re, xr, sizeof(real) * (size_t)n * FFT_W);
+    memcpy(im, xi, sizeof(real) * (size_t)n * FFT_W);
+  }
+}
+
+/* Transforms the lines a[o ostride + s sstride + k kstride], k < n, for
+ * s < inner and o < outer, FFT_W values of s at a time. */
+static void fft_pass(cplx* a, int n, long kstride, long sstride, long inner, long outer, long ostride,
+                     const cplx* tw, int inverse) {
+  const long nblk = (inner + FFT_W - 1) / FFT_W;
+#pragma omp parallel
+  {
+    real* buf = (real*)malloc(sizeof(real) * 4 * (size_t)n * FFT_W);
+    real *re = buf, *im = buf + (size_t)n * FFT_W, *wre = im + (size_t)n * FFT_W, *wim = wre + (size_t)n * FFT_W;
+#pragma omp for schedule(static) collapse(2)
+    for (long o = 0; o < outer; o++)
+      for (long b = 0; b < nblk; b++) {
+        const long s0 = b * FFT_W;
+        const int w = (int)(inner - s0 < FFT_W ? inner - s0 : FFT_W);
+        cplx* base = a + o * ostride + s0 * sstride;
+        for (int k = 0; k < n; k++) {
+          int v = 0;
+          for (; v < w; v++) {
+            const cplx c = base[v * sstride + (long)k * kstride];
+            re[(long)k * FFT_W + v] = CRE(c);
+            im[(long)k * FFT_W + v] = CIM(c);
+          }
+          for (; v < FFT_W; v++) re[(long)k * FFT_W + v] = im[(long)k * FFT_W + v] = 0;
+        }
+        fft_lines_soa(re, im, wre, wim, n, tw, inverse);
+        for (int k = 0; k < n; k++)
+          for (int v = 0; v < w; v++)
+            base[v * sstride + (long)k * kstride] = re[(long)k * FFT_W + v] + im[(long)k * FFT_W + v] * I;
+      }
+    free(buf);
+  }
+}
+
 static void fft3d_tw(cplx* a, const int* E, cplx* const* tw, int inverse) {
-  const int E0 = E[0], E1 = E[1], E2 = E[2];
-  const long lines0 = (long)E1 * E2;
-  if (E0 > 1) {
-#pragma omp parallel for schedule(static)
-    for (long l = 0; l < lines0; l++) fft_line(a + l * E0, E0, tw[0], inverse);
-  }
-  if (E1 > 1) {
-#pragma omp parallel
-    {
-      cplx* tmp = (cplx*)malloc(sizeof(cplx) * E1);
-#pragma omp for schedule(static)
-      for (long l = 0; l < (long)E0 * E2; l++) {
-        const long x = l % E0, z = l / E0;
-        cplx* base = a + z * (long)E0 * E1 + x;
-        for (int y = 0; y < E1; y++) tmp[y] = base[(long)y * E0];
-        fft_line(tmp, E1, tw[1], inverse);
-        for (int y = 0; y < E1; y++) base[(long)y * E0] = tmp[y];
-      }
-      free(tmp);
-    }
-  }
-  if (E2 > 1) {
-#pragma omp parallel
-    {
-      cplx* tmp = (cplx*)malloc(sizeof(cplx) * E2);
-#pragma omp for schedule(static)
-      for (long l = 0; l < (long)E0 * E1; l++) {
-        cplx* base = a + l;
-        for (int z = 0; z < E2; z++) tmp[z] = base[(long)z * E0 * E1];
-        fft_line(tmp, E2, tw[2], inverse);
-        for (int z = 0; z < E2; z++) base[(long)z * E0 * E1] = tmp[z];
-      }
-      free(tmp);
-    }
-  }
+  const long E0 = E[0], E1 = E[1], E2 = E[2];
+  /* x lines: start (z E1 + y) E0; y lines: start z E0 E1 + x, stride E0; z lines: start y E0 + x, stride E0 E1 */
+  if (E0 > 1) fft_pass(a, (int)E0, 1, E0, E1 * E2, 1, 0, tw[0], inverse);
+  if (E1 > 1) fft_pass(a, (int)E1, E0, 1, E0, E2, E0 * E1, tw[1], inverse);
+  if (E2 > 1) fft_pass(a, (int)E2, E0 * E1, 1, E0 * E1, 1, 0, tw[2], inverse);
 }
 
 void SFX(orc_fft3d)(real* data, const int* E, int inverse) {

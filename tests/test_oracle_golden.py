@@ -35,6 +35,17 @@ def test_fft_known_answers(oracle):
     assert rel(oracle.fft3d(x, False, "f"), np.fft.fftn(x)) < 1e-6
 
 
+@pytest.mark.parametrize("shape", [(2, 4, 8), (32, 2, 1), (1, 128, 2), (256, 1, 4), (2, 2, 512), (64, 64, 64)])
+def test_fft_radix_stages_against_numpy(oracle, shape):
+    """Every power-of-two length (odd and even log2, so with and without the radix-2 stage) on every axis,
+    lines fewer and more than the 16 the passes transform at once."""
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    assert rel(oracle.fft3d(x, False), np.fft.fftn(x)) < 1e-13
+    assert rel(oracle.fft3d(x, True), np.fft.ifftn(x) * x.size) < 1e-13
+    assert rel(oracle.fft3d(x, False, "f"), np.fft.fftn(x)) < 2e-6
+
+
 def test_embedding_rule(oracle):
     E = np.zeros(3, np.int32)
     assert oracle.lib().orc_embedding_dims(np.array([32, 32, 32], np.int32), E) == 0
