@@ -93,54 +93,6 @@ static inline cplx tw_at(const cplx* tw, int n, long k, int inverse) {
   return inverse ? CONJ(w) : w;
 }
 
-static void fft_line(cplx* a, int n, const cplx* tw, int inverse) {
-  if (n < 2) return;
-  cplx work[n];
-  cplx *x = a, *y = work;
-  int m = 1;
-  int lg = 0;
-  while ((1 << lg) < n) lg++;
-  if (lg & 1) {
-    /* one radix-2 stage: y[2j + q] = W_n^(jq) sum_p x[j + p n/2] (-1)^(pq) */
-    const int l = n / 2;
-    for (int j = 0; j < l; j++) {
-      const cplx c0 = x[j], c1 = x[j + l];
-      y[2 * j] = c0 + c1;
-      y[2 * j + 1] = tw_at(tw, n, j, inverse) * (c0 - c1);
-    }
-    cplx* t = x;
-    x = y;
-    y = t;
-    m = 2;
-  }
-  /* radix-4 stages: y[k + 4jm + qm] = W_(4l)^(jq) sum_p x[k + jm + plm] W_4^(pq), l = n / (4m) */
-  for (; m < n; m *= 4) {
-    const int l = n / (4 * m);
-    const long step = n / (4 * l);
-    for (int j = 0; j < l; j++) {
-      const cplx w1 = tw_at(tw, n, j * step, inverse), w2 = tw_at(tw, n, 2 * j * step, inverse),
-                 w3 = tw_at(tw, n, 3 * j * step, inverse);
-      const cplx* x0 = x + (long)j * m;
-      cplx* y0 = y + 4L * j * m;
-      const long lm = (long)l * m;
-      for (int k = 0; k < m; k++) {
-        const cplx a0 = x0[k], a1 = x0[k + lm], a2 = x0[k + 2 * lm], a3 = x0[k + 3 * lm];
-        const cplx b0 = a0 + a2, b1 = a0 - a2, b2 = a1 + a3, d = a1 - a3;
-        /* (a1 - a3) W_4 with W_4 = -i (forward) or +i (inverse) */
-        const cplx b3 = inverse ? (-CIM(d) + CRE(d) * I) : (CIM(d) - CRE(d) * I);
-        y0[k] = b0 + b2;
-        y0[k + m] = w1 * (b1 + b3);
-        y0[k + 2 * m] = w2 * (b0 - b2);
-        y0[k + 3 * m] = w3 * (b1 - b3);
-      }
-    }
-    cplx* t = x;
-    x = y;
-    y = t;
-  }
-  if (x != a) memcpy(a, x, sizeof(cplx) * n);
-}
-
 static cplx* make_twiddles(int n) {
   cplx* t = (cplx*)malloc(sizeof(cplx) * (n > 1 ? n / 2 : 1));
   for (int k = 0; k < n / 2; k++) {
@@ -151,8 +103,11 @@ static cplx* make_twiddles(int n) {
 }
 
 /* FFT_W lines at a time, stored split and line-fastest: element k of line v is
- * (re[k FFT_W + v], im[k FFT_W + v]).  The stages are fft_line's, with every
- * butterfly applied to the FFT_W lines in one contiguous (vectorisable) loop. */
+ * (re[k FFT_W + v], im[k FFT_W + v]).  Stage with m points per sub-transform
+ * and l = n / (r m) groups (radix r = 2 or 4, W_r = exp(-+2 pi i / r)):
+ *   y[k + r j m + q m] = W_(r l)^(j q) sum_p x[k + j m + p l m] W_r^(p q),
+ * every butterfly applied to the FFT_W lines in one contiguous (vectorisable)
+ * loop.  The result is in re/im; wre/wim are the other buffer. */
 #define FFT_W 16
 static void fft_lines_soa(real* re, real* im, real* wre, real* wim, int n, const cplx* tw, int inverse) {
   real *xr = re, *xi = im, *yr = wre, *yi = wim, *t;
