@@ -355,6 +355,14 @@ def run_ours(args, dist):
                                             "GBps_algorithmic": v[2] / (v[1] / 1e3) / 1e9}
                     for k, v in per_iter.items()}}
     info = data.info
+    try:  # the same rate in the reference's byte model (four FFTs per step); the spectral formulation moves less
+        b_ref = reference_bytes_per_step(int(info.N), int(info.kriging_nnz), C, int(info.n_highres),
+                                         int(info.n_stdres))
+        gbs_ref = b_ref * grads / (ms / 1e3) / 1e9   # one gradient evaluation per leapfrog step, this GPU
+        roofline["reference_formulation"] = {"bytes_per_chain_step": b_ref, "equivalent_GBps": gbs_ref,
+                                             "frac_of_peak": gbs_ref / peak[0]}
+    except Exception as e:  # an accounting extra must not break the benchmark line
+        roofline["reference_formulation"] = {"error": str(e)[:200]}
     cfg = config_of(args.workload, {
         "global_batch": C * dist.world, "l2": "working set larger than L2 (state 0.5 GB per GPU)",
         "n_highres": info.n_highres, "n_stdres": info.n_stdres, "kriging_nnz": int(info.kriging_nnz),
@@ -579,6 +587,13 @@ def run_served(args, dist):
     }
     sv.close()
     return line
+
+
+def reference_bytes_per_step(N, nnz, chains, n_h, n_s):
+    """Algorithmic bytes of one leapfrog step of one chain in the reference's formulation (four full complex64 3D
+    FFTs per step, real-space state): 104 N + 16 nnz / C + 12 n_h + 8 n_s, with the kriging matrix (values and
+    columns, read for W x and W^T r) shared by the C chains of one volume."""
+    return 104.0 * N + 16.0 * nnz / chains + 12.0 * n_h + 8.0 * n_s
 
 
 def peaks():

@@ -50,3 +50,10 @@ def test_config_names_the_workload_and_its_sizes():
     assert cfg["workload"] == "batched64"
     assert cfg["chains"] == 64 and cfg["leapfrog"] == 25
     assert (cfg["burnin"], cfg["nsave"], cfg["thin"]) == (500, 500, 3)
+
+
+def test_reference_byte_model_on_the_32cubed_volume():
+    # 64^3 embedding, 2,467,584 kriging nonzeros shared by 64 chains, 19,660 / 2,298 data voxels
+    b = bench.reference_bytes_per_step(64 ** 3, 2467584, 64, 19660, 2298)
+    assert abs(b - (104 * 262144 + 16 * 2467584 / 64 + 12 * 19660 + 8 * 2298)) < 1e-6
+    assert 28.0e6 < b < 28.3e6
