@@ -131,3 +131,17 @@ def test_cli_rejects_invalid_covariance(tmp_path):
 
 def test_cli_exists_next_to_the_library():
     assert os.path.dirname(api.cli_path()) == os.path.dirname(api.lib_path())
+
+
+# Every option the reference's parser accepts (include/dualres/impl/CommandParser/GPMCommandParser.inl:219-606)
+REFERENCE_OPTIONS = ["--burnin", "--covariance", "--debug", "--help", "--highres", "--hmask", "--leapfrog",
+                     "--mhtarget", "--monitor", "--neighborhood", "--nsave", "--omask", "--output",
+                     "--rational-quadratic", "--samples", "--seed", "--smask", "--stdres", "--theta", "--thin",
+                     "--threads"]
+
+
+def test_cli_accepts_every_reference_option(tmp_path):
+    r = _run(["--help"], tmp_path)
+    assert r.returncode == 0                        # --help itself is accepted; the others are listed
+    missing = [o for o in REFERENCE_OPTIONS if o != "--help" and o not in r.stderr + r.stdout]
+    assert not missing, missing
