@@ -432,6 +432,8 @@ static void gradient_impl(MODEL* m, const cplx* mu_star) {
     for (int i = 0; i < m->n_h; i++) m->sub_grad[i] += m->sigma_sq_inv[1] * acc[i];
     free(acc);
   }
+  /* the scatter runs in parallel, as MultiResParameters.h:370 does (D holds distinct indices) */
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < m->n_h; i++) m->temp[m->D[i]] += m->sub_grad[i];
 }
 
