@@ -576,8 +576,6 @@ struct Chainset {
   int64_t graph_nodes = 0;
   std::vector<void*> allocs;
   float2* tmp = nullptr;        // [N] scratch for evaluation calls
-  double* tmp_part = nullptr;   // spectral-energy partials
-  int tmp_blocks = 0;
   int NR = 1;
   bool plane = false;           // fused xy-plane update (E0 == E1 <= 128)
   int path = 0;                 // 0 plane kernel, 1 plane kernel with bulk prefetch, 2 x-line kernel + y passes
@@ -608,6 +606,10 @@ struct Chainset {
   int device = 0;
   ~Chainset() {
     cudaSetDevice(device);
+    // Drain the chain set's work before anything is freed: its kernels read the volume's arrays, and the volume
+    // frees them on its own stream, which is not ordered after this one (a chain set destroyed on an error path
+    // may still have work in flight).
+    if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
     if (done_event) cudaEventDestroy(done_event);
     if (stream) {
@@ -1212,8 +1214,6 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   ch.chain0 = 0;
   ch.err = S->alloc<int>(1);
   S->tmp = S->alloc<float2>(N);
-  S->tmp_blocks = 296;
-  S->tmp_part = S->alloc<double>(S->tmp_blocks);
   init_chain_states(S);
 
   // initial state: sigma, then u0 = IFFT(scatter(Yh)) + sqrt(N lambda) w / 10, then mu at data/output voxels
@@ -1359,18 +1359,6 @@ static void gather_data(Chainset* S, const float2* field, int c, int half, bool 
   }
 }
 
-static double spectral_energy(Chainset* S, const float2* u, float sh, int mode) {
-  const DevVolume& v = S->vol->dv;
-  k_spectral_energy<<<S->tmp_blocks, 256, 0, S->stream>>>(u, v.sinv, v.N, sh, mode, S->tmp_part);
-  CK_LAUNCH();
-  std::vector<double> h(S->tmp_blocks);
-  CK(cudaMemcpyAsync(h.data(), S->tmp_part, sizeof(double) * S->tmp_blocks, cudaMemcpyDeviceToHost, S->stream));
-  CK(cudaStreamSynchronize(S->stream));
-  double s = 0.0;
-  for (double x : h) s += x;
-  return s;
-}
-
 static double part_sum(Chainset* S, int c, int slot, int nb) {
   std::vector<double> h(nb);
   CK(cudaMemcpyAsync(h.data(), S->dc.part + ((long long)c * NSLOT + slot) * S->dc.maxblk, sizeof(double) * nb,
@@ -1381,10 +1369,56 @@ static double part_sum(Chainset* S, int c, int slot, int nb) {
   return s;
 }
 
-// data-term residual norms and gD for chain c from muD half `half` (sel relative to acc)
-static void data_term(Chainset* S, int c, int sel) {
-  if (S->vol->dv.n_s > 0) launch_spmv(S, -1, sel, c, true);
-  launch_spmv(S, -1, sel, c, false);
+// Log prior, log likelihood (lpll[0..1]) and gradient (grad, 2N floats) at mu through the sampler's own kernels:
+// step 0 of the leapfrog sequence (kriging products on the chain set's path, the inverse z pass, then the plane or
+// x-line kernel) from a zero momentum, with eps = 2 so that the half kick is exactly 1 and no drift, because the
+// step is both the first and the last.  The momentum it leaves is q = IFFT(gradient) in the spectral basis, and
+// its step-0 partial sums are the energies at mu.  It works in the proposal half of the chain's buffers and in the
+// momentum, which hold nothing between iterations, so the chain's state is unchanged.
+static void eval_sampler(Chainset* S, int chain, const float* mu, double* lpll, float* grad) {
+  CK(cudaSetDevice(S->vol->device));
+  const DevVolume& v = S->vol->dv;
+  std::vector<ChainState> st, saved;
+  read_states(S, &st);
+  saved = st;
+  const int half = st[chain].acc ^ 1;
+  DevChains none{};
+  upload_field(S, mu);
+  gather_data(S, S->tmp, chain, half, false);
+  fft3d<float2>(S->tmp, S->vol->hv.E, +1, 0, 1, S->vol->tw_f, S->stream, v, none);
+  CK(cudaMemcpyAsync(S->dc.U + ((long long)chain * 2 + half) * v.N, S->tmp, sizeof(float2) * v.N,
+                     cudaMemcpyDeviceToDevice, S->stream));
+  CK(cudaMemsetAsync(S->dc.Q + (long long)chain * v.N, 0, sizeof(float2) * v.N, S->stream));
+  for (int c = 0; c < S->C; c++) st[c].L_cur = -1;
+  st[chain].L_cur = 0;
+  st[chain].eps_cur = 2.0f;
+  st[chain].acc = half;
+  write_states(S, st);
+  try {
+    enqueue_steps(S, 0, XF_FIXED_MOMENTUM | XF_WRITE_Q_LAST);
+    if (lpll) {
+      const double lp = part_sum(S, chain, SL_LP0, S->dc.nb_x);
+      const double Rh = part_sum(S, chain, SL_RH0, S->dc.nb_wt);
+      const double Rs = v.n_s > 0 ? part_sum(S, chain, SL_RS0, S->dc.nb_w) : 0.0;
+      lpll[0] = -0.5 * lp / (double)v.N;
+      lpll[1] = -0.5 * ((double)st[chain].sh * Rh + (v.n_s > 0 ? (double)st[chain].ss * Rs : 0.0));
+    }
+    if (grad) {
+      CK(cudaMemcpyAsync(S->tmp, S->dc.Q + (long long)chain * v.N, sizeof(float2) * v.N, cudaMemcpyDeviceToDevice,
+                         S->stream));
+      fft3d<float2>(S->tmp, S->vol->hv.E, -1, 0, 1, S->vol->tw_f, S->stream, v, none);
+      k_scale<<<cdiv_i(v.N, 256), 256, 0, S->stream>>>(S->tmp, v.N, 1.0f / (float)v.N);
+      CK_LAUNCH();
+      CK(cudaMemcpyAsync(grad, S->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToHost, S->stream));
+    }
+    CK(cudaStreamSynchronize(S->stream));
+  } catch (...) {
+    cudaStreamSynchronize(S->stream);
+    write_states(S, saved);
+    throw;
+  }
+  write_states(S, saved);
+  check_device_error(S);
 }
 
 }  // namespace drb
@@ -1664,43 +1698,14 @@ int dr_get_state(dr_chainset* s, int chain, float* mu, float* s2inv) {
 int dr_log_posterior(dr_chainset* s, int chain, const float* mu, double* out) {
   API_BEGIN
   if (!s || !mu || !out || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");
-  CK(cudaSetDevice(s->vol->device));
-  std::vector<ChainState> st;
-  read_states(s, &st);
-  const DevVolume& v = s->vol->dv;
-  const ChainState& h = st[chain];
-  upload_field(s, mu);
-  gather_data(s, s->tmp, chain, h.acc ^ 1, false);
-  data_term(s, chain, 1);
-  const double Rh = part_sum(s, chain, SL_RH0, s->dc.nb_wt);
-  const double Rs = v.n_s > 0 ? part_sum(s, chain, SL_RS0, s->dc.nb_w) : 0.0;
-  DevChains none{};
-  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
-  const double e = spectral_energy(s, s->tmp, h.sh, 0);
-  out[0] = -0.5 * e / (double)v.N;
-  out[1] = -0.5 * ((double)h.sh * Rh + (v.n_s > 0 ? (double)h.ss * Rs : 0.0));
+  eval_sampler(s, chain, mu, out, nullptr);
   API_END
 }
 
 int dr_gradient(dr_chainset* s, int chain, const float* mu, float* grad) {
   API_BEGIN
   if (!s || !mu || !grad || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");
-  CK(cudaSetDevice(s->vol->device));
-  std::vector<ChainState> st;
-  read_states(s, &st);
-  const DevVolume& v = s->vol->dv;
-  upload_field(s, mu);
-  gather_data(s, s->tmp, chain, st[chain].acc ^ 1, false);
-  data_term(s, chain, 1);
-  DevChains none{};
-  fft3d<float2>(s->tmp, s->vol->hv.E, +1, 0, 1, s->vol->tw_f, s->stream, v, none);
-  k_prior_grad_spectral<<<cdiv_i(v.N, 256), 256, 0, s->stream>>>(s->tmp, v.sinv, v.N);
-  CK_LAUNCH();
-  fft3d<float2>(s->tmp, s->vol->hv.E, -1, 0, 1, s->vol->tw_f, s->stream, v, none);
-  k_scatter_add_re<<<cdiv_i(v.n_h, 256), 256, 0, s->stream>>>(s->tmp, v.d_flat, v.n_h, s->dc.gD, s->C, chain);
-  CK_LAUNCH();
-  CK(cudaMemcpyAsync(grad, s->tmp, sizeof(float2) * v.N, cudaMemcpyDeviceToHost, s->stream));
-  CK(cudaStreamSynchronize(s->stream));
+  eval_sampler(s, chain, mu, nullptr, grad);
   API_END
 }
 
@@ -2092,14 +2097,14 @@ struct Server {
     }
   }
 
+  // Reads a finished job's summary and frees its device objects; the fields that dr_server_status and
+  // dr_server_result read are published under mtx together with the DONE state.
   void finalize(const std::shared_ptr<Job>& j) {
     Chainset* cs = j->cs.get();
     check_device_error(cs);
-    j->n_output = cs->vol->dv.n_o;
-    j->mean.resize(j->n_output);
-    j->var.resize(j->n_output);
-    j->act.resize(j->n_output);
-    summary_of(cs, -1, j->mean.data(), j->var.data(), j->act.data());
+    const int n_output = cs->vol->dv.n_o;
+    std::vector<float> mean(n_output), var(n_output), act(n_output);
+    summary_of(cs, -1, mean.data(), var.data(), act.data());
     std::vector<ChainState> st;
     read_states(cs, &st);
     int64_t g = 0;
@@ -2109,10 +2114,33 @@ struct Server {
       const int d = h.iteration - h.burnin;
       mh += h.mh_running_sum / std::max(d, 1);
     }
-    j->grads = g;
-    j->mh = (float)(mh / st.size());
     j->cs.reset();
     j->vol.reset();
+    std::lock_guard<std::mutex> lk(mtx);
+    j->n_output = n_output;
+    j->mean = std::move(mean);
+    j->var = std::move(var);
+    j->act = std::move(act);
+    j->grads = g;
+    j->mh = (float)(mh / st.size());
+    const int64_t b = j->bytes;
+    j->state = DR_JOB_DONE;
+    j->t_finish = now();
+    in_use -= b;
+    n_done++;
+    grads_done += j->grads;
+    last_finish = j->t_finish;
+    cv_done.notify_all();
+  }
+
+  // Frees a failed job's device objects (the chain set drains its stream first) and records the failure.
+  void fail_resident(const std::shared_ptr<Job>& j, int code, const std::string& msg, bool counted) {
+    j->cs.reset();
+    j->vol.reset();
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lk(mtx);
+    if (counted) in_use -= j->bytes;
+    fail(j, code, msg);
   }
 
   void scheduler_loop() {
@@ -2128,21 +2156,26 @@ struct Server {
           if (in_use + j->est_bytes > budget && !active.empty()) break;
           ready_q.pop_front();
         }
+        int64_t bytes = 0;
         try {
           volume_build_device(j->vol.get(), j->desc.covariance, j->desc.covfun, o.device);
           auto cs = std::make_unique<Chainset>();
           chainset_build(cs.get(), j->vol.get(), j->C, &j->opts);
-          j->bytes = j->vol->bytes + cs->bytes;
+          bytes = j->vol->bytes + cs->bytes;
           j->cs = std::move(cs);
           j->iters_total = j->opts.burnin + (j->opts.thin == 0 ? 1 : j->opts.thin) * j->opts.nsave;
         } catch (const Error& e) {
-          j->cs.reset();
-          j->vol.reset();
-          std::lock_guard<std::mutex> lk(mtx);
-          fail(j, e.code, e.what());
+          fail_resident(j, e.code, e.what(), false);
+          continue;
+        } catch (const std::bad_alloc&) {
+          fail_resident(j, DR_ERR_NOMEM, "host allocation failed", false);
+          continue;
+        } catch (const std::exception& e) {
+          fail_resident(j, DR_ERR_INVALID, e.what(), false);
           continue;
         }
         std::lock_guard<std::mutex> lk(mtx);
+        j->bytes = bytes;
         j->state = DR_JOB_RUNNING;
         j->t_admit = now();
         in_use += j->bytes;
@@ -2170,24 +2203,14 @@ struct Server {
             j->in_flight = true;
             launched = true;
           } else {
-            const int64_t b = j->bytes;
             finalize(j);
-            std::lock_guard<std::mutex> lk(mtx);
-            j->state = DR_JOB_DONE;
-            j->t_finish = now();
-            in_use -= b;
-            n_done++;
-            grads_done += j->grads;
-            last_finish = j->t_finish;
-            cv_done.notify_all();
           }
         } catch (const Error& e) {
-          const int64_t b = j->bytes;
-          j->cs.reset();
-          j->vol.reset();
-          std::lock_guard<std::mutex> lk(mtx);
-          in_use -= b;
-          fail(j, e.code, e.what());
+          fail_resident(j, e.code, e.what(), true);
+        } catch (const std::bad_alloc&) {
+          fail_resident(j, DR_ERR_NOMEM, "host allocation failed", true);
+        } catch (const std::exception& e) {
+          fail_resident(j, DR_ERR_INVALID, e.what(), true);
         }
       }
       active.erase(std::remove_if(active.begin(), active.end(),
@@ -2553,6 +2576,18 @@ __global__ void k_noalloc_finish(const double* epart, int neblk, const double* p
 
 }  // namespace drb
 
+// Makes `dev` current for its scope and gives the caller's current device back at the end, on success and on error.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    CK(cudaSetDevice(dev));
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 extern "C" int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_device, float s_hr, float s_sr,
                                         double* out) {
   API_BEGIN
@@ -2563,7 +2598,7 @@ extern "C" int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_devi
                                         " points exceeds the scratch limit of 2^21 (use dr_log_posterior)");
   if (dv.n_h > NA_MAX_ROWS || dv.n_s > NA_MAX_ROWS)
     throw Error(DR_ERR_UNSUPPORTED, "dr_log_posterior_noalloc: more than 2^20 data voxels (use dr_log_posterior)");
-  CK(cudaSetDevice(v->device));
+  const DeviceScope scope(v->device);
   unsigned char* base = noalloc_scratch(v->device);
   float2* field = (float2*)(base + NA_FIELD);
   ChainState* st = (ChainState*)(base + NA_ST);

@@ -293,7 +293,9 @@ __global__ void __launch_bounds__(XCfg<E0>::NT) k_xline(DevVolume v, DevChains c
       q.y = fmaf(keps, gt.y, q.y);
       float2 un = u;
       if (last) {
-        if (live) {
+        // the final energies; a step that is both first and last only evaluates (a gradient / log posterior
+        // call) and keeps the energies at mu
+        if (live && !first) {
           pa += (double)(u.x * u.x + u.y * u.y) * (double)s;
           pb += (double)(q.x * q.x + q.y * q.y) / (double)lm;
         }
@@ -536,7 +538,7 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
         q.y = fmaf(keps, gt.y, q.y);
         float2 un = u;
         if (last) {
-          if (live) {
+          if (live && !first) {  // first and last: an evaluation step, energies at mu only
             pa += (double)(u.x * u.x + u.y * u.y) * (double)s;
             pb += (double)(q.x * q.x + q.y * q.y) / (double)lm;
           }
@@ -961,20 +963,6 @@ __global__ void k_spectrum(const double2* lam, float* sinv, double* lam_re, long
 __global__ void k_gather_re(const float2* field, const int* idx, int n, float* out, int pitch, int col) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n) out[(long long)j * pitch + col] = field[idx[j]].x;
-}
-
-// u <- -u sinv / N on live modes, 0 on S (prior part of the gradient before the forward FFT).
-__global__ void k_prior_grad_spectral(float2* u, const float* sinv, long long N) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const float s = sinv[i];
-  const float f = s > 0.f ? -s / (float)N : 0.f;
-  u[i] = make_float2(u[i].x * f, u[i].y * f);
-}
-
-__global__ void k_scatter_add_re(float2* field, const int* idx, int n, const float* vals, int pitch, int col) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) field[idx[j]].x += vals[(long long)j * pitch + col];
 }
 
 // Block partials of sum_live |u|^2 * sinv  (mode 0) or sum_live |u|^2 / (sinv + sh)  (mode 1).

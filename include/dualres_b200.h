@@ -205,7 +205,11 @@ int dr_leapfrog_fixed(dr_chainset* cs, int chain, const float* mu0, const float*
  * first call before any stream capture.  All calls share the array: calls
  * that overlap on the GPU (several host threads, or several devices sharing a
  * context) race, so serialise them.  The call runs on the legacy default
- * stream and returns when the result is on the host. */
+ * stream and returns when the result is on the host.  The legacy stream is
+ * not ordered after work on streams created with cudaStreamNonBlocking, so
+ * the writes that produce mu_device must be finished before the call
+ * (synchronise the producing stream, or produce mu_device on the legacy
+ * stream).  The caller's current device is the same after the call. */
 int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_device, float s_hr, float s_sr, double* out);
 
 /* ---- serving: continuous batching of denoising jobs --------------------- */

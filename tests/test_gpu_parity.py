@@ -1,12 +1,18 @@
 """GPU parity of the CUDA path against the FP64 oracle and the golden fixtures.
 
+dr_log_posterior and dr_gradient run step 0 of the sampler's own leapfrog
+sequence (kriging products, inverse z pass, plane or x-line kernel), so these
+bars apply to the kernels the sampler runs, on each of its update paths.
+
 Tolerances (stated per check):
   * eigenvalues: FP64 on both sides, rel 1e-10;
   * log prior / log likelihood at identical inputs: rel 1e-5 (the accuracy bar for this path);
   * gradient: norm-wise rel 1e-5 on well-conditioned spectra; on the fixture
     with 1940/4096 non-positive modes (g2) the bar is 1e-3, because FP32
-    rounding of u = IFFT(mu) is amplified by 1/lambda_min (the reference's FP32
-    build has the same amplification);
+    rounding of u = IFFT(mu) is amplified by 1/lambda_min.  There the
+    reference's own FP32 arithmetic (the oracle's FP32 build: four FP32 FFTs
+    and an FP32 spectrum) is off by 0.22 on the same input, and the device
+    must stay at least 100x closer to FP64 than that;
   * fixed-momentum leapfrog: norm-wise rel 1e-4 (the trajectory bar for this path);
   * kriging sparsity: bit-exact; weights abs 1e-6.
 """
@@ -58,9 +64,9 @@ def chains_of(vol, n=1, **kw):
     return d.MultiResParameters(vol, hmc, n)
 
 
-def oracle_model(oracle, g):
+def oracle_model(oracle, g, precision="d"):
     W = (g["W_rowptr"], g["W_col"], g["W_val"])
-    m = oracle.Model(g["D"], g["Yh"], g["qform_hr"], tuple(g["theta"]), g["Ys"], W, g["O"])
+    m = oracle.Model(g["D"], g["Yh"], g["qform_hr"], tuple(g["theta"]), g["Ys"], W, g["O"], precision=precision)
     m.set_sigma(*g["sigma"])
     return m
 
@@ -96,11 +102,18 @@ def test_log_posterior_and_gradient(oracle, name, update_path):
     assert abs(lp / float(g["log_prior"]) - 1) < 1e-5
     assert abs(ll / float(g["log_likelihood"]) - 1) < 1e-5
     grad = p.gradient(0, mu)
-    tol = 1e-3 if int(g["n_S"]) > 0.1 * mu.size else 1e-5
-    assert rel(grad, g["grad"]) < tol
+    ill = int(g["n_S"]) > 0.1 * mu.size
+    tol = 1e-3 if ill else 1e-5
+    r = rel(grad, g["grad"])
+    assert r < tol, r
     # the oracle (FP64) agrees with the fixture
     m = oracle_model(oracle, g)
     assert abs(m.log_prior(mu) / lp - 1) < 1e-5
+    if ill:
+        # the reference's FP32 arithmetic on the same input, for scale
+        r32 = rel(oracle_model(oracle, g, "f").gradient(mu), g["grad"])
+        print(f"{name}: device gradient rel {r:.2e}, reference FP32 arithmetic rel {r32:.2e}")
+        assert r < 0.01 * r32, (r, r32)
 
 
 @pytest.mark.parametrize("name", golden_cases())
@@ -203,3 +216,28 @@ def test_chain_is_independent_of_batch(update_path):
     b, sb = p4.get_state(0)
     assert rel(b, a) < 1e-4
     assert abs(sa[0] / sb[0] - 1) < 1e-4
+
+
+def test_evaluation_leaves_the_chain_state_unchanged(update_path):
+    """dr_gradient and dr_log_posterior run the sampler's step 0 in the proposal half of the chain's buffers: the
+    accepted state, sigma and the next iterations are those of a chain set that was never evaluated."""
+    import dualres_b200 as d
+    g = load("g1_rbf_e1")
+    v = volume_of(g)
+    a = chains_of(v, 2, burnin=4, nsave=4, thin=1, leapfrog=4, seed=17)
+    b = chains_of(v, 2, burnin=4, nsave=4, thin=1, leapfrog=4, seed=17)
+    a.update(2)
+    b.update(2)
+    other = (g["mu"] * 0.7).astype(np.complex64)
+    for c in (0, 1):
+        a.gradient(c, other)
+        a.log_prior_likelihood(c, other)
+    for c in (0, 1):
+        (ma, sa), (mb, sb) = a.get_state(c), b.get_state(c)
+        assert np.array_equal(ma, mb) and np.array_equal(sa, sb)
+    a.update(3)
+    b.update(3)
+    for c in (0, 1):
+        (ma, _), (mb, _) = a.get_state(c), b.get_state(c)
+        assert np.array_equal(ma, mb)
+    assert [s["iteration"] for s in a.stats()] == [s["iteration"] for s in b.stats()]
