@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=-1.0, help="served workloads: arrivals per second")
     ap.add_argument("--no-ess", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-served", action="store_true", help="skip the short served stream in the batched line")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--profile-kernel", type=int, default=-1,
                     help="set up, run --warmup iterations, then launch kernel K of the leapfrog step 4 times "
@@ -115,6 +116,8 @@ WORKLOADS = {
     "single_c1": dict(chains=1, vol="c1", burnin=200, nsave=200, thin=1, leapfrog=25),
     "single_c2": dict(chains=1, vol="c2", burnin=200, nsave=200, thin=1, leapfrog=25),
     "tiny": dict(chains=2, vol="small", burnin=10, nsave=10, thin=1, leapfrog=5),  # test-sized
+    # the largest class of the uneven batch (80x80x64 latent, 256x256x128 embedding: the x-line path), 4 chains
+    "xline256": dict(chains=4, vol="x256", burnin=300, nsave=300, thin=3, leapfrog=25),
     # served streams: a step is one job; jobs arrive as a Poisson process
     "served": dict(chains=1, vol="c4", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
     "served_c1": dict(chains=1, vol="c1", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
@@ -130,6 +133,8 @@ def make_volume(name):
         return synth.small_volume()
     if name == "c4":
         return synth.config_c4_volume(0)
+    if name == "x256":
+        return synth.make_volume((80, 80, 64), 1.0, (1.0, 0.35, 1.4), 0.6, 0.4, 6.9, "ellipsoid", 0.60, 5, name="x256")
     return synth.config_c1() if name == "c1" else synth.config_c2()
 
 
@@ -138,6 +143,7 @@ def config_of(w, extra=None):
     desc = {"c1": ("32x32x32 @ 1mm", "64^3", [0.806, 0.132, 1.0], 6.9),
             "c2": ("64x64x48 @ 1.5mm", "128^3", [1.0, 0.4, 1.5], 6.9),
             "small": ("10x9x7 @ 1mm", "32x16x16", [0.8, 0.3, 1.0], 3.2),
+            "x256": ("80x80x64 @ 1mm", "256x256x128", [1.0, 0.35, 1.4], 6.9),
             "c4": ("uniform over 32^3, 48x48x40, 64x64x48, 80x80x64 @ 1mm", "64^3 .. 256x256x128",
                    "RBF v=1, b~U[0.1,0.6], e~U[1,2]", 6.9)}[vol]
     cfg = {"workload": w, **{k: v for k, v in WORKLOADS[w].items()},
@@ -335,6 +341,16 @@ def run_ours(args, dist):
                                 "min": float(np.min(ess)) / (job_ms / 1e3)}
         extra["job_grad_evals_per_sec"] = sum(x["grad_evals"] for x in st) / (job_ms / 1e3)
         job.close()
+
+    # ---- a short served stream of fits of the same volume class (continuous batching through dr_server_*)
+    if not args.no_served and dist.world == 1 and C > 1:
+        try:
+            srv = served_sample("served_c1", 12, 2, args.seed + 11, dev)
+            srv["over_plain_gpu"] = srv["value"] / extra["plain_gpu_single_chain"]["value"] \
+                if "value" in extra.get("plain_gpu_single_chain", {}) else None
+            extra["served_c1"] = srv
+        except Exception as e:  # an extra must not break the benchmark line
+            extra["served_c1"] = {"error": str(e)[:200]}
 
     # ---- roofline of the dominant kernel (timed live with CUDA events on the library stream)
     per_iter = {}
@@ -589,6 +605,42 @@ def run_served(args, dist):
     return line
 
 
+def served_sample(workload, jobs, warmup_jobs, seed, device, rate=None):
+    """A short served stream for the default benchmark line: `jobs` fits of `workload` arriving as a Poisson process,
+    after `warmup_jobs` untimed ones; gradient evaluations per second over the makespan, fits per second, latency."""
+    import dualres_b200 as d
+    wl = WORKLOADS[workload]
+    rate = wl["rate"] if rate is None else rate
+    hmc = lambda i: d.HMCParameters(burnin=wl["burnin"], nsave=wl["nsave"], thin=wl["thin"],  # noqa: E731
+                                    leapfrog=wl["leapfrog"], seed=seed + i)
+    vols = [served_volume(wl, i, seed) for i in range(warmup_jobs + jobs)]
+    gaps = np.random.default_rng(seed).exponential(1.0 / rate, size=jobs)
+    sv = d.Server(device=device, iterations_per_round=8, host_threads=4)
+    for i in range(warmup_jobs):
+        sv.submit_volume(vols[i], hmc(i), wl["chains"])
+    sv.drain(3600)
+    t_start = time.perf_counter()
+    t_next, ids = t_start, []
+    for k in range(jobs):
+        t_next += gaps[k]
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(sv.submit_volume(vols[warmup_jobs + k], hmc(warmup_jobs + k), wl["chains"]))
+    sv.drain(3600)
+    makespan = time.perf_counter() - t_start
+    res = [sv.result(j) for j in ids]
+    sv.close()
+    lat = np.array([r.latency_s for r in res])
+    grads = sum(r.grad_evals for r in res)
+    return {"workload": workload, "jobs": jobs, "arrival_rate_per_s": rate, "value": grads / makespan, "unit": UNIT,
+            "fits_per_s": jobs / makespan, "makespan_s": makespan,
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "what": "a dualgpmf fit per job (one chain, burnin %d, nsave %d, thin %d, L %d) through dr_server_*; "
+                    "gradient evaluations over the makespan from the first arrival to the last result"
+                    % (wl["burnin"], wl["nsave"], wl["thin"], wl["leapfrog"])}
+
+
 def reference_bytes_per_step(N, nnz, chains, n_h, n_s):
     """Algorithmic bytes of one leapfrog step of one chain in the reference's formulation (four full complex64 3D
     FFTs per step, real-space state): 104 N + 16 nnz / C + 12 n_h + 8 n_s, with the kriging matrix (values and
@@ -640,16 +692,52 @@ def cpu_rate(m, iters, L, threads, seed=5):
     return g / dt, dt, g
 
 
+def cpu_throughput(vol, W, L, cores, target_s=10.0):
+    """Gradient evaluations per second of `cores` independent single-threaded chains of the FP32 restatement run
+    side by side (one host thread each; ctypes releases the GIL during the C calls), each for about target_s."""
+    import threading
+    from oracle import oracle as o
+    models = [oracle_model(vol, W)[0] for _ in range(cores)]
+    o.set_threads(1)
+    _, dt1, _ = cpu_rate(models[0], 1, L, 1)
+    iters = max(1, int(target_s / max(dt1, 1e-3)))
+    grads = [0] * cores
+
+    def work(i):
+        o.set_threads(1)  # the OpenMP thread count is per host thread
+        m = models[i]
+        rng = np.random.default_rng(100 + i)
+        m.set_mu((rng.standard_normal(m.shape) * 0.1).astype(np.complex64))
+        m.set_sigma(2.0, 5.0)
+        grads[i] = m.run_iterations(iters, L, 0.02, 1000 + i)
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(cores)]
+    t0 = time.perf_counter()
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    dt = time.perf_counter() - t0
+    return {"value": sum(grads) / dt, "unit": UNIT, "cores": cores, "chains": cores,
+            "sample": f"{cores} independent chains x {iters} HMC iterations (L={L}), one host thread each, "
+                      f"{dt:.1f} s wall"}
+
+
 def cpu_baseline_line(vol, W, L, target_s=12.0):
     threads = os.cpu_count() or 1
     m, _ = oracle_model(vol, W)
     r1, dt1, _ = cpu_rate(m, 1, L, threads)
     iters = max(1, int(target_s / max(dt1, 1e-3)))
     r, dt, g = cpu_rate(m, iters, L, threads)
-    return {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
+    line = {"value": r, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{iters} HMC iterations (L={L}, {g} gradient evals) of one chain on the same volume, "
                       f"FP32 restatement of MultiResParameters<float>::update (4 FFTs per leapfrog step), "
                       f"{dt:.1f} s"}
+    try:  # the same restatement as independent single-threaded chains, one per host thread
+        line["throughput"] = cpu_throughput(vol, W, L, threads)
+    except Exception as e:  # an extra must not break the benchmark line
+        line["throughput"] = {"error": str(e)[:200]}
+    return line
 
 
 def run_reference(args, dist):

@@ -95,7 +95,8 @@ class ChainStats(C.Structure):
     _fields_ = [("iteration", C.c_int), ("saved", C.c_int), ("integrator_steps", C.c_int), ("eps", C.c_float),
                 ("mh_rate", C.c_float), ("sigma_hr", C.c_float), ("sigma_sr", C.c_float),
                 ("last_log_ratio", C.c_double), ("accepted", C.c_int64), ("grad_evals", C.c_int64),
-                ("done", C.c_int)]
+                ("done", C.c_int), ("last_eps", C.c_float), ("initial_energy", C.c_double),
+                ("proposed_energy", C.c_double)]
 
 
 _lib = None
@@ -368,7 +369,7 @@ class MultiResParameters:
         a = np.ascontiguousarray(x, dtype=np.complex64).reshape(self.data.shape)
         return a
 
-    PATHS = ("plane", "plane+prefetch", "lines")
+    PATHS = ("plane", "plane+prefetch", "lines", "plane-stream")
 
     def config(self):
         """The chain set's update path, kriging-product blocks per SM, tuned iteration time (ms, 0 if untuned) and

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <iomanip>
 #include <iostream>
 #include <sstream>
 #include <stdexcept>
@@ -392,23 +393,46 @@ int run(const Options& o) {
                     (uint64_t)o.seed, o.samples ? 1 : 0};
   dr_chainset* cs = nullptr;
   check(dr_chainset_create(vol, o.chains, &ho, &cs));
-  // burn-in, then the timed post-burn-in part (mcmc_summary::sampling_time covers the saving phase)
-  const int total = o.burnin + o.thin * o.nsave;
-  const int chunk = o.monitor ? std::max(1, total / 50) : o.burnin;
-  int done_it = 0;
-  while (done_it < o.burnin) {
-    const int n = std::min(chunk, o.burnin - done_it);
-    check(dr_step(cs, n));
-    done_it += n;
-    if (o.monitor) {
-      dr_chain_stats st;
-      check(dr_chain_stats_get(cs, &st));
-      std::cout << "iteration " << st.iteration << "  eps " << st.eps << "  L " << st.integrator_steps
-                << "  log MH ratio " << st.last_log_ratio << std::endl;
+  // burn-in, then the timed post-burn-in part (mcmc_summary::sampling_time covers the saving phase).  With
+  // --monitor every iteration prints each chain's energy transition, step size and MH ratio, as
+  // MultiResParameters::update does (MultiResParameters.h:706-713), one iteration at a time.
+  std::vector<dr_chain_stats> mon(o.chains);
+  std::vector<int> last_it(o.chains, 0);
+  auto monitor_line = [&]() {
+    check(dr_chain_stats_get(cs, mon.data()));
+    const std::streamsize prec = std::cout.precision();
+    for (int c = 0; c < o.chains; c++) {
+      const dr_chain_stats& m = mon[c];
+      if (m.iteration == last_it[c]) continue;  // a chain that has saved nsave samples no longer moves
+      last_it[c] = m.iteration;
+      if (o.chains > 1) std::cout << "chain " << c << ": ";
+      std::cout << std::setprecision(4) << "Energy Transition (" << m.initial_energy << " -> " << m.proposed_energy
+                << ");  step size (" << m.last_eps << ");  MH = (" << std::exp(m.last_log_ratio) << ")"
+                << std::endl;
     }
+    std::cout.precision(prec);
+  };
+  if (o.monitor) {
+    for (int it = 0; it < o.burnin; it++) {
+      check(dr_step(cs, 1));
+      monitor_line();
+    }
+  } else if (o.burnin > 0) {
+    check(dr_step(cs, o.burnin));
   }
   const auto t0 = std::chrono::high_resolution_clock::now();
-  check(dr_run(cs));
+  if (o.monitor) {
+    for (;;) {
+      check(dr_chain_stats_get(cs, mon.data()));
+      bool all_done = true;
+      for (const auto& m : mon) all_done = all_done && m.done;
+      if (all_done) break;
+      check(dr_step(cs, 1));
+      monitor_line();
+    }
+  } else {
+    check(dr_run(cs));
+  }
   const double sampling_s = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
 
   std::vector<dr_chain_stats> st(o.chains);

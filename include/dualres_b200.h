@@ -129,6 +129,9 @@ typedef struct {
   int64_t accepted;        /* accepted transitions */
   int64_t grad_evals;      /* gradient evaluations so far (sum of L + 1) */
   int done;                /* nsave samples saved */
+  float last_eps;          /* step size of the last transition (the eps argument of update) */
+  double initial_energy;   /* initial and proposed energy of the last transition, as */
+  double proposed_energy;  /* --monitor prints them (MultiResParameters.h:700-713) */
 } dr_chain_stats;
 
 /* n_chains independent chains on one volume, advanced together.  Each chain

@@ -145,3 +145,31 @@ def test_cli_patient_sized_rotated_volume(tmp_path):
     assert np.allclose(Q, vol.qform_hr, atol=1e-5)
     sel = vol.highres != 0
     assert np.all(np.isfinite(mean[sel])) and np.count_nonzero(mean[sel]) > 0.99 * sel.sum()
+
+
+def test_cli_monitor_prints_every_transition(tmp_path):
+    """--monitor prints one line per iteration, as MultiResParameters::update does (MultiResParameters.h:706-713):
+    the initial and proposed energy, the step size and the MH ratio R = exp(proposed - initial); and the fit is the
+    same as without it."""
+    import re
+    vol = synth.small_volume(seed=43)
+    tmp = str(tmp_path)
+    base = _write_volume(tmp, vol) + ["--covariance", *[str(t) for t in vol.theta], "--neighborhood",
+                                      str(vol.radius), "--burnin", "12", "--nsave", "5", "--thin", "2",
+                                      "--leapfrog", "4", "--seed", "5"]
+    r = _cli(base + ["--monitor", "--output", "mon"], tmp)
+    assert r.returncode == 0, r.stderr + r.stdout
+    pat = re.compile(r"^Energy Transition \((\S+) -> (\S+)\);  step size \((\S+)\);  MH = \((\S+)\)$")
+    lines = [m for m in (pat.match(x) for x in r.stdout.splitlines()) if m]
+    assert len(lines) == 12 + 2 * 5, r.stdout
+    for m in lines:
+        e0, ep, eps, mh = (float(x) for x in m.groups())
+        assert eps > 0
+        # printed with 4 significant digits: compare R with exp(ep - e0) where the difference is resolved
+        if abs(ep - e0) < 5 and abs(e0) < 1e3:
+            assert abs(mh - np.exp(ep - e0)) <= 0.05 * max(1.0, mh) + 1e-3, (e0, ep, mh)
+    q = _cli(base + ["--output", "plain"], tmp)
+    assert q.returncode == 0, q.stderr + q.stdout
+    a = nifti.read(os.path.join(tmp, "mon_posterior_mean.nii.gz"))[0]
+    b = nifti.read(os.path.join(tmp, "plain_posterior_mean.nii.gz"))[0]
+    assert np.array_equal(a, b)

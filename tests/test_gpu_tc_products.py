@@ -52,7 +52,7 @@ def _field(shape, rng, scale):
     return ((rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * scale).astype(np.complex64)
 
 
-@pytest.mark.parametrize("n_chains", [16, 64, 100])
+@pytest.mark.parametrize("n_chains", [16, 64, 100, 200])
 def test_gradient_and_leapfrog_match_oracle(oracle, products, n_chains):
     from dualres_b200 import synth
     vol = synth.small_volume(seed=61, dims=(14, 13, 12), radius=4.2)
@@ -124,19 +124,22 @@ def test_tma_row_gathers_equal_thread_gathers(products, monkeypatch):
     data.close()
 
 
-def test_full_run_matches_csr_run(products):
+@pytest.mark.parametrize("n_chains", [32, 200])
+def test_full_run_matches_csr_run(products, n_chains):
+    """A full run of the sampler with the tensor-core products against one with the CSR products; 200 chains run
+    the 256-chain product (two stages in shared memory, two gather groups)."""
     import dualres_b200 as d
     from dualres_b200 import synth
     vol = synth.small_volume(seed=62, dims=(16, 14, 12), radius=4.2)
     data = d.MultiResData.from_volume(vol)
     means = {}
     for tc in (True, False):
-        ch = products(data, 32, tc, burnin=80, nsave=80, leapfrog=8, seed=11 if tc else 12)
+        ch = products(data, n_chains, tc, burnin=80, nsave=80, leapfrog=8, seed=11 if tc else 12)
         ch.run()
         st = ch.stats()
         assert all(s["done"] == 1 for s in st)
-        x = np.array([ch.summary(c)["mean"] for c in range(32)], np.float64)
-        means[tc] = (x.mean(axis=0), x.std(axis=0, ddof=1) / np.sqrt(32))
+        x = np.array([ch.summary(c)["mean"] for c in range(n_chains)], np.float64)
+        means[tc] = (x.mean(axis=0), x.std(axis=0, ddof=1) / np.sqrt(n_chains))
         ch.close()
     (ma, sa), (mb, sb) = means[True], means[False]
     z = np.abs(ma - mb) / np.sqrt(sa ** 2 + sb ** 2 + 1e-12)
