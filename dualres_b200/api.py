@@ -369,7 +369,7 @@ class MultiResParameters:
         a = np.ascontiguousarray(x, dtype=np.complex64).reshape(self.data.shape)
         return a
 
-    PATHS = ("plane", "plane+prefetch", "lines", "plane-stream")
+    PATHS = ("plane", "plane+prefetch", "lines")
 
     def config(self):
         """The chain set's update path, kriging-product blocks per SM, tuned iteration time (ms, 0 if untuned) and

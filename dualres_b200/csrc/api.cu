@@ -86,20 +86,11 @@ static void set_pass_attrs() {
   }
 }
 
-template <int E, int PF>
+template <int E, bool PF>
 static void set_plane_attr(int dyn_max) {
-  const PlaneLayout Ly = plane_layout(E, PlaneGeom<E>::SIZE, plane_prefetches<PF>());
+  const PlaneLayout Ly = plane_layout(E, PlaneGeom<E>::SIZE, PF);
   if (Ly.total <= dyn_max)
     CK(cudaFuncSetAttribute(k_xyplane<E, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, Ly.total));
-}
-
-template <int E>
-static void set_stream_attr(int dyn_max) {
-  const StreamLayout Ly = stream_layout(E, PlaneGeom<E>::SIZE);
-  if (Ly.total <= dyn_max) {
-    CK(cudaFuncSetAttribute(k_xyplane_stream<E, 512, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, Ly.total));
-    CK(cudaFuncSetAttribute(k_xyplane_stream<E, 256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, Ly.total));
-  }
 }
 
 template <class C>
@@ -138,15 +129,12 @@ static DeviceTables& device_tables(int dev) {
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     t.sms = sms;
     t.tma_dyn_max = optin - 256;  // the plane kernels' static shared memory is at most 128 bytes
-    set_plane_attr<4, 0>(t.tma_dyn_max); set_plane_attr<8, 0>(t.tma_dyn_max);
-    set_plane_attr<16, 0>(t.tma_dyn_max); set_plane_attr<32, 0>(t.tma_dyn_max);
-    set_plane_attr<64, 0>(t.tma_dyn_max); set_plane_attr<128, 0>(t.tma_dyn_max);
-    set_plane_attr<4, 1>(t.tma_dyn_max); set_plane_attr<8, 1>(t.tma_dyn_max);
-    set_plane_attr<16, 1>(t.tma_dyn_max); set_plane_attr<32, 1>(t.tma_dyn_max);
-    set_plane_attr<64, 1>(t.tma_dyn_max);
-    set_plane_attr<16, 2>(t.tma_dyn_max); set_plane_attr<32, 2>(t.tma_dyn_max);
-    set_plane_attr<64, 2>(t.tma_dyn_max); set_plane_attr<64, 3>(t.tma_dyn_max);
-    set_stream_attr<16>(t.tma_dyn_max); set_stream_attr<32>(t.tma_dyn_max); set_stream_attr<64>(t.tma_dyn_max);
+    set_plane_attr<4, false>(t.tma_dyn_max); set_plane_attr<8, false>(t.tma_dyn_max);
+    set_plane_attr<16, false>(t.tma_dyn_max); set_plane_attr<32, false>(t.tma_dyn_max);
+    set_plane_attr<64, false>(t.tma_dyn_max); set_plane_attr<128, false>(t.tma_dyn_max);
+    set_plane_attr<4, true>(t.tma_dyn_max); set_plane_attr<8, true>(t.tma_dyn_max);
+    set_plane_attr<16, true>(t.tma_dyn_max); set_plane_attr<32, true>(t.tma_dyn_max);
+    set_plane_attr<64, true>(t.tma_dyn_max);
     CK(cudaFuncSetAttribute(k_kriging_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
     CK(cudaFuncSetAttribute(k_spd_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
     CK(cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
@@ -590,8 +578,7 @@ struct Chainset {
   float2* tmp = nullptr;        // [N] scratch for evaluation calls
   int NR = 1;
   bool plane = false;           // fused xy-plane update (E0 == E1 <= 128)
-  int path = 0;                 // 0 plane kernel, 1 plane kernel with bulk prefetch, 2 x-line kernel + y passes,
-                                // 3 persistent plane kernel streaming the next plane's state into shared memory
+  int path = 0;                 // 0 plane kernel, 1 plane kernel with bulk prefetch, 2 x-line kernel + y passes
   int grid = 8;                 // kriging-product blocks per SM
   double tuned_ms = 0.0;        // iteration time of the chosen configuration when it was tuned (0: not tuned)
   bool tcp = false;             // kriging products on the tensor cores (dense tiles of the volume)
@@ -600,10 +587,6 @@ struct Chainset {
   bool tc_tg = false;           // W^T rs: the chain vectors arrive by TMA row gathers over tc_map_wt
   CUtensorMap tc_map_w{}, tc_map_wt{};  // (tc_map_w unused: W mu_D gathers with its threads); rs as [n_s] rows
   bool tma = false;             // path 1
-  bool pstream = false;         // path 3
-  int pstream_nt = 512;         // path 3: threads per CTA (512 at 64 registers, or 256 at 128)
-  int prefetch_nt = 512;        // path 1: threads per block (512 at 64 registers, or 256 at 128)
-  bool plane_minb3 = false;     // path 0 at E = 64: three blocks per SM (85 registers) instead of four (64)
   int tma_smem = 0, tma_grid = 0;
 
   int64_t bytes = 0;
@@ -756,60 +739,35 @@ static void launch_xline(Chainset* S, int step, int flags) {
   CK_LAUNCH();
 }
 
-template <int E, int PF>
+template <int E, bool PF>
 static void launch_plane_t(Chainset* S, int step, int flags) {
   const DevVolume& v = S->vol->dv;
   const dim3 grid(v.E2, S->C);
-  const size_t smem = (size_t)plane_layout(E, PlaneGeom<E>::SIZE, plane_prefetches<PF>()).total;
+  const size_t smem = (size_t)plane_layout(E, PlaneGeom<E>::SIZE, PF).total;
   k_xyplane<E, PF><<<grid, PlaneCfg<E, PF>::NT, smem, S->stream>>>(v, S->dc, step, flags, S->vol->tw_f);
-  CK_LAUNCH();
-}
-
-template <int E>
-static void launch_plane_stream_t(Chainset* S, int step, int flags) {
-  const DevVolume& v = S->vol->dv;
-  const int items = v.E2 * S->C;
-  const int grid = std::max(1, std::min(items, 2 * device_tables(S->device).sms));
-  const size_t smem = (size_t)stream_layout(E, PlaneGeom<E>::SIZE).total;
-  if (S->pstream_nt == 256)
-    k_xyplane_stream<E, 256, 2><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, S->vol->tw_f);
-  else
-    k_xyplane_stream<E, 512, 2><<<grid, 512, smem, S->stream>>>(v, S->dc, step, flags, S->vol->tw_f);
   CK_LAUNCH();
 }
 
 static void launch_plane(Chainset* S, int step, int flags) {
   const DevVolume& v = S->vol->dv;
   if (v.E2 > S->dc.maxblk) throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the plane count");
-  if (S->pstream) {
-    switch (v.E0) {
-      case 16: launch_plane_stream_t<16>(S, step, flags); return;
-      case 32: launch_plane_stream_t<32>(S, step, flags); return;
-      case 64: launch_plane_stream_t<64>(S, step, flags); return;
-      default: throw Error(DR_ERR_UNSUPPORTED, "plane size not supported by the streaming kernel");
-    }
-  }
   if (S->tma) {
-    const bool narrow = S->prefetch_nt == 256 && v.E0 >= 16;
     switch (v.E0) {
-      case 4: launch_plane_t<4, 1>(S, step, flags); return;
-      case 8: launch_plane_t<8, 1>(S, step, flags); return;
-      case 16: if (narrow) launch_plane_t<16, 2>(S, step, flags); else launch_plane_t<16, 1>(S, step, flags); return;
-      case 32: if (narrow) launch_plane_t<32, 2>(S, step, flags); else launch_plane_t<32, 1>(S, step, flags); return;
-      case 64: if (narrow) launch_plane_t<64, 2>(S, step, flags); else launch_plane_t<64, 1>(S, step, flags); return;
+      case 4: launch_plane_t<4, true>(S, step, flags); return;
+      case 8: launch_plane_t<8, true>(S, step, flags); return;
+      case 16: launch_plane_t<16, true>(S, step, flags); return;
+      case 32: launch_plane_t<32, true>(S, step, flags); return;
+      case 64: launch_plane_t<64, true>(S, step, flags); return;
       default: throw Error(DR_ERR_UNSUPPORTED, "plane size not supported by the bulk-copy kernel");
     }
   }
   switch (v.E0) {
-    case 4: launch_plane_t<4, 0>(S, step, flags); break;
-    case 8: launch_plane_t<8, 0>(S, step, flags); break;
-    case 16: launch_plane_t<16, 0>(S, step, flags); break;
-    case 32: launch_plane_t<32, 0>(S, step, flags); break;
-    case 64:
-      if (S->plane_minb3) launch_plane_t<64, 3>(S, step, flags);
-      else launch_plane_t<64, 0>(S, step, flags);
-      break;
-    case 128: launch_plane_t<128, 0>(S, step, flags); break;
+    case 4: launch_plane_t<4, false>(S, step, flags); break;
+    case 8: launch_plane_t<8, false>(S, step, flags); break;
+    case 16: launch_plane_t<16, false>(S, step, flags); break;
+    case 32: launch_plane_t<32, false>(S, step, flags); break;
+    case 64: launch_plane_t<64, false>(S, step, flags); break;
+    case 128: launch_plane_t<128, false>(S, step, flags); break;
     default: throw Error(DR_ERR_UNSUPPORTED, "plane size not supported");
   }
 }
@@ -913,33 +871,19 @@ static void tc_upload(Volume* V, const TcPlanHost& P, const float* dval, int nnz
   M->segs = reinterpret_cast<const int4*>(V->upload(P.segs));
   M->cta_seg_ptr = V->upload(P.cta_seg_ptr);
   M->tile_seg_ptr = V->upload(P.tile_seg_ptr);
-  // each chunk's nonzeros: a counting sort of the CSR entries by chunk (in CSR order within a chunk), with the
-  // position in the chunk's block as 16 bits; the values are packed on the device
-  std::vector<int> nz_ptr((size_t)P.chunks + 1, 0), slot(nnz);
-  std::vector<uint16_t> nz_pos(std::max(nnz, 1));
-  for (int k = 0; k < nnz; k++) nz_ptr[(size_t)(P.dest[k] / TC_BLK) + 1]++;
-  for (long long q = 0; q < P.chunks; q++) nz_ptr[q + 1] += nz_ptr[q];
-  {
-    std::vector<int> fill(nz_ptr.begin(), nz_ptr.end() - 1);
-    for (int k = 0; k < nnz; k++) {
-      const int q = P.dest[k] / TC_BLK;
-      slot[k] = fill[q]++;
-      nz_pos[slot[k]] = (uint16_t)(P.dest[k] % TC_BLK);
-    }
-  }
-  M->nz_ptr = V->upload(nz_ptr);
-  M->nz_pos = V->upload(nz_pos);
-  float* nz_val = V->alloc<float>(std::max(nnz, 1));
+  const size_t nblob = (size_t)P.chunks * TC_BLK;
+  float* blob = V->alloc<float>(nblob);
+  CK(cudaMemsetAsync(blob, 0, sizeof(float) * std::max<size_t>(nblob, 1), st));
   if (nnz > 0) {
-    int* dslot = nullptr;
-    const cudaError_t e = cudaMallocAsync(&dslot, sizeof(int) * nnz, st);
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, "cudaMallocAsync (tile slots)");
-    CK(cudaMemcpyAsync(dslot, slot.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
-    k_tc_pack<<<cdiv_i(nnz, 256), 256, 0, st>>>(dval, dslot, nnz, nz_val);
+    int* dest = nullptr;
+    const cudaError_t e = cudaMallocAsync(&dest, sizeof(int) * nnz, st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, "cudaMallocAsync (tile positions)");
+    CK(cudaMemcpyAsync(dest, P.dest.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+    k_tc_fill<<<cdiv_i(nnz, 256), 256, 0, st>>>(dval, dest, nnz, blob);
     CK_LAUNCH();
-    CK(cudaFreeAsync(dslot, st));
+    CK(cudaFreeAsync(dest, st));
   }
-  M->nz_val = nz_val;
+  M->blob = blob;
 }
 
 // Builds the volume's dense tiles once; false when the tensor-core products are not available for it (no std-res
@@ -983,8 +927,8 @@ static bool volume_tc(Volume* V) {
     return false;
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
-  const double tile_bytes = (double)(hv.w_col.size() + hv.wt_col.size()) * 10 + (double)(pw.chunks + pt.chunks) * 132;
-  if (tile_bytes > 0.25 * (double)fr) return false;
+  const double blob_bytes = (double)(pw.chunks + pt.chunks) * TC_BLK * 4;
+  if (blob_bytes > 0.25 * (double)fr) return false;
   tc_upload(V, pw, dv.w_val, (int)hv.w_col.size(), &V->tc_w);
   tc_upload(V, pt, dv.wt_val, (int)hv.wt_col.size(), &V->tc_wt);
   V->tc_max_segs = std::max(V->tc_w.n_segs, V->tc_wt.n_segs);
@@ -1037,7 +981,7 @@ static bool tc_env_off() {
 }
 
 struct PathOptions {
-  bool plane = false, prefetch = false, stream = false;
+  bool plane = false, prefetch = false;
 };
 static PathOptions path_options(const DevVolume& v, int device) {
   PathOptions po;
@@ -1046,12 +990,11 @@ static PathOptions path_options(const DevVolume& v, int device) {
   const int elems = v.E0 == 64 ? PlaneGeom<64>::SIZE : (v.E0 == 128 ? PlaneGeom<128>::SIZE : v.E0 * (v.E0 + 1));
   po.plane = plane_layout(v.E0, elems, false).total <= dt.tma_dyn_max;
   po.prefetch = po.plane && v.E0 <= 64 && plane_layout(v.E0, elems, true).total <= dt.tma_dyn_max;
-  po.stream = po.plane && v.E0 >= 16 && v.E0 <= 64 && stream_layout(v.E0, elems).total <= dt.tma_dyn_max;
   return po;
 }
 
 struct TuneChoice {
-  int path = 0;      // 0 plane, 1 plane + prefetch, 2 x-line, 3 persistent streaming plane
+  int path = 0;      // 0 plane, 1 plane + prefetch, 2 x-line
   int grid = 8;      // kriging-product blocks per SM (CSR products)
   double ms = 0.0;   // measured milliseconds per iteration
   int tc = 0;        // 1: kriging products on the tensor cores
@@ -1150,8 +1093,8 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
       cudaGetLastError();
     }
   };
-  for (int path : {0, 1, 2, 3}) {
-    if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch) || (path == 3 && !po.stream)) continue;
+  for (int path : {0, 1, 2}) {
+    if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
     try_candidate(TuneChoice{path, 8, 0.0, tc ? 1 : 0});
   }
   if (best.ms < 1e300) {
@@ -1217,8 +1160,6 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     path = 2;
   } else if (std::getenv("DRB_PLANE_PREFETCH")) {
     path = po.prefetch ? 1 : path;
-  } else if (std::getenv("DRB_PLANE_STREAM")) {
-    path = po.stream ? 3 : path;
   } else if (autotune_enabled()) {
     const TuneChoice t = autotune(V, C, o);
     path = t.path;
@@ -1229,15 +1170,11 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   if (!forced) {
     if (const char* g = std::getenv("DRB_PRODUCT_BLOCKS_PER_SM")) grid = std::max(1, std::min(16, std::atoi(g)));
   }
-  if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch) || (path == 3 && !po.stream)) path = po.plane ? 0 : 2;
+  if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) path = po.plane ? 0 : 2;
   S->path = path;
   S->grid = grid;
   S->plane = path != 2;
   S->tma = path == 1;
-  S->pstream = path == 3;
-  if (const char* e = std::getenv("DRB_PLANE_STREAM_THREADS")) S->pstream_nt = std::atoi(e) == 256 ? 256 : 512;
-  if (const char* e = std::getenv("DRB_PLANE_PREFETCH_THREADS")) S->prefetch_nt = std::atoi(e) == 256 ? 256 : 512;
-  if (const char* e = std::getenv("DRB_PLANE_BLOCKS_PER_SM")) S->plane_minb3 = std::atoi(e) == 3;
   ch.t2_stride = (long long)v.E2 * v.by * v.bx;
   if (S->plane) {
     // T1 is only needed by the initial transforms: borrow the momentum buffer
@@ -1969,12 +1906,10 @@ int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* a
       default: b = s->plane ? 0.0 : C * (t2 + t1) * 8; break;
     }
     if (s->tcp && (which == 3 || which == 4)) {
-      // tensor-core products: the packed nonzeros (value + position) and chunk tables, the chain vectors of every
-      // chunk column, the segment partials written and read back, and the epilogue's operands (rs; or mu_D in and
-      // gD out)
+      // tensor-core products: the dense FP32 blob, the chain vectors of every chunk column, the segment partials
+      // written and read back, and the epilogue's operands (rs; or mu_D in and gD out)
       const DevTcMatrix& M = which == 3 ? s->vol->tc_w : s->vol->tc_wt;
-      b = (double)(which == 3 ? s->vol->hv.w_col.size() : s->vol->hv.wt_col.size()) * 6 + (double)M.chunks * 4 +
-          (double)M.chunks * TC_KC * 4 + (double)M.chunks * TC_KC * C * 4 +
+      b = (double)M.chunks * TC_BLK * 4 + (double)M.chunks * TC_KC * C * 4 +
           2.0 * M.n_segs * s->tc_N * TC_M * 4 + (which == 3 ? (double)v.n_s * C * 4 : 2.0 * v.n_h * C * 4);
     }
     *algo_bytes = b;
@@ -2092,10 +2027,9 @@ static int64_t estimate_bytes(const HostVolume& hv, int C, const dr_hmc_opts& o)
               C * (2 * (nh + no) * 4 + (nh + ns) * 4 + no * 24) + N * 8 + (double)C * 9 * 2048 * 8;
   if (o.store_samples) cs += (double)std::max(o.nsave, 1) * (no * 4 + 24) * C;
   if (tc_chains(C) > 0 && ns > 0) {
-    // the tiles of W and W^T for the tensor-core products: every nonzero packed (value, position, and a slot
-    // index while packing), chunk tables (the column unions are a few times the nonzeros: 5.8x and 3.1x on a 32^3
-    // volume; 10x each is budgeted), and the segment partials
-    vol += 2 * nnz * 10 + 2 * (nnz * 10 / 32.0) * 132 + (nh + ns) * 8;
+    // dense tiles of W and W^T for the tensor-core products (their column unions are a few times the nonzeros:
+    // 5.8x and 3.1x on a 32^3 volume; 10x each is budgeted), index tables, and the segment partials
+    vol += 2 * nnz * 10 * 4 + (nh + ns) * 8;
     cs += (double)((ns + nh) / TC_M + 2 + 2 * 148) * tc_chains(C) * TC_M * 4;
   }
   return (int64_t)(1.10 * (vol + cs)) + (16 << 20);

@@ -99,10 +99,9 @@ struct DevChains {
 
 // A kriging matrix (W or W^T) cut into dense tiles for the tensor-core
 // products: rows in tiles of 128 (spatially ordered), the union of a tile's
-// columns in chunks of 32.  Chunk q is one 128 x 32 FP32 block in the K-major
-// core-matrix layout, element (m, k) at float (k / 4) * 512 + m * 4 + k % 4 of
-// the block, stored as its nonzeros (value + 16-bit position in the block) and
-// expanded into shared memory by the product kernel.  The chunks are
+// columns in chunks of 32.  Chunk q holds one 128 x 32 FP32 block in the
+// K-major core-matrix layout: element (m, k) at float (k / 4) * 512 + m * 4 +
+// k % 4 of the block.  The chunks are
 // split into contiguous ranges, one per CTA; a range cut at tile boundaries
 // gives segments, each summing into its own partial slot.
 struct DevTcMatrix {
@@ -112,9 +111,7 @@ struct DevTcMatrix {
   int chunks;
   const int* tile_rows;     // [T * 128] matrix row of each tile row, or -1
   const int* chunk_cols;    // [chunks * 32] matrix column of each chunk column, or -1
-  const int* nz_ptr;        // [chunks + 1] first nonzero of each chunk in nz_val / nz_pos
-  const float* nz_val;      // the nonzeros, chunk by chunk
-  const uint16_t* nz_pos;   // each nonzero's float index in its chunk's 128 x 32 block (layout below)
+  const float* blob;        // [chunks][128 * 32]
   const int4* segs;         // [n_segs] {tile, first chunk, end chunk, 0}, ordered by chunk
   const int* cta_seg_ptr;   // [G + 1] segments of each CTA
   const int* tile_seg_ptr;  // [T + 1] segments of each tile

@@ -182,10 +182,9 @@ __host__ __device__ constexpr int plan_nbmax() {
 // 32 / nbmax lines; every stage runs with warp-level synchronisation only.
 // The block synchronises once at the end, so the tile is complete on return.
 template <int N, int DIR, class C>
-__device__ __forceinline__ void fft_smem_warp(C* sm, int ls, int es, int nlines, const C* __restrict__ tw,
-                                              int tid = (int)threadIdx.x) {
+__device__ __forceinline__ void fft_smem_warp(C* sm, int ls, int es, int nlines, const C* __restrict__ tw) {
   constexpr int NBM = plan_nbmax<N>(), LPW = 32 / NBM;
-  const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int li = lane / NBM, b = lane % NBM;
   for (int base = warp * LPW; base < nlines; base += nw * LPW) {
     const int line = base + li;
@@ -314,11 +313,10 @@ __device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)
 // Row FFTs (lines = y rows, elements along x) of a padded plane, all E rows; x >= rlim read as zero, x >= wlim not
 // written.
 template <int E, int R1, int R2, int DIR>
-__device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict__ tw, int rlim = E, int wlim = E,
-                                           int tid = (int)threadIdx.x) {
+__device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict__ tw, int rlim = E, int wlim = E) {
   using PL = PaddedPlane<E>;
   constexpr int NBM = Plan2<E, R1, R2>::NBM, LPW = 32 / NBM;
-  const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int li = lane / NBM;
   const int bl[1] = {lane % NBM};
   for (int base = warp * LPW; base < E; base += nw * LPW) {
@@ -336,10 +334,10 @@ __device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict_
 // not written.
 template <int E, int R1, int R2, int DIR>
 __device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* __restrict__ tw, int rlim = E,
-                                           int wlim = E, int tid = (int)threadIdx.x) {
+                                           int wlim = E) {
   using PL = PaddedPlane<E>;
   constexpr int NBM = Plan2<E, R1, R2>::NBM, PL_LANE = NBM / 4;
-  const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int li = lane & 7, bb = lane >> 3;
   int bl[PL_LANE];
 #pragma unroll

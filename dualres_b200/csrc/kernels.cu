@@ -334,10 +334,11 @@ __global__ void __launch_bounds__(XCfg<E0>::NT) k_xline(DevVolume v, DevChains c
 //   spectral plane; kick / drift as in k_xline; forward x, forward y --> T2.
 // For E = 64 and 128 the plane uses the padded layout of PaddedPlane (bank-
 // conflict free radix stages); other sizes use an odd row pitch.  With
-// PREFETCH the plane's U, q and 1/lambda planes are brought into shared
-// memory at entry by bulk asynchronous copies (1D TMA, completion on an
-// mbarrier) so that their DRAM latency overlaps the inverse transforms; the
-// wait is bounded and a time-out is recorded in ch.err.
+// PREFETCH the plane's U and q planes are brought into shared memory at
+// entry by bulk asynchronous copies (1D TMA, completion on an mbarrier) so
+// that their DRAM latency overlaps the inverse transforms; 1/lambda, one array
+// shared by every chain, stays in L2.  The wait is bounded and a time-out is
+// recorded in ch.err.
 template <int E>
 struct PlaneGeom {
   static constexpr bool PADDED = (E == 64 || E == 128);
@@ -350,13 +351,12 @@ struct PlaneGeom {
   }
 };
 
-// PREFETCH: 0 none; 1 bulk prefetch of U and q with 512 threads (64 registers), 2 the same with 256 threads (128
-// registers), both fitting two blocks per SM for E <= 64; 3 no prefetch, three blocks per SM (85 registers).
-template <int E, int PREFETCH> struct PlaneCfg {
-  static constexpr int NT = (E >= 128 || PREFETCH == 1) ? 512 : 256;
-  static constexpr int MINB = PREFETCH == 3 ? 3 : (PREFETCH ? 2 : (E <= 64 ? 4 : 1));  // blocks per SM targeted
+// PREFETCH: the U and q planes are bulk-copied into shared memory at entry; 256 threads and 128 registers, two
+// blocks per SM (E <= 64).  Without it four blocks of 256 threads at 64 registers (E <= 64).
+template <int E, bool PREFETCH> struct PlaneCfg {
+  static constexpr int NT = E >= 128 ? 512 : 256;
+  static constexpr int MINB = PREFETCH ? 2 : (E <= 64 ? 4 : 1);  // blocks per SM the register budget targets
 };
-template <int PREFETCH> constexpr bool plane_prefetches() { return PREFETCH == 1 || PREFETCH == 2; }
 
 // Shared-memory layout in bytes: [mbarrier | plane | U | q].
 struct PlaneLayout {
@@ -374,35 +374,26 @@ __host__ __device__ inline PlaneLayout plane_layout(int E, int plane_elems, bool
 
 // The padded planes prune both transforms to the box (ncols x nrows of T2): the inverse transforms read only the
 // box (everything else is zero and is never stored), and the forward transforms write only what lands in it.
-template <int E, int PREFETCH>
-__device__ __forceinline__ void plane_fft(float2* sm, int ncols, int nrows, int dir, const float2* tw,
-                                          int tid = (int)threadIdx.x) {
+template <int E>
+__device__ __forceinline__ void plane_fft(float2* sm, int ncols, int nrows, int dir, const float2* tw) {
   using G = PlaneGeom<E>;
   if constexpr (G::PADDED) {
     if (dir > 0) {
-      plane_cols<E, G::R1, G::R2, +1>(sm, ncols, tw, nrows, E, tid);
-      plane_rows<E, G::R1, G::R2, +1>(sm, tw, ncols, E, tid);
+      plane_cols<E, G::R1, G::R2, +1>(sm, ncols, tw, nrows, E);
+      plane_rows<E, G::R1, G::R2, +1>(sm, tw, ncols, E);
     } else {
-      plane_rows<E, G::R1, G::R2, -1>(sm, tw, E, ncols, tid);
-      plane_cols<E, G::R1, G::R2, -1>(sm, ncols, tw, E, nrows, tid);
+      plane_rows<E, G::R1, G::R2, -1>(sm, tw, E, ncols);
+      plane_cols<E, G::R1, G::R2, -1>(sm, ncols, tw, E, nrows);
     }
   } else {
     if (dir > 0) {
-      fft_smem_warp<E, +1>(sm, 1, G::P, ncols, tw, tid);
-      fft_smem_warp<E, +1>(sm, G::P, 1, E, tw, tid);
+      fft_smem_warp<E, +1>(sm, 1, G::P, ncols, tw);
+      fft_smem_warp<E, +1>(sm, G::P, 1, E, tw);
     } else {
-      fft_smem_warp<E, -1>(sm, G::P, 1, E, tw, tid);
-      fft_smem_warp<E, -1>(sm, 1, G::P, ncols, tw, tid);
+      fft_smem_warp<E, -1>(sm, G::P, 1, E, tw);
+      fft_smem_warp<E, -1>(sm, 1, G::P, ncols, tw);
     }
   }
-}
-
-// threadIdx.x through an opaque move: index arithmetic derived from it is computed where it is used, so a
-// persistent loop over items keeps no hoisted per-thread tables live across the whole loop.
-__device__ __forceinline__ int opaque_tid() {
-  int t;
-  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
-  return t;
 }
 
 // One plane of one chain after its inverse transforms, in two parts.  plane_update: the kick (and at step 0 the
@@ -414,9 +405,9 @@ template <int E, int NT>
 __device__ __forceinline__ void plane_update(float2* sm, const DevVolume& v, const DevChains& ch,
                                              const ChainState& st, int c, int z, bool first, bool last, bool need_q,
                                              int flags, const float2* srcU, const float2* srcQ, const float* srcS,
-                                             float2* Udst, float2* Qc, double& pa_out, double& pb_out,
-                                             int tid = (int)threadIdx.x) {
+                                             float2* Udst, float2* Qc, double& pa_out, double& pb_out) {
   using G = PlaneGeom<E>;
+  const int tid = threadIdx.x;
   const float eps = st.eps_cur, sh = st.sh;
   const bool write_q = !last || (flags & XF_WRITE_Q_LAST);
   const float keps = ((first || last) ? 0.5f : 1.0f) * eps;
@@ -515,8 +506,9 @@ __device__ __forceinline__ void plane_update(float2* sm, const DevVolume& v, con
 template <int E, int NT>
 __device__ __forceinline__ void plane_finish(float2* sm, const DevChains& ch, int c, int z, bool first, bool last,
                                              double pa, double pb, float2* T, int bx, int by, const float2* twE,
-                                             double* red, int tid = (int)threadIdx.x) {
+                                             double* red) {
   using G = PlaneGeom<E>;
+  const int tid = threadIdx.x;
   if (first || last) {
     const double ta = block_sum(pa, red);
     if (tid == 0) ch.part[((long long)c * NSLOT + (first ? SL_E0 : SL_LPL)) * ch.maxblk + z] = ta;
@@ -525,7 +517,7 @@ __device__ __forceinline__ void plane_finish(float2* sm, const DevChains& ch, in
   }
   if (last) return;
   __syncthreads();
-  plane_fft<E, 0>(sm, bx, by, -1, twE, tid);
+  plane_fft<E>(sm, bx, by, -1, twE);
   for (int e = tid; e < by * bx; e += NT) {
     const int y = e / bx, x = e % bx;
     T[y * bx + x] = sm[G::at(y, x)];
@@ -535,9 +527,9 @@ __device__ __forceinline__ void plane_finish(float2* sm, const DevChains& ch, in
 // Loads the T2 box of one plane into the plane buffer (for the padded layout only the box: the pruned inverse
 // transforms read nothing outside it).
 template <int E, int NT>
-__device__ __forceinline__ void plane_load_box(float2* sm, const float2* __restrict__ T, int bx, int by,
-                                               int tid = (int)threadIdx.x) {
+__device__ __forceinline__ void plane_load_box(float2* sm, const float2* __restrict__ T, int bx, int by) {
   using G = PlaneGeom<E>;
+  const int tid = threadIdx.x;
   if constexpr (G::PADDED) {
     for (int e = tid; e < by * bx; e += NT) {
       const int y = e / bx, x = e % bx;
@@ -551,13 +543,13 @@ __device__ __forceinline__ void plane_load_box(float2* sm, const float2* __restr
   }
 }
 
-template <int E, int PREFETCH>
+template <int E, bool PREFETCH>
 __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETCH>::MINB) k_xyplane(DevVolume v, DevChains ch, int step, int flags,
                                                                        const float2* __restrict__ tw) {
   constexpr int NT = PlaneCfg<E, PREFETCH>::NT;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ double red[NT / 32];
-  const PlaneLayout Ly = plane_layout(E, PlaneGeom<E>::SIZE, plane_prefetches<PREFETCH>());
+  const PlaneLayout Ly = plane_layout(E, PlaneGeom<E>::SIZE, PREFETCH);
   float2* sm = reinterpret_cast<float2*>(smraw + Ly.plane_off);
   const int c = blockIdx.y, z = blockIdx.x;
   const ChainState& st = ch.st[c];
@@ -580,7 +572,7 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   const float2* srcU = Usrc;
   const float2* srcQ = Qc;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
-  if constexpr (plane_prefetches<PREFETCH>()) {
+  if constexpr (PREFETCH) {
     // U and q only: 1/lambda is one array shared by every chain and stays in L2
     srcU = reinterpret_cast<const float2*>(smraw + Ly.u_off);
     srcQ = reinterpret_cast<const float2*>(smraw + Ly.q_off);
@@ -595,8 +587,8 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   }
   plane_load_box<E, NT>(sm, T, bx, by);
   __syncthreads();
-  plane_fft<E, PREFETCH>(sm, bx, by, +1, twE);
-  if constexpr (plane_prefetches<PREFETCH>()) {
+  plane_fft<E>(sm, bx, by, +1, twE);
+  if constexpr (PREFETCH) {
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
@@ -609,111 +601,6 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   double pa, pb;
   plane_update<E, NT>(sm, v, ch, st, c, z, first, last, need_q, flags, srcU, srcQ, Sg, Udst, Qc, pa, pb);
   plane_finish<E, NT>(sm, ch, c, z, first, last, pa, pb, T, bx, by, twE, red);
-}
-
-// ----------------------------------------------------------------- persistent streaming plane kernel
-// The plane update as a persistent kernel: each CTA walks the (z-plane, chain) items blockIdx.x, blockIdx.x +
-// gridDim.x, ... of the chains active at this step, and while it works on one item a bulk asynchronous copy (1D
-// TMA, completion on an mbarrier) brings the next item's U and q planes into a second shared-memory buffer, so the
-// next item's HBM reads overlap this item's forward transforms, the next T2 load and the next inverse transforms.
-// The update then reads U and q from shared memory; 1/lambda (one array shared by all chains, L2-resident) is read
-// from global memory.  Two CTAs per SM (the shared memory of two U / q buffers and the plane): 512 threads at 64
-// registers, or 256 threads at 128.  Every wait is bounded in time; on a time-out the CTA records it in ch.err,
-// waits (bounded) for its own copy in flight and returns.
-
-struct StreamLayout {
-  int plane_off, u_off, q_off, total;
-};
-__host__ __device__ inline StreamLayout stream_layout(int E, int plane_elems) {
-  StreamLayout L;
-  L.plane_off = 128;
-  L.u_off = (L.plane_off + plane_elems * 8 + 127) / 128 * 128;
-  L.q_off = L.u_off + E * E * 8;
-  L.total = L.q_off + E * E * 8;
-  return L;
-}
-
-// The first item from `it` on (stride `stride`) whose chain runs at `step`, or `items`.
-__device__ __forceinline__ int stream_next_active(const DevChains& ch, int E2, int items, int step, int it,
-                                                  int stride) {
-  for (; it < items; it += stride)
-    if (step <= ch.st[it / E2].L_cur) return it;
-  return items;
-}
-
-// One thread issues the copies of item `it`'s U (and q) planes into the buffers: one phase of the barrier.
-template <int E>
-__device__ __forceinline__ void stream_issue(const DevChains& ch, long long N, int E2, int it, bool first, bool need_q,
-                                          float2* bufU, float2* bufQ, uint64_t* bar) {
-  constexpr uint32_t bu = E * E * 8;
-  const int c = it / E2, z = it % E2;
-  const int acc = ch.st[c].acc;
-  const float2* Usrc = ch.U + ((long long)c * 2 + (first ? acc : (acc ^ 1))) * N + (long long)z * E * E;
-  mbar_arrive_expect_tx(bar, need_q ? 2 * bu : bu);
-  bulk_g2s(bufU, Usrc, bu, bar);
-  if (need_q) bulk_g2s(bufQ, ch.Q + (long long)c * N + (long long)z * E * E, bu, bar);
-}
-
-template <int E, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_xyplane_stream(DevVolume v, DevChains ch, int step, int flags,
-                                                             const float2* __restrict__ tw) {
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ double red[NT / 32];
-  __shared__ int s_next;
-  const StreamLayout Ly = stream_layout(E, PlaneGeom<E>::SIZE);
-  float2* sm = reinterpret_cast<float2*>(smraw + Ly.plane_off);
-  float2* bufU = reinterpret_cast<float2*>(smraw + Ly.u_off);
-  float2* bufQ = reinterpret_cast<float2*>(smraw + Ly.q_off);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
-  const int items = v.E2 * ch.C;
-  const bool first = step == 0;
-  const bool need_q = !(first && (flags & XF_FIXED_MOMENTUM) == 0);
-  if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-    const int it = stream_next_active(ch, v.E2, items, step, (int)blockIdx.x, (int)gridDim.x);
-    if (it < items) stream_issue<E>(ch, v.N, v.E2, it, first, need_q, bufU, bufQ, bar);
-    s_next = it;
-  }
-  __syncthreads();
-  int cur = s_next;
-  uint32_t phase = 0;
-  while (cur < items) {
-    const int c = cur / v.E2, z = cur % v.E2;
-    const ChainState& st = ch.st[c];
-    const int tid = opaque_tid();
-    plane_load_box<E, NT>(sm, ch.T2 + (long long)c * ch.t2_stride + (long long)z * v.by * v.bx, v.bx, v.by, tid);
-    __syncthreads();
-    plane_fft<E, 0>(sm, v.bx, v.by, +1, tw + tw_offset(E), tid);
-    const bool ok = mbar_wait_bounded(bar, phase);
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) {
-        atomicExch(ch.err, 1);
-        mbar_wait_bounded(bar, phase, 500000000ull);
-      }
-      return;
-    }
-    phase ^= 1;
-    double pa, pb;
-    {
-      const long long off = (long long)z * E * E;
-      plane_update<E, NT>(sm, v, ch, st, c, z, first, step == st.L_cur, need_q, flags, bufU, bufQ, v.sinv + off,
-                          ch.U + ((long long)c * 2 + (st.acc ^ 1)) * v.N + off, ch.Q + (long long)c * v.N + off, pa,
-                          pb, opaque_tid());
-    }
-    // every thread is done with the buffers: the next item's copies may overwrite them
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int nx = stream_next_active(ch, v.E2, items, step, cur + (int)gridDim.x, (int)gridDim.x);
-      if (nx < items) stream_issue<E>(ch, v.N, v.E2, nx, first, need_q, bufU, bufQ, bar);
-      s_next = nx;
-    }
-    plane_finish<E, NT>(sm, ch, c, z, first, step == ch.st[c].L_cur, pa, pb,
-                        ch.T2 + (long long)c * ch.t2_stride + (long long)z * v.by * v.bx, v.bx, v.by,
-                        tw + tw_offset(E), red, opaque_tid());
-    __syncthreads();
-    cur = s_next;
-  }
 }
 
 // ----------------------------------------------------------------- kriging products

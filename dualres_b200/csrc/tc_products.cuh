@@ -10,16 +10,14 @@
 // Precision: each FP32 operand is split as x = hi + lo (hi = the TF32 bits of
 // x, lo = x - hi, exact), and D accumulates hi_A hi_B + hi_A lo_B + lo_A hi_B
 // in FP32 (three kind::tf32 MMAs per K step), which keeps about 21 bits of
-// every product -- the FP32 CSR products' accuracy, not TF32's.  A is stored
-// as each chunk's nonzeros (FP32 value + 16-bit position in the 128 x 32 block,
-// 6 bytes each, against 16 KB for a dense chunk); the gather warps zero the
-// stage's A blocks and scatter the split values into them while their B loads
-// are in flight.
+// every product -- the FP32 CSR products' accuracy, not TF32's.  The blob holds
+// A in FP32 (16 KB per chunk); both splits are made in shared memory by the
+// gather warps, A's while their B loads are in flight.
 //
 // k_tc_product: one CTA per SM over a contiguous range of chunks (32 columns
 // of one tile).  Warp roles:
-//   warp 0     for W^T rs, issues the TMA row gathers of the chunk's chain
-//              vectors into the stage (mbarrier transaction count);
+//   warp 0     one thread bulk-copies the chunk's A block (16 KB) into the
+//              stage (mbarrier transaction count);
 //   warp 1     allocates TMEM; one thread issues the MMAs of a chunk when both
 //              its A and B are in, then commits the stage back to the
 //              producers; at a tile boundary it commits the accumulator;
@@ -28,10 +26,9 @@
 //              chunk's chain vectors X[col][chain] are loaded (coalesced over
 //              chains), all of a thread's loads before any is used -- or, for
 //              W^T rs, taken from shared memory where warp 0's TMA row gathers
-//              (tile::gather4) put them; meanwhile the stage's A blocks are
-//              zeroed and the chunk's nonzeros are scattered into them as hi
-//              and lo; then B is split and written as hi / lo in the K-major
-//              layout, and the stage is handed to the MMA thread;
+//              (tile::gather4) put them; meanwhile the landed A block is split
+//              in place into hi and lo; then B is split and written as hi / lo
+//              in the K-major layout, and the stage is handed to the MMA thread;
 //   last 4     epilogue: TMEM -> registers -> the segment's partial slot.
 // Every mbarrier wait is bounded; a wait that gives up records 3 in ch.err,
 // the roles drain their copies and MMAs, and TMEM is released.
@@ -55,11 +52,6 @@ constexpr int TC_KC = 32;               // columns per chunk
 constexpr int TC_BLK = TC_M * TC_KC;    // floats in one block (hi or lo) of a chunk
 constexpr int TC_HDR = 4096;            // barriers, TMEM address, chain offsets
 
-// Barrier of the nthreads threads (whole warps) that use barrier id.
-__device__ __forceinline__ void group_sync(int id, int nthreads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
-
 // Barrier of the nthreads threads (whole warps) that use barrier id, returning the AND of their v: every thread of
 // the group reaches it once per chunk, so a wait that gave up in one warp ends the group's loop in all of them.
 __device__ __forceinline__ bool group_all(bool v, int id, int nthreads) {
@@ -78,11 +70,11 @@ __device__ __forceinline__ bool group_all(bool v, int id, int nthreads) {
 __host__ __device__ constexpr int tc_stages(int N) { return N <= 64 ? 4 : (N <= 128 ? 3 : 2); }
 // Gather groups (chunks in flight in the gather): at most 3, and never more than the stages.  A group handles
 // chunks G apart and waits for stage s by the parity of empty[s]'s phase; before that wait it has only seen the
-// MMA of its previous chunk's stage complete (chunk q - S), so the phase it waits for (the MMA of chunk q + G - S)
-// is at most one phase ahead of the barrier only if G <= S.  With G > S the barrier can be two phases behind, the
-// parity test then reports the preceding phase as the awaited one, the group overwrites a stage whose MMA has not
-// run, and fullB's 128-arrival phases mix two groups' arrivals, after which the MMA thread waits for a phase that
-// never completes.
+// MMA of its previous chunk's stage complete (chunk q - G - S), so the phase before the awaited one (the MMA of
+// chunk q - 2S) is certain to be complete only if G <= S.  With G > S the barrier can be two phases behind, the
+// parity test then reports the preceding phase of the same parity as the awaited one, the group overwrites a
+// stage whose MMA has not run, and fullB's 128-arrival phases mix two groups' arrivals, after which the MMA thread
+// waits for a phase that never completes.
 __host__ __device__ constexpr int tc_groups(int N) { return tc_stages(N) < 3 ? tc_stages(N) : 3; }
 __host__ __device__ constexpr int tc_threads(int N) { return 32 * (2 + 4 * tc_groups(N) + 4); }
 __host__ __device__ inline int tc_stage_bytes(int N) { return 2 * TC_BLK * 4 + 2 * N * TC_KC * 4; }
@@ -146,26 +138,33 @@ __global__ void __launch_bounds__(tc_threads(N), 1)
   bool ok = true;
 
   if (warp == 0) {
-    // TMA row gathers (TG only): lanes 0-7 (and 8-15 for the second half of mu_D) gather 4 rows each.  A CTA's
-    // chunks are one contiguous range (its segments in order), and the column indices of the next chunk are
-    // loaded while the current one is issued.
+    // the whole warp: lane 0 bulk-copies A, lanes 0-7 (and 8-15 for the second half of mu_D) gather 4 rows each.
+    // A CTA's chunks are one contiguous range (its segments in order), and the column indices of the next chunk
+    // are loaded while the current one is issued.
+    const int halves = mode == 0 ? 2 : 1;
+    const uint32_t xbytes = TG ? (uint32_t)halves * TC_KC * N * 4 : 0u;
+    const int c_begin = seg0 < seg1 ? A.segs[seg0].y : 0, c_end = seg0 < seg1 ? A.segs[seg1 - 1].z : 0;
+    int jn = 0;
     if constexpr (TG) {
-      const int halves = mode == 0 ? 2 : 1;
-      const uint32_t xbytes = (uint32_t)halves * TC_KC * N * 4;
-      const int c_begin = seg0 < seg1 ? A.segs[seg0].y : 0, c_end = seg0 < seg1 ? A.segs[seg1 - 1].z : 0;
-      int jn = 0;
       if (c_begin < c_end) jn = __ldg(A.chunk_cols + (long long)c_begin * TC_KC + lane);
-      int q = 0;
-      for (int c = c_begin; c < c_end; c++, q++) {
-        const int s = q % stages;
-        int j = jn;
+    }
+    int q = 0;
+    for (int c = c_begin; c < c_end; c++, q++) {
+      const int s = q % stages;
+      int j = jn;
+      if constexpr (TG) {
         if (c + 1 < c_end) jn = __ldg(A.chunk_cols + (long long)(c + 1) * TC_KC + lane);
         if (j < 0) j = 0;
-        if (!__all_sync(0xffffffffu, q < stages || mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1))) {
-          ok = false;
-          break;
-        }
-        if (lane == 0) mbar_arrive_expect_tx(fullA + s, xbytes);
+      }
+      if (!__all_sync(0xffffffffu, q < stages || mbar_wait_bounded(empty + s, ((q / stages) & 1) ^ 1))) {
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
+        mbar_arrive_expect_tx(fullA + s, TC_BLK * 4 + xbytes);
+        bulk_g2s(stage0 + s * sbytes, A.blob + (long long)c * TC_BLK, TC_BLK * 4, fullA + s);
+      }
+      if constexpr (TG) {
         __syncwarp();
         const int h = lane >> 3, r4 = (lane & 7) * 4;
         const int y0 = __shfl_sync(0xffffffffu, j, r4), y1 = __shfl_sync(0xffffffffu, j, r4 + 1);
@@ -176,11 +175,11 @@ __global__ void __launch_bounds__(tc_threads(N), 1)
           tma_gather4(dst, &xmap, 0, y0 + ro, y1 + ro, y2 + ro, y3 + ro, fullA + s);
         }
       }
-      // the copies still in flight land before the CTA may exit
-      if (lane == 0)
-        for (int r = q - stages < 0 ? 0 : q - stages; r < q; r++) mbar_wait_bounded(fullA + r % stages, (r / stages) & 1);
-      if (!ok && lane == 0) atomicExch(ch.err, 3);
     }
+    // the copies still in flight land before the CTA may exit
+    if (lane == 0)
+      for (int r = q - stages < 0 ? 0 : q - stages; r < q; r++) mbar_wait_bounded(fullA + r % stages, (r / stages) & 1);
+    if (!ok && lane == 0) atomicExch(ch.err, 3);
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_tf32(TC_M, N);
@@ -288,29 +287,20 @@ __global__ void __launch_bounds__(tc_threads(N), 1)
             xv[i][2] = (on && j.z >= 0) ? __ldg(X + o + j.z * Cp) : 0.f;
             xv[i][3] = (on && j.w >= 0) ? __ldg(X + o + j.w * Cp) : 0.f;
           }
+          // A: hi in place, lo into the second block, while the loads above are in flight
+          if (!mbar_wait_bounded(fullA + s, (q / stages) & 1)) {
+            ok = false;
+            break;
+          }
         }
-        // A: zero both blocks (the MMAs of the stage's previous chunk are complete), then scatter the chunk's
-        // nonzeros as hi and lo; the B loads above stay in flight meanwhile
         float4* ah = reinterpret_cast<float4*>(stage0 + s * sbytes);
         float4* al = ah + TC_BLK / 4;
 #pragma unroll
         for (int i = 0; i < TC_BLK / 4 / 128; i++) {
-          ah[t + 128 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
-          al[t + 128 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        group_sync(1 + grp, 128);
-        {
-          float* ahf = reinterpret_cast<float*>(ah);
-          float* alf = reinterpret_cast<float*>(al);
-          const int z0 = __ldg(A.nz_ptr + c), z1 = __ldg(A.nz_ptr + c + 1);
-#pragma unroll 4
-          for (int z = z0 + t; z < z1; z += 128) {
-            const float a = __ldg(A.nz_val + z);
-            const int pos = __ldg(A.nz_pos + z);
-            const float h = tf32_hi(a);
-            ahf[pos] = h;
-            alf[pos] = a - h;
-          }
+          const float4 a = ah[t + 128 * i];
+          const float4 h = make_float4(tf32_hi(a.x), tf32_hi(a.y), tf32_hi(a.z), tf32_hi(a.w));
+          ah[t + 128 * i] = h;
+          al[t + 128 * i] = make_float4(a.x - h.x, a.y - h.y, a.z - h.z, a.w - h.w);
         }
 #pragma unroll
         for (int i = 0; i < NI; i++) {
@@ -460,11 +450,10 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
   }
 }
 
-// Packs the CSR values chunk by chunk: value k to slot[k] of nz_val.
-__global__ void k_tc_pack(const float* __restrict__ val, const int* __restrict__ slot, int nnz,
-                          float* __restrict__ nz_val) {
+// Scatters the CSR values into the dense blob (zeroed first): value k at dest[k].
+__global__ void k_tc_fill(const float* __restrict__ val, const int* __restrict__ dest, int nnz, float* __restrict__ blob) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < nnz) nz_val[slot[k]] = val[k];
+  if (k < nnz) blob[dest[k]] = val[k];
 }
 
 }  // namespace drb

@@ -36,27 +36,19 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.fixture(params=["plane", "prefetch", "prefetch256", "stream", "stream256", "lines"])
+@pytest.fixture(params=["plane", "prefetch", "lines"])
 def update_path(request, monkeypatch):
-    """The device update paths: the fused xy-plane kernel (E0 == E1 <= 128, the
-    default); the same kernel with bulk-copy prefetch of the state planes (512 or
-    256 threads per block); the persistent plane kernel that streams the next
-    plane's state into shared memory (512 or 256 threads); and the x-line kernel
-    with separate y passes (every other embedding)."""
-    for k in ("DRB_NO_PLANE", "DRB_PLANE_PREFETCH", "DRB_PLANE_PREFETCH_THREADS", "DRB_PLANE_STREAM",
-              "DRB_PLANE_STREAM_THREADS"):
-        monkeypatch.delenv(k, raising=False)
+    """The three device update paths: the fused xy-plane kernel (E0 == E1 <= 128,
+    the default), the same kernel with bulk-copy prefetch of the state planes,
+    and the x-line kernel with separate y passes (every other embedding)."""
+    monkeypatch.delenv("DRB_NO_PLANE", raising=False)
+    monkeypatch.delenv("DRB_PLANE_PREFETCH", raising=False)
     monkeypatch.setenv("DRB_AUTOTUNE", "0")  # the path under test, not the tuner's choice
-    p = request.param
-    if p == "lines":
+    if request.param == "lines":
         monkeypatch.setenv("DRB_NO_PLANE", "1")
-    elif p.startswith("prefetch"):
+    elif request.param == "prefetch":
         monkeypatch.setenv("DRB_PLANE_PREFETCH", "1")
-        monkeypatch.setenv("DRB_PLANE_PREFETCH_THREADS", "256" if p.endswith("256") else "512")
-    elif p.startswith("stream"):
-        monkeypatch.setenv("DRB_PLANE_STREAM", "1")
-        monkeypatch.setenv("DRB_PLANE_STREAM_THREADS", "256" if p.endswith("256") else "512")
-    return p
+    return request.param
 
 
 def volume_of(g):
