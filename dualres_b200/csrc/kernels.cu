@@ -208,10 +208,13 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
 // last step only kicks and accumulates the final energies (:702-705).
 template <int E0> struct XCfg {
   static constexpr int NT = E0 >= 512 ? 512 : 256;
+  // blocks per SM the register budget targets: at E0 = 256 the 67.6 KB tile allows three (85 registers, no
+  // spills; two at the unconstrained 126 registers), at E0 <= 128 four
+  static constexpr int MINB = E0 >= 512 ? 1 : (E0 == 256 ? 3 : 4);
 };
 
 template <int E0>
-__global__ void __launch_bounds__(XCfg<E0>::NT) k_xline(DevVolume v, DevChains ch, int step, int flags,
+__global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolume v, DevChains ch, int step, int flags,
                                                         const float2* __restrict__ tw) {
   constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = XCfg<E0>::NT;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -607,6 +610,11 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
 // Chain-minor operands: X[j * Cp + c].  A warp's lanes are CG chain lanes x
 // G = 32 / CG nonzero groups; each lane owns NR chains (c = cc + CG r).
 //
+// Batches of 32 nonzeros whose values and columns a warp loads before using any (csr_batches): 8 for 2-8 chains
+// per warp (four chains on a 256x256x128 embedding: W 263 -> 235 us), 2 for one chain (deeper was slower there:
+// 12.5 against 10.2 us on a 32^3 volume) and for 16, 1 for 32 (their gathers already overlap).
+__host__ __device__ constexpr int csr_prefetch(int CG) { return (CG >= 2 && CG <= 8) ? 8 : (CG == 32 ? 1 : 2); }
+
 // Accumulates sum_k val[k] X[col[k]] over the 32-nonzero batches b0, b0 + bs,
 // ... of [ks, ke): the batch's values and columns are loaded once, coalesced,
 // and broadcast by shuffle, so the X loads of a batch are independent and
@@ -695,9 +703,9 @@ __global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, in
     float acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
-    // two batches ahead help narrow chain groups; with 32 chains per warp the gathers already overlap
-    csr_batches<CG, NR, (CG == 32 ? 1 : 2)>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], warp, 8, x, Cp,
-                                            lane, acc);
+    // batches ahead keep the matrix stream in flight (csr_prefetch)
+    csr_batches<CG, NR, csr_prefetch(CG)>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], warp, 8, x, Cp,
+                                          lane, acc);
     if (lane < CG) {
 #pragma unroll
       for (int r = 0; r < NR; r++) red[warp][lane + CG * r] = acc[r];
@@ -755,7 +763,8 @@ __global__ void __launch_bounds__(256, 4) k_spmv_wt(DevVolume v, DevChains ch, i
 #pragma unroll
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
     if (v.n_s > 0)
-      csr_batches<CG, NR, 2>(v.wt_val, v.wt_col, v.wt_rowptr[row], v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc);
+      csr_batches<CG, NR, csr_prefetch(CG) < 2 ? 2 : csr_prefetch(CG)>(v.wt_val, v.wt_col, v.wt_rowptr[row],
+                                                                       v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc);
     if (lane < CG) {
       const float yh = v.Yh[row];
 #pragma unroll
