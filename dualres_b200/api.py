@@ -103,16 +103,17 @@ _lib = None
 
 
 def lib_path():
-    return _build.LIB
+    """The library this process loads: the bounds-checked build when DRB_LIBRARY=checked, else the release build."""
+    return _build.LIB_CHECKED if os.environ.get("DRB_LIBRARY") == "checked" else _build.LIB
 
 
 def lib(build_if_missing=True):
     """Load the in-tree shared library (building it if it is missing or stale)."""
     global _lib
     if _lib is None:
-        path = _build.LIB
+        path = lib_path()
         if build_if_missing:
-            _build.build()
+            _build.build(checked=path == _build.LIB_CHECKED)
         if not os.path.exists(path):
             raise DrError(DR_ERR_STATE, f"CUDA library not built: {path}")
         L = C.CDLL(path)
@@ -137,6 +138,7 @@ def _declare(L):
     L.dr_volume_destroy.restype = None
     L.dr_chainset_create.argtypes = [vp, C.c_int, C.POINTER(HmcOpts), C.POINTER(vp)]
     L.dr_chainset_config_get.argtypes = [vp, _ip, _ip, _dp, _ip]
+    L.dr_chainset_ztile_get.argtypes = [vp, _ip]
     L.dr_chainset_destroy.argtypes = [vp]
     L.dr_chainset_destroy.restype = None
     L.dr_step.argtypes = [vp, C.c_int]
@@ -376,8 +378,10 @@ class MultiResParameters:
         whether the kriging products run on the tensor cores."""
         p, g, ms, tc = C.c_int(0), C.c_int(0), C.c_double(0), C.c_int(0)
         check(lib().dr_chainset_config_get(self.h, C.byref(p), C.byref(g), C.byref(ms), C.byref(tc)))
+        zt = C.c_int(0)
+        check(lib().dr_chainset_ztile_get(self.h, C.byref(zt)))
         return dict(path=self.PATHS[p.value], blocks_per_sm=g.value, tuned_ms=ms.value,
-                    tensor_products=bool(tc.value), tma_row_gather=tc.value == 2)
+                    tensor_products=bool(tc.value), tma_row_gather=tc.value == 2, z_tile_chains=zt.value)
 
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))

@@ -16,6 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libdualres_b200.so")
+# the bounds-checked build (DRB_BOUNDS_CHECK): every data-dependent index tested before its access; loaded instead of
+# LIB when DRB_LIBRARY=checked
+LIB_CHECKED = os.path.join(LIBDIR, "libdualres_b200_checked.so")
 SOURCES = ["api.cu", "host_setup.cpp", "estimate.cpp"]
 DEPS = ["api.cu", "kernels.cu", "common.cuh", "fft.cuh", "tma.cuh", "mce.cuh", "kriging.cuh", "umma.cuh",
         "tc_products.cuh", "drb.h", "host_setup.cpp", "host_setup.h", "estimate.cpp", "estimate.h"]
@@ -32,10 +35,10 @@ def nvcc_path():
     raise RuntimeError("nvcc not found")
 
 
-def _stale():
-    if not os.path.exists(LIB):
+def _stale(lib=LIB):
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     inc = os.path.join(HERE, "..", "include", "dualres_b200.h")
     deps = [os.path.join(CSRC, d) for d in DEPS] + [inc]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
@@ -68,16 +71,13 @@ def build_cli(force=False, verbose=False):
     return CLI
 
 
-def build(force=False, verbose=False):
-    if not force and not _stale():
-        build_cli(force, verbose)
-        return LIB
+def _compile(lib, extra, verbose):
     os.makedirs(LIBDIR, exist_ok=True)
     gxx = shutil.which("g++") or "g++"
-    cmd = [nvcc_path(), "-shared", "-std=c++17", "-O3", "-lineinfo", *ARCH,
+    cmd = [nvcc_path(), "-shared", "-std=c++17", "-O3", "-lineinfo", *ARCH, *extra,
            "-ccbin", gxx, "-Xcompiler", "-fPIC,-fopenmp,-O3",
            "--expt-relaxed-constexpr", "-Xptxas", "-O3",
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES], "-lgomp"]
+           "-o", lib + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES], "-lgomp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), flush=True)
@@ -85,11 +85,21 @@ def build(force=False, verbose=False):
     if res.returncode != 0:
         sys.stderr.write((res.stdout or "") + (res.stderr or ""))
         raise RuntimeError("nvcc failed")
-    os.replace(LIB + ".tmp", LIB)
-    build_cli(True, verbose)
+    os.replace(lib + ".tmp", lib)
+
+
+def build(force=False, verbose=False, checked=False):
+    """The library (and the dualgpmf command line); with checked=True also the bounds-checked library."""
+    if force or _stale():
+        _compile(LIB, [], verbose)
+        build_cli(True, verbose)
+    else:
+        build_cli(force, verbose)
+    if checked and (force or _stale(LIB_CHECKED)):
+        _compile(LIB_CHECKED, ["-DDRB_BOUNDS_CHECK"], verbose)
     return LIB
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, checked="--checked" in sys.argv)
     print(LIB)

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include <cudaTypedefs.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/dualres_b200.h"
 #include "host_setup.h"
@@ -59,6 +60,14 @@ struct Error : std::runtime_error {
   } while (0)
 
 static int cdiv_i(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// An NVTX range for the enclosing scope (shown by Nsight tools; no cost without one attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ---------------------------------------------------------------- per-device set-up
 struct DeviceTables {
@@ -170,8 +179,9 @@ static void launch_pass_n(int dir, int pro, int epi, const PassArgs& a, const De
   else if (dir > 0 && pro == PRO_LOAD && epi == EPI_STORE)
     k_pass<N, +1, PRO_LOAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
   else if constexpr (sizeof(C) == 8) {
-    // the z passes touch the chain-minor arrays: with 8 or more chains, tiles of 4 lines x 8 chains
-    const bool grouped = a.chain_only < 0 && nch >= 8 && a.B > 1;
+    // the z passes touch the chain-minor arrays: with 8 or more chains, tiles of 4 lines x 8 chains unless the chain
+    // set's tuning chose tiles of 32 lines of one chain (ch.ztile)
+    const bool grouped = a.chain_only < 0 && nch >= 8 && a.B > 1 && ch.ztile != 1;
     const dim3 ggrid(cdiv_i((long long)a.A * a.B, TILE_LINES / 8), cdiv_i(nch, 8));
     if (dir > 0 && pro == PRO_DATAGRAD && epi == EPI_STORE) {
       if (grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
@@ -487,6 +497,7 @@ static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
 
 // Device part of a volume from an already prepared HostVolume (V->hv).
 static void volume_build_device(Volume* V, const float* covariance, int covfun, int device) {
+  const NvtxRange range("volume: device set-up (kriging solves, FP64 spectrum)");
   const auto t0 = std::chrono::steady_clock::now();
   V->device = device;
   DeviceTables& dt = device_tables(device);
@@ -556,6 +567,7 @@ static void volume_build_device(Volume* V, const float* covariance, int covfun, 
 }
 
 static void volume_build(Volume* V, const dr_volume_desc* d) {
+  const NvtxRange range("volume: create");
   const auto t0 = std::chrono::steady_clock::now();
   device_tables(d->device);
   std::string err;
@@ -642,9 +654,15 @@ static void volume_release(Volume* v) {
 template <int CG, int NR>
 static void launch_spmv_t(const DevVolume& v, const DevChains& ch, int nb, int step, int sel, int chain_only, bool w,
                           cudaStream_t s) {
-  if (w)
+  // a block per row while a block gets few rows; with at most 8 chains per warp, a warp per row once a block would
+  // take 8 or more of them in turn
+  bool rows = false;
+  if constexpr (CG <= 8) rows = w && v.n_s >= 8 * nb;
+  if (rows) {
+    if constexpr (CG <= 8) k_spmv_w_rows<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
+  } else if (w) {
     k_spmv_w<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
-  else
+  } else
     k_spmv_wt<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
   CK_LAUNCH();
 }
@@ -779,6 +797,8 @@ static void enqueue_steps(Chainset* S, int L, int flags) {
   const float2* tw = S->vol->tw_f;
   const int C = S->C;
   for (int s = 0; s <= L; s++) {
+    const NvtxRange range(s == 0 ? "leapfrog step 0 (momentum, half kick, drift)"
+                                 : (s == L ? "leapfrog last step (half kick, energies)" : "leapfrog step"));
     const int sel = s == 0 ? 0 : 1;
     if (s > 0) {
       if (!S->plane)
@@ -860,8 +880,11 @@ static void init_chain_states(Chainset* S) {
 // planes whose padded layout fits shared memory), the same with bulk prefetch
 // of the state planes, and the x-line kernel with separate y passes (always).
 // ---------------------------------------------------------------- tensor-core kriging products
-static void tc_upload(Volume* V, const TcPlanHost& P, const float* dval, int nnz, DevTcMatrix* M) {
+static void tc_upload(Volume* V, const TcPlanHost& P, const float* dval, int nnz, int n_rows, int n_cols,
+                      DevTcMatrix* M) {
   cudaStream_t st = V->stream;
+  M->n_rows = n_rows;
+  M->n_cols = n_cols;
   M->T = P.T;
   M->G = P.G;
   M->n_segs = (int)(P.segs.size() / 4);
@@ -929,8 +952,8 @@ static bool volume_tc(Volume* V) {
   CK(cudaMemGetInfo(&fr, &tot));
   const double blob_bytes = (double)(pw.chunks + pt.chunks) * TC_BLK * 4;
   if (blob_bytes > 0.25 * (double)fr) return false;
-  tc_upload(V, pw, dv.w_val, (int)hv.w_col.size(), &V->tc_w);
-  tc_upload(V, pt, dv.wt_val, (int)hv.wt_col.size(), &V->tc_wt);
+  tc_upload(V, pw, dv.w_val, (int)hv.w_col.size(), dv.n_s, dv.n_h, &V->tc_w);
+  tc_upload(V, pt, dv.wt_val, (int)hv.wt_col.size(), dv.n_h, dv.n_s, &V->tc_wt);
   V->tc_max_segs = std::max(V->tc_w.n_segs, V->tc_wt.n_segs);
   CK(cudaStreamSynchronize(V->stream));
   V->tc_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -994,6 +1017,7 @@ static PathOptions path_options(const DevVolume& v, int device) {
 }
 
 struct TuneChoice {
+  int ztile = 8;     // chains per z-pass tile (8 or 1) for chain sets of 8 or more chains
   int path = 0;      // 0 plane, 1 plane + prefetch, 2 x-line
   int grid = 8;      // kriging-product blocks per SM (CSR products)
   double ms = 0.0;   // measured milliseconds per iteration
@@ -1006,7 +1030,7 @@ static bool autotune_enabled() {
 }
 
 struct TuneKey {
-  int dev, E0, E1, E2, bx, by, bz, C, n_h, n_s, L;
+  int dev, E0, E1, E2, bx, by, bz, C, n_h, n_s, L;  // n_h, n_s as tune_bucket()s
   bool operator<(const TuneKey& o) const {
     return std::tie(dev, E0, E1, E2, bx, by, bz, C, n_h, n_s, L) <
            std::tie(o.dev, o.E0, o.E1, o.E2, o.bx, o.by, o.bz, o.C, o.n_h, o.n_s, o.L);
@@ -1047,9 +1071,15 @@ struct PoolKeep {
   }
 };
 
+// Quarter-octave bucket of a voxel count: volumes of one shape whose data counts differ by less than about 19 %
+// share a tuning result (it chooses a speed, not a result), so a stream of similar jobs tunes once.
+static int tune_bucket(int n) { return n <= 0 ? -1 : (int)std::lround(4.0 * std::log2((double)n)); }
+
 static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
+  const NvtxRange range("chain set: tuning");
   const DevVolume& v = V->dv;
-  const TuneKey key{V->device, v.E0, v.E1, v.E2, v.bx, v.by, v.bz, C, v.n_h, v.n_s, o->leapfrog};
+  const TuneKey key{V->device, v.E0, v.E1, v.E2, v.bx, v.by, v.bz, C, tune_bucket(v.n_h), tune_bucket(v.n_s),
+                    o->leapfrog};
   {
     std::lock_guard<std::mutex> lk(g_tune_mtx);
     auto it = g_tune.find(key);
@@ -1095,14 +1125,20 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   };
   for (int path : {0, 1, 2}) {
     if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) continue;
-    try_candidate(TuneChoice{path, 8, 0.0, tc ? 1 : 0});
+    try_candidate(TuneChoice{8, path, 8, 0.0, tc ? 1 : 0});
   }
   if (best.ms < 1e300) {
     const int path = best.path;
-    if (tc) try_candidate(TuneChoice{path, 8, 0.0, 0});
+    if (tc) try_candidate(TuneChoice{8, path, 8, 0.0, 0});
     // narrower chain sets may do better with fewer, longer-lived CSR product blocks
     if (C < 32)
-      for (int grid : {4, 2}) try_candidate(TuneChoice{path, grid, 0.0, 0});
+      for (int grid : {4, 2}) try_candidate(TuneChoice{8, path, grid, 0.0, 0});
+    // the z passes' tile shape on the best configuration: 32 lines of one chain instead of 4 lines x 8 chains
+    if (C >= 8) {
+      TuneChoice t = best;
+      t.ztile = 1;
+      try_candidate(t);
+    }
   }
   if (!(best.ms < 1e300)) {  // nothing could be timed: default, not cached
     TuneChoice d;
@@ -1152,10 +1188,13 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   // override the default
   int tc = C >= 32 ? 1 : 0;
   if (const char* e = std::getenv("DRB_TC_PRODUCTS")) tc = std::atoi(e) != 0;
+  int ztile = 8;
+  if (const char* e = std::getenv("DRB_ZTILE")) ztile = std::atoi(e) == 1 ? 1 : 8;
   if (forced) {
     path = forced->path;
     grid = forced->grid;
     tc = forced->tc;
+    ztile = forced->ztile;
   } else if (std::getenv("DRB_NO_PLANE")) {
     path = 2;
   } else if (std::getenv("DRB_PLANE_PREFETCH")) {
@@ -1164,6 +1203,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     const TuneChoice t = autotune(V, C, o);
     path = t.path;
     grid = t.grid;
+    if (!std::getenv("DRB_ZTILE")) ztile = t.ztile;
     if (!std::getenv("DRB_TC_PRODUCTS")) tc = t.tc;
     S->tuned_ms = t.ms;
   }
@@ -1212,6 +1252,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   ch.save_rec = o->store_samples ? S->alloc<double>((size_t)std::max(o->nsave, 1) * C * 3, true) : nullptr;
   ch.seed = o->seed;
   ch.chain0 = 0;
+  ch.ztile = ztile;
   ch.err = S->alloc<int>(1);
   S->tmp = S->alloc<float2>(N);
   init_chain_states(S);
@@ -1269,6 +1310,7 @@ static void ensure_graph(Chainset* S) {
 static void launch_iterations(Chainset* S, int iters) {
   ensure_graph(S);
   for (int i = 0; i < iters; i++) {
+    const NvtxRange range("HMC iteration (graph)");
     CK(cudaGraphLaunch(S->graph, S->stream));
     g_launches += S->graph_nodes;
   }
@@ -1280,6 +1322,7 @@ static void check_device_error(Chainset* S) {
   int err = 0;
   CK(cudaMemcpyAsync(&err, S->dc.err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
   CK(cudaStreamSynchronize(S->stream));
+  if (err == ERR_BOUNDS) throw Error(DR_ERR_STATE, "a bounds check failed: an index left its array (checked build)");
   if (err == 3) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core kriging product pipeline)");
   if (err) throw Error(DR_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
 }
@@ -1294,6 +1337,7 @@ static void step(Chainset* S, int iters, double* device_ms = nullptr) {
     CK(cudaEventRecord(e0, S->stream));
   }
   for (int i = 0; i < iters; i++) {
+    const NvtxRange range("HMC iteration (graph)");
     CK(cudaGraphLaunch(S->graph, S->stream));
     g_launches += S->graph_nodes;
   }
@@ -1351,10 +1395,10 @@ static void upload_field(Chainset* S, const float* mu) {
 
 static void gather_data(Chainset* S, const float2* field, int c, int half, bool with_output) {
   const DevVolume& v = S->vol->dv;
-  k_gather_re<<<cdiv_i(v.n_h, 256), 256, 0, S->stream>>>(field, v.d_flat, v.n_h, S->dc.muD + (long long)half * v.n_h * S->C, S->C, c);
+  k_gather_re<<<cdiv_i(v.n_h, 256), 256, 0, S->stream>>>(field, v.d_flat, v.n_h, S->dc.muD + (long long)half * v.n_h * S->C, S->C, c, v.N, S->dc.err);
   CK_LAUNCH();
   if (with_output && v.n_o > 0) {
-    k_gather_re<<<cdiv_i(v.n_o, 256), 256, 0, S->stream>>>(field, v.o_flat, v.n_o, S->dc.muO + (long long)half * v.n_o * S->C, S->C, c);
+    k_gather_re<<<cdiv_i(v.n_o, 256), 256, 0, S->stream>>>(field, v.o_flat, v.n_o, S->dc.muO + (long long)half * v.n_o * S->C, S->C, c, v.N, S->dc.err);
     CK_LAUNCH();
   }
 }
@@ -1376,6 +1420,7 @@ static double part_sum(Chainset* S, int c, int slot, int nb) {
 // its step-0 partial sums are the energies at mu.  It works in the proposal half of the chain's buffers and in the
 // momentum, which hold nothing between iterations, so the chain's state is unchanged.
 static void eval_sampler(Chainset* S, int chain, const float* mu, double* lpll, float* grad) {
+  const NvtxRange range("evaluation (sampler step 0)");
   CK(cudaSetDevice(S->vol->device));
   const DevVolume& v = S->vol->dv;
   std::vector<ChainState> st, saved;
@@ -1456,7 +1501,11 @@ struct dr_chainset : Chainset {};
 extern "C" {
 
 const char* dr_last_error(void) { return g_err.c_str(); }
+#ifdef DRB_BOUNDS_CHECK
+const char* dr_version(void) { return "dualres_b200 0.1 (sm_100a, bounds-checked)"; }
+#else
 const char* dr_version(void) { return "dualres_b200 0.1 (sm_100a)"; }
+#endif
 int64_t dr_kernel_launches(int reset) {
   const int64_t n = g_launches;
   if (reset) g_launches = 0;
@@ -1561,6 +1610,13 @@ int dr_chainset_config_get(const dr_chainset* s, int* path, int* blocks_per_sm, 
   if (blocks_per_sm) *blocks_per_sm = s->grid;
   if (tuned_ms) *tuned_ms = s->tuned_ms;
   if (tensor_products) *tensor_products = s->tcp ? (s->tc_tg ? 2 : 1) : 0;
+  API_END
+}
+
+int dr_chainset_ztile_get(const dr_chainset* s, int* z_tile_chains) {
+  API_BEGIN
+  if (!s || !z_tile_chains) throw Error(DR_ERR_INVALID, "NULL argument");
+  *z_tile_chains = s->C >= 8 && s->dc.ztile != 1 ? 8 : 1;
   API_END
 }
 
@@ -1775,6 +1831,7 @@ int dr_leapfrog_fixed(dr_chainset* s, int chain, const float* mu0, const float* 
   // the chain keeps mu0 as its state; the other chains are untouched
   for (int c = 0; c < s->C; c++) saved[c].L_cur = -1;
   write_states(s, saved);
+  check_device_error(s);
   API_END
 }
 
@@ -2041,8 +2098,14 @@ struct Server {
   std::condition_variable cv_work, cv_done;
   std::map<uint64_t, std::shared_ptr<Job>> jobs;
   std::deque<std::shared_ptr<Job>> setup_q, ready_q;
+  // admitted jobs whose device set-up (kriging solves, spectrum, chain set and its tuning) runs on a device-set-up
+  // thread, so that the scheduler keeps launching the resident jobs' rounds meanwhile; then built, for the scheduler
+  std::deque<std::shared_ptr<Job>> device_q, built_q;
+  int in_device_setup = 0;
+  int64_t reserved = 0;  // footprint estimates of the jobs in device set-up (admission counts them with in_use)
   std::vector<std::shared_ptr<Job>> active;  // scheduler thread only
-  std::vector<std::thread> workers;
+  std::vector<std::thread> workers, device_workers;
+  std::condition_variable cv_device;
   std::thread sched;
   bool stop = false;
   uint64_t next_id = 1;
@@ -2100,6 +2163,58 @@ struct Server {
     }
   }
 
+  // Device set-up of admitted jobs (volume on the device, chain set with its tuning), each on the job's own streams,
+  // concurrent with the scheduler's launches; the job's reserved estimate is then replaced by its allocated bytes.
+  void device_worker_loop() {
+    cudaSetDevice(o.device);
+    for (;;) {
+      std::shared_ptr<Job> j;
+      {
+        std::unique_lock<std::mutex> lk(mtx);
+        cv_device.wait(lk, [&] { return stop || !device_q.empty(); });
+        if (stop) return;
+        j = device_q.front();
+        device_q.pop_front();
+      }
+      int64_t bytes = 0;
+      int code = DR_OK;
+      std::string msg;
+      try {
+        volume_build_device(j->vol.get(), j->desc.covariance, j->desc.covfun, o.device);
+        auto cs = std::make_unique<Chainset>();
+        chainset_build(cs.get(), j->vol.get(), j->C, &j->opts);
+        bytes = j->vol->bytes + cs->bytes;
+        j->cs = std::move(cs);
+        j->iters_total = j->opts.burnin + (j->opts.thin == 0 ? 1 : j->opts.thin) * j->opts.nsave;
+      } catch (const Error& e) {
+        code = e.code;
+        msg = e.what();
+      } catch (const std::bad_alloc&) {
+        code = DR_ERR_NOMEM;
+        msg = "host allocation failed";
+      } catch (const std::exception& e) {
+        code = DR_ERR_INVALID;
+        msg = e.what();
+      }
+      if (code != DR_OK) {
+        fail_resident(j, code, msg, false);
+        std::lock_guard<std::mutex> lk(mtx);
+        reserved -= j->est_bytes;
+        in_device_setup--;
+        cv_work.notify_all();
+        continue;
+      }
+      std::lock_guard<std::mutex> lk(mtx);
+      reserved -= j->est_bytes;
+      in_use += bytes;
+      peak_bytes = std::max(peak_bytes, in_use);
+      j->bytes = bytes;
+      in_device_setup--;
+      built_q.push_back(j);
+      cv_work.notify_all();
+    }
+  }
+
   // Reads a finished job's summary and frees its device objects; the fields that dr_server_status and
   // dr_server_result read are published under mtx together with the DONE state.
   void finalize(const std::shared_ptr<Job>& j) {
@@ -2149,41 +2264,25 @@ struct Server {
   void scheduler_loop() {
     cudaSetDevice(o.device);
     for (;;) {
-      // admit prepared jobs that fit
-      while ((int)active.size() < o.max_active) {
-        std::shared_ptr<Job> j;
-        {
-          std::lock_guard<std::mutex> lk(mtx);
-          if (stop || ready_q.empty()) break;
-          j = ready_q.front();
-          if (in_use + j->est_bytes > budget && !active.empty()) break;
-          ready_q.pop_front();
-        }
-        int64_t bytes = 0;
-        try {
-          volume_build_device(j->vol.get(), j->desc.covariance, j->desc.covfun, o.device);
-          auto cs = std::make_unique<Chainset>();
-          chainset_build(cs.get(), j->vol.get(), j->C, &j->opts);
-          bytes = j->vol->bytes + cs->bytes;
-          j->cs = std::move(cs);
-          j->iters_total = j->opts.burnin + (j->opts.thin == 0 ? 1 : j->opts.thin) * j->opts.nsave;
-        } catch (const Error& e) {
-          fail_resident(j, e.code, e.what(), false);
-          continue;
-        } catch (const std::bad_alloc&) {
-          fail_resident(j, DR_ERR_NOMEM, "host allocation failed", false);
-          continue;
-        } catch (const std::exception& e) {
-          fail_resident(j, DR_ERR_INVALID, e.what(), false);
-          continue;
-        }
+      // admit prepared jobs that fit: their estimated footprint is reserved and their device set-up handed to the
+      // device-set-up threads; built jobs join the resident set
+      {
         std::lock_guard<std::mutex> lk(mtx);
-        j->bytes = bytes;
-        j->state = DR_JOB_RUNNING;
-        j->t_admit = now();
-        in_use += j->bytes;
-        peak_bytes = std::max(peak_bytes, in_use);
-        active.push_back(j);
+        while (!stop && !ready_q.empty() && (int)active.size() + in_device_setup < o.max_active) {
+          std::shared_ptr<Job> j = ready_q.front();
+          if (in_use + reserved + j->est_bytes > budget && !(active.empty() && in_device_setup == 0)) break;
+          ready_q.pop_front();
+          reserved += j->est_bytes;
+          j->state = DR_JOB_RUNNING;
+          j->t_admit = now();
+          in_device_setup++;
+          device_q.push_back(j);
+          cv_device.notify_one();
+        }
+        while (!built_q.empty()) {
+          active.push_back(built_q.front());
+          built_q.pop_front();
+        }
         peak_running = std::max(peak_running, (int)active.size());
       }
       // advance every resident job by one round, finalise finished ones
@@ -2275,6 +2374,8 @@ int dr_server_create(const dr_server_opts* opts, dr_server** out) {
   const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
   const int per = std::max(1, hw / sv->o.host_threads);
   for (int i = 0; i < sv->o.host_threads; i++) sv->workers.emplace_back([sv, per] { sv->worker_loop(per); });
+  // two device-set-up threads: one job's kriging solves and tuning overlap another's, and the resident jobs' rounds
+  for (int i = 0; i < 2; i++) sv->device_workers.emplace_back([sv] { sv->device_worker_loop(); });
   sv->sched = std::thread([sv] { sv->scheduler_loop(); });
   *out = sv;
   API_END
@@ -2287,7 +2388,9 @@ void dr_server_destroy(dr_server* sv) {
     sv->stop = true;
   }
   sv->cv_work.notify_all();
+  sv->cv_device.notify_all();
   for (auto& t : sv->workers) t.join();
+  for (auto& t : sv->device_workers) t.join();
   if (sv->sched.joinable()) sv->sched.join();
   delete sv;
 }
@@ -2626,7 +2729,8 @@ extern "C" int dr_log_posterior_noalloc(const dr_volume* v, const float* mu_devi
   cudaStream_t s = 0;
   CK(cudaMemcpyAsync(st, &h, sizeof(ChainState), cudaMemcpyHostToDevice, s));
   // Re mu at the data voxels, then the kriging residuals and their norms
-  k_gather_re<<<cdiv_i(dv.n_h, 256), 256, 0, s>>>((const float2*)mu_device, dv.d_flat, dv.n_h, ch.muD, 1, 0);
+  k_gather_re<<<cdiv_i(dv.n_h, 256), 256, 0, s>>>((const float2*)mu_device, dv.d_flat, dv.n_h, ch.muD, 1, 0, dv.N,
+                                                   nullptr);
   CK_LAUNCH();
   if (dv.n_s > 0) launch_spmv_dc(dv, ch, 1, -1, 0, 0, true, s);
   launch_spmv_dc(dv, ch, 1, -1, 0, 0, false, s);

@@ -103,4 +103,23 @@ __device__ __forceinline__ double block_sum(double v, double* scratch) {
   return s;
 }
 
+// ---------------------------------------------------------------- bounds checks
+// Builds with DRB_BOUNDS_CHECK (the checked library, a debug build that stands in for a memory checker) test every
+// data-dependent index before its access: an index outside [0, n) records 4 in the error word (when one is given)
+// and the caller skips the access, so the kernel neither faults nor reads out of range, and the host reports the
+// failure after the launch.  In other builds the test is a constant true and costs nothing.
+constexpr int ERR_BOUNDS = 4;
+__device__ __forceinline__ bool in_bounds(long long i, long long n, int* err) {
+#ifdef DRB_BOUNDS_CHECK
+  if (i >= 0 && i < n) return true;
+  if (err) atomicExch(err, ERR_BOUNDS);
+  return false;
+#else
+  (void)i;
+  (void)n;
+  (void)err;
+  return true;
+#endif
+}
+
 }  // namespace drb

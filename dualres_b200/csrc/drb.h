@@ -95,6 +95,7 @@ struct DevChains {
   uint64_t seed;
   int chain0;               // global id of chain 0 (RNG key component)
   int* err;                 // device error word: bounded waits that gave up
+  int ztile;                // chains per z-pass tile with 8 or more chains: 8 (4 lines x 8 chains) or 1 (32 lines)
 };
 
 // A kriging matrix (W or W^T) cut into dense tiles for the tensor-core
@@ -105,6 +106,7 @@ struct DevChains {
 // split into contiguous ranges, one per CTA; a range cut at tile boundaries
 // gives segments, each summing into its own partial slot.
 struct DevTcMatrix {
+  int n_rows, n_cols;       // the matrix's shape (W: n_s x n_h; W^T: n_h x n_s)
   int T;                    // tiles
   int G;                    // CTAs of the product kernel (0: no nonzeros)
   int n_segs;

@@ -145,16 +145,21 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
   auto chain = [&](int l) { return cbase + l / LPC; };
   auto in_index = [&](int l, int i) -> long long { return s_in0[l] + (long long)i * B; };
   auto out_index = [&](int l, int k) -> long long { return s_out0[l] + (long long)k * B; };
+  // bounds of the data-dependent indices (checked builds only): a chain's stride in the input / output (the whole
+  // array when there is one field), the box, the data and output voxels
+  const long long in_lim = a.in_cs > 0 ? a.in_cs : 0x7fffffffffffffffLL;
+  const long long out_lim = a.out_cs > 0 ? a.out_cs : 0x7fffffffffffffffLL;
+  const long long box = (long long)v.bx * v.by * v.bz;
   auto load = [&](int l, int i) -> C {
     C val = mk((decltype(C().x))0, (decltype(C().x))0);
     if (valid(l) && i < n_in) {
       const long long idx = in_index(l, i);
       const int c = chain(l);
       if (PRO == PRO_LOAD) {
-        val = reinterpret_cast<const C*>(a.in)[(long long)c * a.in_cs + idx];
-      } else {
+        if (in_bounds(idx, in_lim, ch.err)) val = reinterpret_cast<const C*>(a.in)[(long long)c * a.in_cs + idx];
+      } else if (in_bounds(idx, box, ch.err)) {
         const int j = v.box_to_d[idx];
-        if (j >= 0) val.x = ch.gD[(long long)j * ch.Cp + c];
+        if (j >= 0 && in_bounds(j, v.n_h, ch.err)) val.x = ch.gD[(long long)j * ch.Cp + c];
       }
     }
     return val;
@@ -180,14 +185,17 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
     const int c = chain(l);
     const C val = sm[k * P + l];
     if (EPI == EPI_STORE) {
-      reinterpret_cast<C*>(a.out)[(long long)c * a.out_cs + idx] = mk(val.x * scale, val.y * scale);
-    } else {
+      if (in_bounds(idx, out_lim, ch.err))
+        reinterpret_cast<C*>(a.out)[(long long)c * a.out_cs + idx] = mk(val.x * scale, val.y * scale);
+    } else if (in_bounds(idx, box, ch.err)) {
       const int slot = l / LPC;
       const int j = v.box_to_d[idx];
-      if (j >= 0) ch.muD[((long long)s_hsel[slot] * v.n_h + j) * ch.Cp + c] = (float)(val.x * scale);
+      if (j >= 0 && in_bounds(j, v.n_h, ch.err))
+        ch.muD[((long long)s_hsel[slot] * v.n_h + j) * ch.Cp + c] = (float)(val.x * scale);
       if (s_wo[slot]) {
         const int o = v.box_to_o[idx];
-        if (o >= 0) ch.muO[((long long)s_hsel[slot] * v.n_o + o) * ch.Cp + c] = (float)(val.x * scale);
+        if (o >= 0 && in_bounds(o, v.n_o, ch.err))
+          ch.muO[((long long)s_hsel[slot] * v.n_o + o) * ch.Cp + c] = (float)(val.x * scale);
       }
     }
   };
@@ -230,6 +238,10 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
   const long long N = v.N;
   const long long lines = (long long)v.E1 * v.E2;
   const long long lam0 = (long long)blockIdx.x * TL;
+  // the block's lines of the state and of T1 lie in their arrays (checked builds)
+  if (!in_bounds(min(lam0 + TL, lines) * E0 - 1, N, ch.err) ||
+      !in_bounds(min(lam0 + TL, lines) * v.bx - 1, ch.t1_stride, ch.err))
+    return;
   const int nl = (int)min((long long)TL, lines - lam0);
   float2* Ub = ch.U + (long long)c * 2 * N;
   const float2* Usrc = Ub + (long long)(first ? acc : (acc ^ 1)) * N;
@@ -558,6 +570,10 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   const ChainState& st = ch.st[c];
   const int Lc = st.L_cur;
   if (step > Lc) return;
+  // the block's plane of the state and of T2 lie in their arrays (checked builds)
+  if (!in_bounds((long long)(z + 1) * E * E - 1, v.N, ch.err) ||
+      !in_bounds((long long)(z + 1) * v.by * v.bx - 1, ch.t2_stride, ch.err))
+    return;
   const bool first = step == 0, last = step == Lc;
   const bool fixed = (flags & XF_FIXED_MOMENTUM) != 0;
   const bool need_q = !(first && !fixed);
@@ -619,10 +635,11 @@ __host__ __device__ constexpr int csr_prefetch(int CG) { return (CG >= 2 && CG <
 // ... of [ks, ke): the batch's values and columns are loaded once, coalesced,
 // and broadcast by shuffle, so the X loads of a batch are independent and
 // stay in flight together.
+// n_cols bounds the column indices (checked builds; err receives the failure).
 template <int CG, int NR, int PF>
 __device__ __forceinline__ void csr_batches(const float* __restrict__ val, const int* __restrict__ col, int ks, int ke,
                                             int b0, int bs, const float* const (&x)[NR], int Cp, int lane,
-                                            float (&acc)[NR]) {
+                                            float (&acc)[NR], int n_cols, int* err) {
   constexpr int G = 32 / CG;
   const int grp = lane / CG;
   if constexpr (PF == 1) {
@@ -634,8 +651,9 @@ __device__ __forceinline__ void csr_batches(const float* __restrict__ val, const
       for (int j0 = 0; j0 < 32; j0 += G) {
         const int j = j0 + grp;
         const float w = __shfl_sync(0xffffffffu, mv, j);
-        const long long cidx = (long long)__shfl_sync(0xffffffffu, mc, j) * Cp;
-        if (j < n) {
+        const int cj = __shfl_sync(0xffffffffu, mc, j);
+        const long long cidx = (long long)cj * Cp;
+        if (j < n && in_bounds(cj, n_cols, err)) {
 #pragma unroll
           for (int r = 0; r < NR; r++) acc[r] = fmaf(w, x[r][cidx], acc[r]);
         }
@@ -664,8 +682,9 @@ __device__ __forceinline__ void csr_batches(const float* __restrict__ val, const
         for (int j0 = 0; j0 < 32; j0 += G) {
           const int j = j0 + grp;
           const float w = __shfl_sync(0xffffffffu, mv, j);
-          const long long cidx = (long long)__shfl_sync(0xffffffffu, mc, j) * Cp;
-          if (j < n) {
+          const int cj = __shfl_sync(0xffffffffu, mc, j);
+          const long long cidx = (long long)cj * Cp;
+          if (j < n && in_bounds(cj, n_cols, err)) {
 #pragma unroll
             for (int r = 0; r < NR; r++) acc[r] = fmaf(w, x[r][cidx], acc[r]);
           }
@@ -705,7 +724,7 @@ __global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, in
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
     // batches ahead keep the matrix stream in flight (csr_prefetch)
     csr_batches<CG, NR, csr_prefetch(CG)>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], warp, 8, x, Cp,
-                                          lane, acc);
+                                          lane, acc, v.n_h, ch.err);
     if (lane < CG) {
 #pragma unroll
       for (int r = 0; r < NR; r++) red[warp][lane + CG * r] = acc[r];
@@ -724,6 +743,60 @@ __global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, in
   if (tact) {
     const int slot = step <= 0 ? SL_RS0 : (step == ch.st[t].L_cur ? SL_RSL : SL_SCRATCH);
     ch.part[((long long)t * NSLOT + slot) * ch.maxblk + blockIdx.x] = sq;
+  }
+}
+
+// The same product with one warp per row of W (grid-stride over rows by warps), for kriging matrices with many
+// rows per block (large volumes with few chains): no block barrier per row, and every warp keeps 8 batches of its
+// row in flight.  The per-chain squared residuals are summed over the block's warps in a fixed order.
+template <int CG, int NR>
+__global__ void __launch_bounds__(256, 4) k_spmv_w_rows(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int C = ch.C, Cp = ch.Cp;
+  const int cc = lane % CG;
+  __shared__ double red[8][CG * NR];
+  bool act[NR];
+  double sq[NR];
+  const float* x[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int c = cc + CG * r;
+    const int cs = min(c, C - 1);
+    x[r] = ch.muD + (long long)(ch.st[cs].acc ^ sel) * v.n_h * Cp + cs;
+    act[r] = false;
+    sq[r] = 0.0;
+    if (c < C && (chain_only < 0 || c == chain_only)) act[r] = step < 0 || step <= ch.st[c].L_cur;
+  }
+  for (int row = blockIdx.x * 8 + warp; row < v.n_s; row += gridDim.x * 8) {
+    float acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = 0.f;
+    csr_batches<CG, NR, 8>(v.w_val, v.w_col, v.w_rowptr[row], v.w_rowptr[row + 1], 0, 1, x, Cp, lane, acc, v.n_h,
+                           ch.err);
+    if (lane < CG) {
+      const float ys = v.Ys[row];
+#pragma unroll
+      for (int r = 0; r < NR; r++) {
+        if (!act[r]) continue;
+        const float rsv = ys - acc[r];
+        ch.rs[(long long)row * Cp + cc + CG * r] = rsv;
+        sq[r] += (double)rsv * rsv;
+      }
+    }
+  }
+  if (lane < CG) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) red[warp][lane + CG * r] = sq[r];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    if (chain_only >= 0 && c != chain_only) continue;
+    const ChainState& st = ch.st[c];
+    if (step >= 0 && step > st.L_cur) continue;
+    double t = 0.0;
+    for (int w = 0; w < 8; w++) t += red[w][c];
+    const int slot = step <= 0 ? SL_RS0 : (step == st.L_cur ? SL_RSL : SL_SCRATCH);
+    ch.part[((long long)c * NSLOT + slot) * ch.maxblk + blockIdx.x] = t;
   }
 }
 
@@ -764,7 +837,8 @@ __global__ void __launch_bounds__(256, 4) k_spmv_wt(DevVolume v, DevChains ch, i
     for (int r = 0; r < NR; r++) acc[r] = 0.f;
     if (v.n_s > 0)
       csr_batches<CG, NR, csr_prefetch(CG) < 2 ? 2 : csr_prefetch(CG)>(v.wt_val, v.wt_col, v.wt_rowptr[row],
-                                                                       v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc);
+                                                                       v.wt_rowptr[row + 1], 0, 1, x, Cp, lane, acc,
+                                                                       v.n_s, ch.err);
     if (lane < CG) {
       const float yh = v.Yh[row];
 #pragma unroll
@@ -1004,9 +1078,11 @@ __global__ void k_spectrum(const double2* lam, float* sinv, double* lam_re, long
 }
 
 // ----------------------------------------------------------------- evaluation helpers
-__global__ void k_gather_re(const float2* field, const int* idx, int n, float* out, int pitch, int col) {
+// Re field[idx[j]] for j < n; N bounds the indices (checked builds, failures to err).
+__global__ void k_gather_re(const float2* field, const int* idx, int n, float* out, int pitch, int col, long long N,
+                            int* err) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) out[(long long)j * pitch + col] = field[idx[j]].x;
+  if (j < n && in_bounds(idx[j], N, err)) out[(long long)j * pitch + col] = field[idx[j]].x;
 }
 
 // Block partials of sum_live |u|^2 * sinv  (mode 0) or sum_live |u|^2 / (sinv + sh)  (mode 1).

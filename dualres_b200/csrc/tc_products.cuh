@@ -282,10 +282,10 @@ __global__ void __launch_bounds__(tc_threads(N), 1)
             const long long o = xoff[n];
             const int4 j = __ldg(cols + kc4);
             const bool on = o >= 0;
-            xv[i][0] = (on && j.x >= 0) ? __ldg(X + o + j.x * Cp) : 0.f;
-            xv[i][1] = (on && j.y >= 0) ? __ldg(X + o + j.y * Cp) : 0.f;
-            xv[i][2] = (on && j.z >= 0) ? __ldg(X + o + j.z * Cp) : 0.f;
-            xv[i][3] = (on && j.w >= 0) ? __ldg(X + o + j.w * Cp) : 0.f;
+            xv[i][0] = (on && j.x >= 0 && in_bounds(j.x, A.n_cols, ch.err)) ? __ldg(X + o + j.x * Cp) : 0.f;
+            xv[i][1] = (on && j.y >= 0 && in_bounds(j.y, A.n_cols, ch.err)) ? __ldg(X + o + j.y * Cp) : 0.f;
+            xv[i][2] = (on && j.z >= 0 && in_bounds(j.z, A.n_cols, ch.err)) ? __ldg(X + o + j.z * Cp) : 0.f;
+            xv[i][3] = (on && j.w >= 0 && in_bounds(j.w, A.n_cols, ch.err)) ? __ldg(X + o + j.w * Cp) : 0.f;
           }
           // A: hi in place, lo into the second block, while the loads above are in flight
           if (!mbar_wait_bounded(fullA + s, (q / stages) & 1)) {
@@ -364,7 +364,10 @@ __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* _
   __shared__ int rows[TC_FR];
   const int t = blockIdx.x / (TC_M / TC_FR), m0 = (blockIdx.x % (TC_M / TC_FR)) * TC_FR;
   const int s0 = A.tile_seg_ptr[t], s1 = A.tile_seg_ptr[t + 1];
-  if (threadIdx.x < TC_FR) rows[threadIdx.x] = A.tile_rows[(long long)t * TC_M + m0 + threadIdx.x];
+  if (threadIdx.x < TC_FR) {
+    const int row = A.tile_rows[(long long)t * TC_M + m0 + threadIdx.x];
+    rows[threadIdx.x] = (row < 0 || in_bounds(row, A.n_rows, ch.err)) ? row : -1;
+  }
   {
     // element i of this thread: row m0 + mi, chain nb + 16 i (rows fastest across the warp); the segments are
     // summed in order, four segments' loads in flight at a time

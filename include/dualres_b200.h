@@ -172,6 +172,10 @@ void dr_chainset_destroy(dr_chainset* cs);
  * path, DRB_TC_PRODUCTS=0 / 1 the products.  Any output may be NULL. */
 int dr_chainset_config_get(const dr_chainset* cs, int* path, int* blocks_per_sm, double* tuned_ms,
                            int* tensor_products);
+/* The tile shape of the chain set's z passes, chosen by the same tuning (DRB_ZTILE=1 / 8 forces it): chains per tile,
+ * 8 for tiles of 4 lines x 8 chains, 1 for tiles of 32 lines of one chain (always 1 below 8 chains).  No reference
+ * counterpart: the reference's FFTW plans have no tiles. */
+int dr_chainset_ztile_get(const dr_chainset* cs, int* z_tile_chains);
 
 /* ---- fixed-input evaluation (MultiResParameters public API) ------------- */
 /* Sets chain `chain` to mu (2N floats) and sigma^-2 = (s_hr, s_sr). */

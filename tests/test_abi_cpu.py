@@ -35,6 +35,20 @@ def test_library_reports_version():
     assert b"sm_100a" in d.lib().dr_version()
 
 
+def test_bounds_checked_library_loads_and_exports_the_same_symbols():
+    """The checked build (DRB_BOUNDS_CHECK: every data-dependent index tested before its access, a failure recorded
+    and the access skipped) is a second library with the same entry points, selected by DRB_LIBRARY=checked."""
+    import ctypes
+
+    from dualres_b200 import build as b
+    b.build(checked=True)
+    L = ctypes.CDLL(b.LIB_CHECKED)
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+    L.dr_version.restype = ctypes.c_char_p
+    assert b"bounds-checked" in L.dr_version()
+
+
 @pytest.mark.parametrize("name", golden_cases())
 def test_host_kriging_matches_oracle(oracle, name):
     import dualres_b200 as d

@@ -42,8 +42,32 @@ def test_switches(monkeypatch):
     monkeypatch.delenv("DRB_PLANE_PREFETCH", raising=False)
     data, a = _chains(vol, 2, 5)
     assert a.config() == {"path": "plane", "blocks_per_sm": 8, "tuned_ms": 0.0, "tensor_products": False,
-                          "tma_row_gather": False}
+                          "tma_row_gather": False, "z_tile_chains": 1}
     monkeypatch.setenv("DRB_NO_PLANE", "1")
     b = d.MultiResParameters(data, d.HMCParameters(burnin=4, nsave=3, thin=1, leapfrog=5, seed=2), 2)
     assert b.config()["path"] == "lines"
     a.close(), b.close(), data.close()
+
+
+def test_tuner_chooses_the_z_tile_shape(monkeypatch):
+    """With 8 or more chains the tuner also times the z passes' tile shape (4 lines x 8 chains against 32 lines of
+    one chain); DRB_ZTILE forces either, and both give the same gradient bit for bit (the tile only changes which
+    lines a block transforms)."""
+    for k in ("DRB_AUTOTUNE", "DRB_NO_PLANE", "DRB_PLANE_PREFETCH", "DRB_ZTILE"):
+        monkeypatch.delenv(k, raising=False)
+    vol = synth.small_volume(seed=53, dims=(12, 12, 10))
+    data, a = _chains(vol, 8, 5)
+    assert a.config()["z_tile_chains"] in (1, 8)
+    monkeypatch.setenv("DRB_AUTOTUNE", "0")
+    rng = np.random.default_rng(4)
+    mu = ((rng.standard_normal(data.shape) + 1j * rng.standard_normal(data.shape)) * 0.3).astype(np.complex64)
+    grads = {}
+    for zt in ("8", "1"):
+        monkeypatch.setenv("DRB_ZTILE", zt)
+        ch = d.MultiResParameters(data, d.HMCParameters(burnin=4, nsave=3, thin=1, leapfrog=5, seed=2), 8)
+        assert ch.config()["z_tile_chains"] == int(zt)
+        ch.set_state(6, mu, (1.5, 3.0))
+        grads[zt] = ch.gradient(6, mu)
+        ch.close()
+    assert np.array_equal(grads["8"].view(np.uint32), grads["1"].view(np.uint32))
+    a.close(), data.close()
