@@ -8,10 +8,12 @@ MultiResParameters::update + HMCParameters::update per chain).  Metric: HMC
 gradient evaluations per second (sum over chains of L + 1 per iteration).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload batched64|single_c1|single_c2|served|served_c1] [--no-ess]
+                    [--workload batched64|single_c1|single_c2|served|served_c1|served_c3] [--no-ess]
 
 Served workloads ("served": the C4 size/parameter distribution; "served_c1":
-fixed C1-size jobs): --steps jobs arrive as a Poisson process (20 jobs/s) at
+one-chain fits of 32^3 images; "served_c3": fits of the batched size, 64
+chains on each request's own 32^3 image): --steps jobs arrive as a Poisson
+process (20 jobs/s) at
 a continuous-batching server; after --warmup untimed jobs, the line reports
 fits completed per second, gradient evaluations per second over the makespan,
 and p50/p99 job latency (submission to result on the host).
@@ -121,6 +123,8 @@ WORKLOADS = {
     # served streams: a step is one job; jobs arrive as a Poisson process
     "served": dict(chains=1, vol="c4", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
     "served_c1": dict(chains=1, vol="c1", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
+    # jobs of the batched size: 64 chains on each request's own 32^3 image (one fit of the batched configuration)
+    "served_c3": dict(chains=64, vol="c1", burnin=300, nsave=300, thin=3, leapfrog=25, rate=20.0),
     "served_tiny": dict(chains=1, vol="small", burnin=20, nsave=20, thin=1, leapfrog=5, rate=50.0),  # test-sized
     # config 4: 32 volumes of the uneven size/parameter distribution fitted together (all submitted at once)
     "uneven32": dict(chains=1, vol="c4", burnin=300, nsave=300, thin=3, leapfrog=25, rate=float("inf"), jobs=32),
@@ -351,6 +355,13 @@ def run_ours(args, dist):
             extra["served_c1"] = srv
         except Exception as e:  # an extra must not break the benchmark line
             extra["served_c1"] = {"error": str(e)[:200]}
+        try:  # three fits of the batched size (64 chains each) arriving together; tuning is cached from above
+            srv = served_sample("served_c3", 3, 0, args.seed + 13, dev)
+            srv["over_plain_gpu"] = srv["value"] / extra["plain_gpu_single_chain"]["value"] \
+                if "value" in extra.get("plain_gpu_single_chain", {}) else None
+            extra["served_c3"] = srv
+        except Exception as e:  # an extra must not break the benchmark line
+            extra["served_c3"] = {"error": str(e)[:200]}
 
     # ---- roofline of the dominant kernel (timed live with CUDA events on the library stream)
     per_iter = {}
@@ -636,9 +647,10 @@ def served_sample(workload, jobs, warmup_jobs, seed, device, rate=None):
     return {"workload": workload, "jobs": jobs, "arrival_rate_per_s": rate, "value": grads / makespan, "unit": UNIT,
             "fits_per_s": jobs / makespan, "makespan_s": makespan,
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-            "what": "a dualgpmf fit per job (one chain, burnin %d, nsave %d, thin %d, L %d) through dr_server_*; "
+            "what": "a dualgpmf fit per job (%d chain%s, burnin %d, nsave %d, thin %d, L %d) through dr_server_*; "
                     "gradient evaluations over the makespan from the first arrival to the last result"
-                    % (wl["burnin"], wl["nsave"], wl["thin"], wl["leapfrog"])}
+                    % (wl["chains"], "" if wl["chains"] == 1 else "s", wl["burnin"], wl["nsave"], wl["thin"],
+                       wl["leapfrog"])}
 
 
 def reference_bytes_per_step(N, nnz, chains, n_h, n_s):
@@ -723,6 +735,65 @@ def cpu_throughput(vol, W, L, cores, target_s=10.0):
                       f"{dt:.1f} s wall"}
 
 
+def posterior_mean_vs_fp64(vol, iters=12, L=25, eps=0.05, seed=1):
+    """The FP32 sampler kernels against the FP64 oracle on identical draws (one chain on `vol`, sigma fixed at
+    4 / 11): per iteration the same 2N standard normals become the momentum (MultiResParameters.h:784-815) and the
+    same uniform decides the accept (MultiResParameters.h:680-705); the device runs the trajectory through its own
+    leapfrog kernels (dr_leapfrog_fixed), the oracle through its FP64 transition (four FFTs per step,
+    MultiResParameters.h:674-727).  Returns the norm-wise relative error of the running mean and variance of Re mu
+    over the output voxels after `iters` iterations, and how many accept decisions differed."""
+    import dualres_b200 as d
+    from oracle import oracle as o
+    o.set_threads(os.cpu_count() or 1)
+    data = d.MultiResData.from_volume(vol)
+    ch = d.MultiResParameters(data, d.HMCParameters(burnin=2, nsave=2, thin=1, leapfrog=L, seed=seed), 1)
+    prep = o.prepare(vol.highres)
+    rp, col, val = data.W()
+    _, ys = data.data()
+    md = o.Model(prep["D"], prep["Yh"], vol.qform_hr, vol.theta, ys, (rp, col, val.astype(np.float64)), prep["O"],
+                 precision="d")
+    sh, ss = 4.0, 11.0
+    md.set_sigma(sh, ss)
+    E = md.E
+    flat = lambda ijk: (ijk[:, 2] * E[0] * E[1] + ijk[:, 1] * E[0] + ijk[:, 0])  # noqa: E731
+    mu = np.zeros(md.shape, np.complex64)
+    mu.ravel()[flat(np.asarray(prep["D"]).reshape(-1, 3))] = prep["Yh"]
+    md.set_mu(mu)
+    ch.set_state(0, mu, (sh, ss))
+    oi = flat(np.asarray(prep["O"]).reshape(-1, 3))
+    rng = np.random.default_rng(seed)
+    s64, q64, s32, q32 = (np.zeros(len(oi)) for _ in range(4))
+    flips = acc = 0
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        z = rng.standard_normal(2 * md.N).astype(np.float32)
+        u = float(rng.random())
+        p, e0z = md.momentum(z)
+        _, out, _ = md.transition(z, u, eps, L)
+        muL, _, en = ch.leapfrog(0, mu, p.astype(np.complex64), eps, L)
+        log_r = (en[3] + en[4] + en[5]) - (e0z + en[0] + en[1])
+        a32 = bool(np.log(u) < log_r)
+        mu = muL if a32 else mu
+        flips += int(a32 != bool(out[1]))
+        acc += int(out[1])
+        x64, x32 = md.get_mu().ravel()[oi].real.astype(np.float64), mu.ravel()[oi].real.astype(np.float64)
+        s64 += x64
+        q64 += x64 * x64
+        s32 += x32
+        q32 += x32 * x32
+    dt = time.perf_counter() - t0
+    ch.close()
+    data.close()
+    m64, m32 = s64 / iters, s32 / iters
+    v64, v32 = q64 / iters - m64 * m64, q32 / iters - m32 * m32
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    return {"rel_mean": rel(m32, m64), "rel_var": rel(v32, v64), "iterations": iters, "leapfrog": L, "eps": eps,
+            "accept_flips": flips, "accept_rate": acc / iters, "seconds": dt,
+            "what": "FP32 sampler kernels (dr_leapfrog_fixed) vs the FP64 oracle on identical draws, one chain on the "
+                    "benchmark volume, sigma fixed; norm-wise relative error of the running posterior mean and "
+                    "variance of Re mu over the output voxels"}
+
+
 def cpu_baseline_line(vol, W, L, target_s=12.0):
     threads = os.cpu_count() or 1
     m, _ = oracle_model(vol, W)
@@ -737,6 +808,10 @@ def cpu_baseline_line(vol, W, L, target_s=12.0):
         line["throughput"] = cpu_throughput(vol, W, L, threads)
     except Exception as e:  # an extra must not break the benchmark line
         line["throughput"] = {"error": str(e)[:200]}
+    try:  # the oracle as the checker of the device's numerics on this volume
+        line["posterior_mean_vs_fp64"] = posterior_mean_vs_fp64(vol)
+    except Exception as e:  # an extra must not break the benchmark line
+        line["posterior_mean_vs_fp64"] = {"error": str(e)[:200]}
     return line
 
 
