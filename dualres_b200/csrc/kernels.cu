@@ -164,7 +164,23 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
     }
     return val;
   };
-  if (B == 1) {
+  // every load of a thread is issued before the first shared-memory store: PER independent loads in flight (tiles
+  // of a whole number of block-widths, up to 16 per thread)
+  constexpr int PER = TL * N / NT;
+  if constexpr (PER >= 1 && PER <= 16 && PER * NT == TL * N) {
+    C r[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int e = threadIdx.x + k * NT;
+      r[k] = B == 1 ? load(e / N, e % N) : load(e % TL, e / TL);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int e = threadIdx.x + k * NT;
+      if (B == 1) sm[(e % N) * P + e / N] = r[k];
+      else sm[(e / TL) * P + e % TL] = r[k];
+    }
+  } else if (B == 1) {
     for (int e = threadIdx.x; e < TL * N; e += NT) {
       const int l = e / N, i = e % N;
       sm[i * P + l] = load(l, i);
