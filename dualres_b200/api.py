@@ -158,6 +158,7 @@ def _declare(L):
     L.dr_debug_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
     L.dr_debug_tc_layout.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp]
     L.dr_debug_bounded_wait.argtypes = [C.c_int, C.c_double, _ip, _dp]
+    L.dr_debug_pool_usage.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
     L.dr_free.restype = None
@@ -485,6 +486,13 @@ def time_kernel(chains, which, step=1, reps=20):
     b = np.zeros(1, np.float64)
     check(lib().dr_debug_time_kernel(chains.h, which, step, reps, _ptr(ms), _ptr(b)))
     return float(ms[0]), float(b[0])
+
+
+def pool_usage(device=0, reset_high=False):
+    """(bytes in use, high-water mark) of the library's device memory pool (dr_debug_pool_usage)."""
+    u, h = C.c_uint64(0), C.c_uint64(0)
+    check(lib().dr_debug_pool_usage(device, 1 if reset_high else 0, C.byref(u), C.byref(h)))
+    return int(u.value), int(h.value)
 
 
 def bounded_wait(limit_ms=200.0, device=0):

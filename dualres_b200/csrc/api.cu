@@ -8,6 +8,7 @@
 #include <condition_variable>
 #include <deque>
 #include <map>
+#include <unordered_map>
 #include <memory>
 #include <thread>
 #include <cmath>
@@ -69,9 +70,45 @@ struct NvtxRange {
   NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
+// DRB_TRACE=1: the set-up phases (volume preparation, kriging, tile plans, tuning candidates) print their host
+// wall time to stderr when their scope ends.
+static bool trace_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("DRB_TRACE");
+    return e && *e && std::string(e) != "0";
+  }();
+  return on;
+}
+struct TraceScope {
+  std::string name;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit TraceScope(std::string n) : name(std::move(n)) {}
+  // ends the current phase and starts the next one
+  void next(std::string n) {
+    print();
+    name = std::move(n);
+    t0 = std::chrono::steady_clock::now();
+  }
+  ~TraceScope() { print(); }
+  TraceScope(const TraceScope&) = delete;
+  TraceScope& operator=(const TraceScope&) = delete;
+
+ private:
+  void print() const {
+    if (trace_on())
+      std::fprintf(stderr, "[drb] %s: %.2f ms\n", name.c_str(),
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+};
+
 // ---------------------------------------------------------------- per-device set-up
 struct DeviceTables {
   bool ready = false;
+  // The library's stream-ordered allocations come from one memory pool per device that keeps freed memory (release
+  // threshold unlimited): a volume's kriging scratch, the tuner's candidate chain sets and a chain set's arrays
+  // reuse one another's memory instead of growing and shrinking a pool around every set-up.  The process's default
+  // pool is left as it is.
+  cudaMemPool_t pool = nullptr;
   int sms = 148;
   int tma_dyn_max = 0;  // dynamic shared memory available to the bulk-copy plane kernel
   bool tc = false;      // the tensor-core kriging products fit this device's shared memory
@@ -115,6 +152,15 @@ static DeviceTables& device_tables(int dev) {
   DeviceTables& t = g_dev[dev];
   if (t.ready) return t;
   CK(cudaSetDevice(dev));
+  {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    CK(cudaMemPoolCreate(&t.pool, &props));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(t.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   std::vector<float2> hf(TW_TOTAL);
   std::vector<double2> hd(TW_TOTAL);
   for (int N = 2; N <= 512; N <<= 1)
@@ -145,8 +191,6 @@ static DeviceTables& device_tables(int dev) {
     set_plane_attr<16, true>(t.tma_dyn_max); set_plane_attr<32, true>(t.tma_dyn_max);
     set_plane_attr<64, true>(t.tma_dyn_max);
     CK(cudaFuncSetAttribute(k_kriging_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
-    CK(cudaFuncSetAttribute(k_spd_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
-    CK(cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KrigSmem)));
     int smax = 0;
     for (int n = 16; n <= 256; n *= 2) smax = std::max(smax, tc_smem_bytes(n));
     t.tc = optin >= smax;
@@ -165,6 +209,14 @@ static DeviceTables& device_tables(int dev) {
   }
   t.ready = true;
   return t;
+}
+
+// Stream-ordered allocation on the current device from the library's pool.
+static cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, bytes, device_tables(dev).pool, st);
 }
 
 // ---------------------------------------------------------------- pass launcher
@@ -276,14 +328,14 @@ struct Volume {
   T* alloc(size_t n) {
     void* p = nullptr;
     if (n == 0) n = 1;
-    const cudaError_t e = cudaMallocAsync(&p, n * sizeof(T), stream);
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    const cudaError_t e = dev_alloc(&p, n * sizeof(T), stream);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     allocs.push_back(p);
     bytes += (int64_t)(n * sizeof(T));
     return (T*)p;
   }
-  template <class T>
-  T* upload(const std::vector<T>& h) {
+  template <class T, class A>
+  T* upload(const std::vector<T, A>& h) {
     T* d = alloc<T>(h.size());
     if (!h.empty()) CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     return d;
@@ -307,120 +359,142 @@ static std::mutex g_vol_mtx;
 // the host builder (QR).
 static bool device_kriging_enabled() { return std::getenv("DRB_HOST_KRIGING") == nullptr; }
 
-// K^-1 of a kriging plan on the device (one block factors K, then all blocks
-// solve for the rows of K^-1); leaves P.S empty when K is not positive definite.
-static void device_spd_inverse(KrigingPlan& P, int device, cudaStream_t st) {
-  const int m = P.m;
-  DeviceTables& dt = device_tables(device);
-  CK(cudaSetDevice(device));
-  const int grid = std::max(1, std::min(m, 2 * dt.sms));
-  std::vector<void*> bufs;
-  auto dalloc = [&](size_t bytes) {
-    void* p = nullptr;
-    const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync (K^-1): ") + cudaGetErrorString(e));
-    bufs.push_back(p);
-    return p;
-  };
-  try {
-    double* dM = (double*)dalloc(sizeof(double) * (size_t)m * m);
-    double* dS = (double*)dalloc(sizeof(double) * (size_t)m * m);
-    double* dB = (double*)dalloc(sizeof(double) * (size_t)m * grid);
-    int* dok = (int*)dalloc(sizeof(int));
-    CK(cudaMemcpyAsync(dM, P.K.data(), sizeof(double) * (size_t)m * m, cudaMemcpyHostToDevice, st));
-    k_spd_factor<<<1, KR_NT, sizeof(KrigSmem), st>>>(dM, m, dok);
+// S = K^-1 on the device by the blocked kernels of kriging.cuh (factor, triangular inverse, Gram product), all
+// CTAs of the GPU taking part; dK (m x m) is left unchanged and dS receives S.  Returns false when K is not
+// positive definite.  Scratch comes from dalloc.
+template <class Alloc>
+static bool device_spd_inverse(const double* dK, int m, double* dS, cudaStream_t st, Alloc&& dalloc) {
+  const int nb = (m + KR_NB - 1) / KR_NB;
+  double* dM = (double*)dalloc(sizeof(double) * (size_t)m * m);
+  double* dX = (double*)dalloc(sizeof(double) * (size_t)m * m);
+  double* dDinv = (double*)dalloc(sizeof(double) * (size_t)nb * KR_NB * KR_NB);
+  int* dok = (int*)dalloc(sizeof(int));
+  static const int one = 1;
+  CK(cudaMemcpyAsync(dM, dK, sizeof(double) * (size_t)m * m, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(dok, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+  TraceScope tr("K^-1: factor (" + std::to_string(nb) + " panels)");
+  for (int k0 = 0; k0 < m; k0 += KR_NB) {
+    k_chol_diag<<<1, KR_NT, 0, st>>>(dM, m, k0, dDinv, dok);
     CK_LAUNCH();
-    int ok = 0;
-    CK(cudaMemcpyAsync(&ok, dok, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (ok) {
-      k_spd_inverse<<<grid, KR_NT, sizeof(KrigSmem), st>>>(dM, m, dS, dB);
-      CK_LAUNCH();
-      k_symmetrize<<<cdiv_i((long long)m * m, 256), 256, 0, st>>>(dS, m);
-      CK_LAUNCH();
-      P.S.resize((size_t)m * m);
-      CK(cudaMemcpyAsync(P.S.data(), dS, sizeof(double) * (size_t)m * m, cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-    }
-  } catch (...) {
-    for (void* p : bufs) cudaFreeAsync(p, st);
-    cudaStreamSynchronize(st);
-    cudaGetLastError();
-    throw;
+    const int r0 = std::min(m, k0 + KR_NB);
+    if (r0 >= m) break;
+    const int T = cdiv_i(m - r0, KR_TILE);
+    k_chol_panel<<<T, KR_NT, 0, st>>>(dM, m, k0, dDinv, dok);
+    CK_LAUNCH();
+    k_chol_update<<<T * (T + 1) / 2, KR_NT, 0, st>>>(dM, m, k0, dok);
+    CK_LAUNCH();
   }
-  for (void* p : bufs) cudaFreeAsync(p, st);
+  int ok = 0;
+  CK(cudaMemcpyAsync(&ok, dok, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (!ok) return false;
+  tr.next("K^-1: triangular inverse + Gram product");
+  for (int bi = 0; bi < nb; bi++) {
+    k_trinv_row<<<bi + 1, KR_NT, 0, st>>>(dM, m, bi, dDinv, dX, dok);
+    CK_LAUNCH();
+  }
+  k_trinv_gram<<<nb * (nb + 1) / 2, KR_NT, 0, st>>>(dX, m, dS, dok);
+  CK_LAUNCH();
+  if (trace_on()) CK(cudaStreamSynchronize(st));
+  return true;
 }
 
 static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
   const auto t0 = std::chrono::steady_clock::now();
-  if (hv.kplan.S.empty() && hv.kplan.inverse_wanted && hv.kplan.m > 0) device_spd_inverse(hv.kplan, device, st);
-  const KrigingPlan& P = hv.kplan;
+  KrigingPlan& P = hv.kplan;
   const int m = P.m, nrows = P.nrows;
-  const bool have_inv = !P.S.empty();
-  std::vector<double> w(P.col.size(), 0.0);
+  CK(cudaSetDevice(device));
+  DeviceTables& dt = device_tables(device);
+  std::vector<void*> bufs;
+  auto dalloc = [&](size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = dev_alloc(&p, std::max<size_t>(bytes, 16), st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("device allocation (kriging): ") + cudaGetErrorString(e));
+    bufs.push_back(p);
+    return p;
+  };
+  auto upload = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  };
+  fill_vector<double> w(P.col.size());  // every entry comes back from the device (zeroed there)
   std::vector<char> keep(nrows, 1);
-  // tasks: every row with neighbours; complete rows with equal k' are solved once
-  std::map<std::vector<double>, int> rep;
-  std::vector<int> dup_of(nrows, -1);
-  std::vector<std::pair<double, int>> order;
-  std::vector<int> route(nrows, 0);
-  int nmax = 1;
-  for (int ri = 0; ri < nrows; ri++) {
-    const int r0 = P.row_start[ri], cnt = P.row_start[ri + 1] - r0;
-    if (cnt == 0) continue;
-    if (cnt == m) {
-      std::vector<double> key(P.kp.begin() + r0, P.kp.begin() + r0 + cnt);
-      auto it = rep.find(key);
-      if (it != rep.end()) {
-        dup_of[ri] = it->second;
-        continue;
-      }
-      rep.emplace(std::move(key), ri);
-    }
-    const bool schur = kriging_schur_route(cnt, m, have_inv);
-    route[ri] = schur ? KR_ROUTE_SCHUR : KR_ROUTE_DIRECT;
-    const int n = schur ? m - cnt : cnt;
-    nmax = std::max(nmax, n);
-    const double cost = (double)n * n * n / 3.0 + (schur ? 2.0 * m * cnt : 0.0);
-    order.emplace_back(-cost, ri);
-  }
-  std::sort(order.begin(), order.end());
-  const int ntasks = (int)order.size();
-  std::vector<int> task_row(std::max(ntasks, 1)), task_route(std::max(ntasks, 1));
-  for (int t = 0; t < ntasks; t++) {
-    task_row[t] = order[t].second;
-    task_route[t] = route[order[t].second];
-  }
   std::vector<int> status(nrows, KR_OK);
-  if (ntasks > 0) {
-    DeviceTables& dt = device_tables(device);
-    CK(cudaSetDevice(device));
-    const size_t slot = (size_t)nmax * nmax + m + nmax + (m + 1) / 2 + 1;
-    int grid = std::min(ntasks, 2 * dt.sms);
-    const size_t budget = (size_t)2 << 30;  // scratch cap
-    grid = std::max(1, std::min(grid, (int)(budget / (slot * sizeof(double)))));
-    std::vector<void*> bufs;
-    auto dalloc = [&](size_t bytes) {
-      void* p = nullptr;
-      const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
-      if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync (kriging): ") + cudaGetErrorString(e));
-      bufs.push_back(p);
-      return p;
-    };
-    auto upload = [&](void* dst, const void* src, size_t bytes) {
-      if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
-    };
-    try {
+  std::vector<int> dup_of(nrows, -1);
+  int ntasks = 0;
+  bool have_inv = false;
+  try {
+    double* dK = (double*)dalloc(sizeof(double) * (size_t)m * m);
+    upload(dK, P.K.data(), sizeof(double) * (size_t)m * m);
+    double* dS = nullptr;
+    if (!P.S.empty()) {  // computed on the host
+      dS = (double*)dalloc(sizeof(double) * (size_t)m * m);
+      upload(dS, P.S.data(), sizeof(double) * (size_t)m * m);
+      have_inv = true;
+    } else if (P.inverse_wanted && m > 0) {
+      const TraceScope tr("kriging: K^-1 (m = " + std::to_string(m) + ")");
+      dS = (double*)dalloc(sizeof(double) * (size_t)m * m);
+      have_inv = device_spd_inverse(dK, m, dS, st, dalloc);
+    }
+    TraceScope tr_rows("kriging: row tasks");
+    // tasks: every row with neighbours; complete rows with equal k' are solved once (grouped by a hash of k', then
+    // compared in place)
+    std::vector<uint64_t> kh(nrows, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int ri = 0; ri < nrows; ri++) {
+      const int r0 = P.row_start[ri], cnt = P.row_start[ri + 1] - r0;
+      if (cnt != m) continue;
+      uint64_t h = 1469598103934665603ull;  // FNV-1a over the bytes of k'
+      const unsigned char* b = reinterpret_cast<const unsigned char*>(P.kp.data() + r0);
+      for (size_t i = 0; i < (size_t)cnt * sizeof(double); i++) h = (h ^ b[i]) * 1099511628211ull;
+      kh[ri] = h;
+    }
+    std::unordered_map<uint64_t, std::vector<int>> rep;
+    std::vector<std::pair<double, int>> order;
+    std::vector<int> route(nrows, 0);
+    int nmax = 1;
+    for (int ri = 0; ri < nrows; ri++) {
+      const int r0 = P.row_start[ri], cnt = P.row_start[ri + 1] - r0;
+      if (cnt == 0) continue;
+      if (cnt == m) {
+        std::vector<int>& reps = rep[kh[ri]];
+        int found = -1;
+        for (int o : reps)
+          if (std::memcmp(P.kp.data() + P.row_start[o], P.kp.data() + r0, sizeof(double) * (size_t)cnt) == 0) {
+            found = o;
+            break;
+          }
+        if (found >= 0) {
+          dup_of[ri] = found;
+          continue;
+        }
+        reps.push_back(ri);
+      }
+      const bool schur = kriging_schur_route(cnt, m, have_inv);
+      route[ri] = schur ? KR_ROUTE_SCHUR : KR_ROUTE_DIRECT;
+      const int n = schur ? m - cnt : cnt;
+      nmax = std::max(nmax, n);
+      const double cost = (double)n * n * n / 3.0 + (schur ? 2.0 * m * cnt : 0.0);
+      order.emplace_back(-cost, ri);
+    }
+    std::sort(order.begin(), order.end());
+    ntasks = (int)order.size();
+    std::vector<int> task_row(std::max(ntasks, 1)), task_route(std::max(ntasks, 1));
+    for (int t = 0; t < ntasks; t++) {
+      task_row[t] = order[t].second;
+      task_route[t] = route[order[t].second];
+    }
+    if (ntasks > 0) {
+      const size_t slot = (size_t)nmax * nmax + m + nmax + (m + 1) / 2 + 1;
+      int grid = std::min(ntasks, 2 * dt.sms);
+      const size_t budget = (size_t)2 << 30;  // scratch cap
+      grid = std::max(1, std::min(grid, (int)(budget / (slot * sizeof(double)))));
+      tr_rows.next("kriging: scratch + uploads (" + std::to_string(ntasks) + " tasks, n <= " + std::to_string(nmax) +
+                   ", " + std::to_string(grid) + " blocks, " + std::to_string(slot * grid * sizeof(double) >> 20) +
+                   " MiB scratch)");
       KrigArgs a{};
       a.m = m;
-      double* dK = (double*)dalloc(sizeof(double) * (size_t)m * m);
-      upload(dK, P.K.data(), sizeof(double) * (size_t)m * m);
       a.K = dK;
-      if (have_inv) {
-        double* dS = (double*)dalloc(sizeof(double) * (size_t)m * m);
-        upload(dS, P.S.data(), sizeof(double) * (size_t)m * m);
-        a.S = dS;
-      }
+      a.S = dS;
       int* d_rs = (int*)dalloc(sizeof(int) * (nrows + 1));
       upload(d_rs, P.row_start.data(), sizeof(int) * (nrows + 1));
       int* d_pid = (int*)dalloc(sizeof(int) * P.pid.size());
@@ -450,20 +524,33 @@ static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
       a.scratch = d_scr;
       a.slot = slot;
       a.nmax = nmax;
+      if (trace_on()) {
+        CK(cudaStreamSynchronize(st));
+        tr_rows.next("kriging: row-solve kernel + download");
+      }
       k_kriging_rows<<<grid, KR_NT, sizeof(KrigSmem), st>>>(a);
       CK_LAUNCH();
       CK(cudaMemcpyAsync(w.data(), d_w, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, st));
       CK(cudaMemcpyAsync(status.data(), d_status, sizeof(int) * nrows, cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
-    } catch (...) {
-      for (void* p : bufs) cudaFreeAsync(p, st);
-      cudaStreamSynchronize(st);
-      cudaGetLastError();
-      throw;
     }
+    // the host route of rows the device could not factor reads K^-1 when it chooses the Schur route
+    bool any_redo = false;
+    for (int ri = 0; ri < nrows; ri++) any_redo |= dup_of[ri] < 0 && status[ri] == KR_NOT_SPD;
+    if (any_redo && have_inv && P.S.empty()) {
+      P.S.resize((size_t)m * m);
+      CK(cudaMemcpyAsync(P.S.data(), dS, sizeof(double) * (size_t)m * m, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+  } catch (...) {
     for (void* p : bufs) cudaFreeAsync(p, st);
-    CK(cudaStreamSynchronize(st));
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    throw;
   }
+  for (void* p : bufs) cudaFreeAsync(p, st);
+  CK(cudaStreamSynchronize(st));
+  const TraceScope tr_host("kriging: host rows, assemble, transpose");
   // rows the device could not factor: host route (Cholesky / QR)
   std::vector<int> redo;
   for (int ri = 0; ri < nrows; ri++) {
@@ -484,7 +571,7 @@ static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
     keep[ri] = keep[src];
     std::copy(w.begin() + P.row_start[src], w.begin() + P.row_start[src + 1], w.begin() + P.row_start[ri]);
   }
-  kriging_assemble(P, w, keep, &hv.w_rowptr, &hv.w_col, &hv.w_val);
+  kriging_assemble(P, w.data(), keep, &hv.w_rowptr, &hv.w_col, &hv.w_val);
   hv.kplan = KrigingPlan();
   hv.kriging_pending = false;
   hv.kriging_device_rows = ntasks;
@@ -507,6 +594,7 @@ static void volume_build_device(Volume* V, const float* covariance, int covfun, 
   V->tw_d = dt.tw_d;
   HostVolume& hv = V->hv;
   if (hv.kriging_pending) kriging_solve_device(hv, device, V->stream);
+  const TraceScope tr("volume: uploads + FP64 spectrum");
   DevVolume& dv = V->dv;
   cudaStream_t st = V->stream;
   dv.E0 = hv.E[0]; dv.E1 = hv.E[1]; dv.E2 = hv.E[2]; dv.N = hv.N;
@@ -531,11 +619,11 @@ static void volume_build_device(Volume* V, const float* covariance, int covfun, 
   V->lam_re = V->alloc<double>(N);
   double2* base = nullptr;
   int* nS = nullptr;
-  CK(cudaMallocAsync(&base, sizeof(double2) * N, st));
-  const cudaError_t e2 = cudaMallocAsync(&nS, sizeof(int), st);
+  CK(dev_alloc((void**)&base, sizeof(double2) * N, st));
+  const cudaError_t e2 = dev_alloc((void**)&nS, sizeof(int), st);
   if (e2 != cudaSuccess) {
     cudaFreeAsync(base, st);
-    throw Error(DR_ERR_NOMEM, "cudaMallocAsync (spectrum scratch)");
+    throw Error(DR_ERR_NOMEM, "device allocation (spectrum scratch)");
   }
   try {
     CK(cudaMemsetAsync(nS, 0, sizeof(int), st));
@@ -571,7 +659,11 @@ static void volume_build(Volume* V, const dr_volume_desc* d) {
   const auto t0 = std::chrono::steady_clock::now();
   device_tables(d->device);
   std::string err;
-  const int rc = host_prepare(d, &V->hv, &err, device_kriging_enabled());
+  int rc;
+  {
+    const TraceScope tr("volume: host preparation (indices, kriging plan)");
+    rc = host_prepare(d, &V->hv, &err, device_kriging_enabled());
+  }
   if (rc != DR_OK) throw Error(rc, err);
   V->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   volume_build_device(V, d->covariance, d->covfun, d->device);
@@ -608,8 +700,8 @@ struct Chainset {
   T* alloc(size_t n, bool zero = true) {
     void* p = nullptr;
     if (n == 0) n = 1;
-    const cudaError_t e = cudaMallocAsync(&p, n * sizeof(T), stream);
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    const cudaError_t e = dev_alloc(&p, n * sizeof(T), stream);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     allocs.push_back(p);
     bytes += (int64_t)(n * sizeof(T));
     if (zero) CK(cudaMemsetAsync(p, 0, n * sizeof(T), stream));
@@ -899,8 +991,8 @@ static void tc_upload(Volume* V, const TcPlanHost& P, const float* dval, int nnz
   CK(cudaMemsetAsync(blob, 0, sizeof(float) * std::max<size_t>(nblob, 1), st));
   if (nnz > 0) {
     int* dest = nullptr;
-    const cudaError_t e = cudaMallocAsync(&dest, sizeof(int) * nnz, st);
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, "cudaMallocAsync (tile positions)");
+    const cudaError_t e = dev_alloc((void**)&dest, sizeof(int) * nnz, st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, "device allocation (tile positions)");
     CK(cudaMemcpyAsync(dest, P.dest.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
     k_tc_fill<<<cdiv_i(nnz, 256), 256, 0, st>>>(dval, dest, nnz, blob);
     CK_LAUNCH();
@@ -920,6 +1012,7 @@ static bool volume_tc(Volume* V) {
   const DeviceTables& dt = device_tables(V->device);
   if (!dt.tc || dv.n_s == 0 || hv.w_col.empty() || hv.wt_col.empty()) return false;
   const auto t0 = std::chrono::steady_clock::now();
+  TraceScope tr("tensor-core tiles: row keys + tile plans");
   CK(cudaSetDevice(V->device));
   auto coords = [&](int flat, int* x, int* y, int* z) {
     *x = flat % hv.E[0];
@@ -946,12 +1039,14 @@ static bool volume_tc(Volume* V) {
     kt[j] = zorder_key(x, y, z);
   }
   TcPlanHost pw, pt;
-  if (!tc_plan(hv.w_rowptr, hv.w_col, kw, dt.sms, &pw) || !tc_plan(hv.wt_rowptr, hv.wt_col, kt, dt.sms, &pt))
+  if (!tc_plan(hv.w_rowptr, hv.w_col.data(), hv.w_col.size(), kw, dt.sms, &pw) ||
+      !tc_plan(hv.wt_rowptr, hv.wt_col.data(), hv.wt_col.size(), kt, dt.sms, &pt))
     return false;
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   const double blob_bytes = (double)(pw.chunks + pt.chunks) * TC_BLK * 4;
   if (blob_bytes > 0.25 * (double)fr) return false;
+  tr.next("tensor-core tiles: blob build");
   tc_upload(V, pw, dv.w_val, (int)hv.w_col.size(), dv.n_s, dv.n_h, &V->tc_w);
   tc_upload(V, pt, dv.wt_val, (int)hv.wt_col.size(), dv.n_h, dv.n_s, &V->tc_wt);
   V->tc_max_segs = std::max(V->tc_w.n_segs, V->tc_wt.n_segs);
@@ -1044,37 +1139,19 @@ static void launch_iterations(Chainset* S, int iters);
 static void read_states(Chainset* S, std::vector<ChainState>* st);
 static void write_states(Chainset* S, const std::vector<ChainState>& st);
 
-// Tunes in two rounds on scratch chain sets of the same shape, each candidate
-// timed for 2 iterations forced past the step-size search (so that all L
-// leapfrog steps run): first the update paths, with the tensor-core products
-// where the volume and chain count allow them (else CSR products at 8 blocks
-// per SM); then, on the fastest path, the other product choices (CSR at 8
-// blocks/SM, and at 4 and 2 for chain sets of fewer than 32 chains).  The
-// fastest candidate is kept and cached per shape.
-// Keeps freed device memory in the device's default pool for its scope (the process's pool attribute, restored at
-// the end), so that the tuner's scratch chain sets reuse one another's memory.
-struct PoolKeep {
-  cudaMemPool_t pool{};
-  uint64_t old = 0;
-  bool ok = false;
-  explicit PoolKeep(int dev) {
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &old) == cudaSuccess) {
-      uint64_t keep = UINT64_MAX;
-      ok = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
-    }
-    cudaGetLastError();
-  }
-  ~PoolKeep() {
-    if (ok) cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &old);
-    cudaGetLastError();
-  }
-};
 
 // Quarter-octave bucket of a voxel count: volumes of one shape whose data counts differ by less than about 19 %
 // share a tuning result (it chooses a speed, not a result), so a stream of similar jobs tunes once.
 static int tune_bucket(int n) { return n <= 0 ? -1 : (int)std::lround(4.0 * std::log2((double)n)); }
 
+// Tunes in two rounds on scratch chain sets of the same shape, each candidate
+// timed for 2 iterations forced past the step-size search (so that all of
+// their leapfrog steps run, at most 6 of them): first the update paths, with
+// the tensor-core products where the volume and chain count allow them (else
+// CSR products at 8 blocks per SM); then, on the fastest path, the other
+// product choices (CSR at 8 blocks/SM, and at 4 and 2 for chain sets of fewer
+// than 32 chains) and the z-pass tile shape.  The fastest candidate is kept
+// and cached per shape.
 static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   const NvtxRange range("chain set: tuning");
   const DevVolume& v = V->dv;
@@ -1087,14 +1164,21 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
   }
   const PathOptions po = path_options(v, V->device);
   const bool tc = tc_chains(C) > 0 && !tc_env_off() && volume_tc(V);
-  const PoolKeep keep(V->device);
   TuneChoice best;
   best.ms = 1e300;
   dr_hmc_opts to = *o;
   to.store_samples = 0;
+  // candidates are timed on iterations of at most TUNE_STEPS leapfrog steps: every step runs the same kernels, so
+  // the ranking holds, and a candidate costs a quarter of a full iteration at L = 25; the time kept for the choice
+  // is scaled to the full L (steps + 1 gradient evaluations per iteration)
+  constexpr int TUNE_STEPS = 6;
+  to.leapfrog = std::min(o->leapfrog, TUNE_STEPS);
+  const double to_full = (double)(o->leapfrog + 1) / (double)(to.leapfrog + 1);
   auto try_candidate = [&](TuneChoice c) {
     // a candidate that cannot be built or run (for instance out of device memory beside the caller's other
     // allocations) is skipped; if none can, the default configuration is used untuned
+    const TraceScope tr("tuning candidate path " + std::to_string(c.path) + " tc " + std::to_string(c.tc) +
+                        " grid " + std::to_string(c.grid) + " ztile " + std::to_string(c.ztile));
     try {
       auto T = std::make_unique<Chainset>();
       chainset_build(T.get(), V, C, &to, &c);
@@ -1117,7 +1201,8 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
       CK(cudaEventElapsedTime(&ms, e0, e1));
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      c.ms = ms / 2.0;
+      c.ms = ms / 2.0 * to_full;
+      if (trace_on()) std::fprintf(stderr, "[drb]   measured %.3f ms per iteration (scaled to L)\n", c.ms);
       if (c.ms < best.ms) best = c;
     } catch (const Error&) {
       cudaGetLastError();
@@ -1163,6 +1248,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     S->vol = V;
     V->n_chainsets++;
   }
+  const TraceScope tr("chain set: build (" + std::to_string(C) + " chains" + (forced ? ", tuning candidate)" : ")"));
   S->device = V->device;
   S->C = C;
   S->opts = *o;
@@ -1874,7 +1960,7 @@ int dr_debug_tc_layout(int n_rows, int n_cols, const int* rowptr, const int* col
   std::vector<int> rp(rowptr, rowptr + n_rows + 1), cl(col, col + nnz);
   std::vector<uint32_t> ky(keys, keys + n_rows);
   TcPlanHost P;
-  if (!tc_plan(rp, cl, ky, g_max, &P)) throw Error(DR_ERR_INVALID, "matrix too large for the tile layout");
+  if (!tc_plan(rp, cl.data(), cl.size(), ky, g_max, &P)) throw Error(DR_ERR_INVALID, "matrix too large for the tile layout");
   std::vector<float> blob((size_t)P.chunks * TC_BLK, 0.f);
   for (int i = 0; i < nnz; i++) blob[P.dest[i]] = val[i];
   std::fill(dense, dense + (size_t)n_rows * n_cols, 0.f);
@@ -1971,6 +2057,19 @@ int dr_debug_time_kernel(dr_chainset* s, int which, int stp, int reps, double* a
     }
     *algo_bytes = b;
   }
+  API_END
+}
+
+int dr_debug_pool_usage(int device, int reset_high, uint64_t* used, uint64_t* high) {
+  API_BEGIN
+  if (!used || !high) throw Error(DR_ERR_INVALID, "bad argument");
+  cudaMemPool_t pool = device_tables(device).pool;
+  if (reset_high) {
+    uint64_t zero = 0;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+  }
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, used));
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, high));
   API_END
 }
 
@@ -2357,13 +2456,6 @@ int dr_server_create(const dr_server_opts* opts, dr_server** out) {
   if (sv->o.max_active <= 0) sv->o.max_active = 64;
   if (sv->o.iterations_per_round <= 0) sv->o.iterations_per_round = 8;
   if (sv->o.host_threads <= 0) sv->o.host_threads = 4;
-  {
-    // Keep freed device memory in the pool between jobs instead of returning it at every synchronisation.
-    cudaMemPool_t pool;
-    CK(cudaDeviceGetDefaultMemPool(&pool, opts->device));
-    uint64_t keep = UINT64_MAX;
-    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-  }
   if (sv->o.hbm_budget_bytes > 0) {
     sv->budget = sv->o.hbm_budget_bytes;
   } else {
@@ -2559,8 +2651,8 @@ int dr_mce_summary(const float* img, int nx, int ny, int nz, const float* qform,
   std::vector<void*> bufs;
   auto dalloc = [&](size_t bytes) {
     void* p = nullptr;
-    const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
-    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    const cudaError_t e = dev_alloc(&p, std::max<size_t>(bytes, 16), st);
+    if (e != cudaSuccess) throw Error(DR_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     bufs.push_back(p);
     return p;
   };

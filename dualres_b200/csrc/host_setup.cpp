@@ -225,6 +225,7 @@ int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, cons
     for (int r = 0; r < 3; r++)
       Pm[3 * i + r] = (double)Qhr[4 * r] * P[3 * i] + (double)Qhr[4 * r + 1] * P[3 * i + 1] +
                       (double)Qhr[4 * r + 2] * P[3 * i + 2];
+#pragma omp parallel for schedule(dynamic, 16)
   for (int i = 0; i < m; i++) {
     K[(size_t)i * m + i] = 1.0;
     for (int j = 0; j < i; j++) {
@@ -270,40 +271,43 @@ int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, cons
   for (long s = 0; s < nvs; s++)
     if (has_data(sr[s])) rows.push_back(s);
   const int nrows = (int)rows.size();
-  std::vector<std::vector<int>> rcol(nrows), rpid(nrows);
-  std::vector<std::vector<double>> rkp(nrows);
   int bad = 0;
-  // candidates per row (kriging_matrix.h:242-299)
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int ri = 0; ri < nrows; ri++) {
+  // candidates per row (kriging_matrix.h:242-299), enumerated twice: a counting pass sizes the rows, then each row
+  // is written straight into its place in the flat arrays
+  auto row_frame = [&](int ri, int base[3], double sm[3]) {
     const long sidx = rows[ri];
     const double s[4] = {(double)(sidx % sx), (double)((sidx / sx) % sy), (double)(sidx / ((long)sx * sy)), 1.0};
-    int base[3];
-    double sm[3];
     for (int r = 0; r < 3; r++) {
       double a = 0.0, b = 0.0;
       for (int k = 0; k < 4; k++) { a += mp[4 * r + k] * s[k]; b += Qs[4 * r + k] * s[k]; }
       base[r] = (int)a;  // truncation toward zero (kriging_matrix.h:255)
       sm[r] = b;
     }
+  };
+  // ordinal of candidate j of a row at `base`, -1 when absent, -2 when outside the bounded map
+  auto candidate = [&](const int base[3], int j, int* h) -> int {
+    h[0] = base[0] + P[3 * j];
+    h[1] = base[1] + P[3 * j + 1];
+    h[2] = base[2] + P[3 * j + 2];
+    const long flat = (long)h[2] * ny * nx + (long)h[1] * nx + h[0];  // flat-offset-only check (:263-266)
+    if (flat < 0 || flat >= nvox || !has_data(hr[flat])) return -1;
+    const long b = (long)(h[2] - bbmin[2]) * bd[0] * bd[1] + (long)(h[1] - bbmin[1]) * bd[0] + (h[0] - bbmin[0]);
+    if (b < 0 || b >= bprod) return -2;
+    return bmap[b];
+  };
+  plan->row_start.assign(nrows + 1, 0);
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : bad)
+  for (int ri = 0; ri < nrows; ri++) {
+    int base[3], h[3];
+    double sm[3];
+    row_frame(ri, base, sm);
+    int n = 0;
     for (int j = 0; j < m; j++) {
-      const int h0 = base[0] + P[3 * j], h1 = base[1] + P[3 * j + 1], h2 = base[2] + P[3 * j + 2];
-      const long flat = (long)h2 * ny * nx + (long)h1 * nx + h0;  // flat-offset-only check (:263-266)
-      if (flat < 0 || flat >= nvox || !has_data(hr[flat])) continue;
-      const long b = (long)(h2 - bbmin[2]) * bd[0] * bd[1] + (long)(h1 - bbmin[1]) * bd[0] + (h0 - bbmin[0]);
-      if (b < 0 || b >= bprod) {
-#pragma omp atomic
-        bad++;
-        continue;
-      }
-      if (bmap[b] < 0) continue;
-      rcol[ri].push_back(bmap[b]);
-      rpid[ri].push_back(j);
-      double hm[3];
-      for (int r = 0; r < 3; r++) hm[r] = Qh[4 * r] * h0 + Qh[4 * r + 1] * h1 + Qh[4 * r + 2] * h2 + Qh[4 * r + 3];
-      const double dx = sm[0] - hm[0], dy = sm[1] - hm[1], dz = sm[2] - hm[2];
-      rkp[ri].push_back(rbf(std::sqrt(dx * dx + dy * dy + dz * dz) + 1e-5, th));
+      const int o = candidate(base, j, h);
+      if (o == -2) bad++;
+      n += o >= 0;
     }
+    plan->row_start[ri + 1] = n;
   }
   if (bad) {
     *err = "kriging: a neighbourhood index falls outside the bounded high-res index map (undefined in the reference)";
@@ -347,17 +351,28 @@ int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, cons
   (void)have_inv;
   plan->m = m;
   plan->nrows = nrows;
-  plan->row_start.assign(nrows + 1, 0);
-  for (int ri = 0; ri < nrows; ri++) plan->row_start[ri + 1] = plan->row_start[ri] + (int)rcol[ri].size();
+  for (int ri = 0; ri < nrows; ri++) plan->row_start[ri + 1] += plan->row_start[ri];
   const size_t tot = (size_t)plan->row_start[nrows];
   plan->pid.resize(tot);
   plan->col.resize(tot);
   plan->kp.resize(tot);
+#pragma omp parallel for schedule(dynamic, 16)
   for (int ri = 0; ri < nrows; ri++) {
-    const size_t o = (size_t)plan->row_start[ri];
-    std::copy(rpid[ri].begin(), rpid[ri].end(), plan->pid.begin() + o);
-    std::copy(rcol[ri].begin(), rcol[ri].end(), plan->col.begin() + o);
-    std::copy(rkp[ri].begin(), rkp[ri].end(), plan->kp.begin() + o);
+    int base[3], h[3];
+    double sm[3];
+    row_frame(ri, base, sm);
+    size_t o = (size_t)plan->row_start[ri];
+    for (int j = 0; j < m; j++) {
+      const int c = candidate(base, j, h);
+      if (c < 0) continue;
+      plan->col[o] = c;
+      plan->pid[o] = j;
+      double hm[3];
+      for (int r = 0; r < 3; r++) hm[r] = Qh[4 * r] * h[0] + Qh[4 * r + 1] * h[1] + Qh[4 * r + 2] * h[2] + Qh[4 * r + 3];
+      const double dx = sm[0] - hm[0], dy = sm[1] - hm[1], dz = sm[2] - hm[2];
+      plan->kp[o] = rbf(std::sqrt(dx * dx + dy * dy + dz * dz) + 1e-5, th);
+      o++;
+    }
   }
   return DR_OK;
 }
@@ -430,8 +445,8 @@ bool kriging_solve_row_host(const KrigingPlan& plan, int ri, std::vector<double>
   return true;
 }
 
-void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, std::vector<int>* col,
-                        std::vector<float>* val) {
+void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, fill_vector<int>* col,
+                        fill_vector<float>* val) {
   const int m = plan.m, nrows = plan.nrows;
   // Rows whose neighbourhood is complete share K; identical k' then share w.
   std::map<std::vector<double>, std::vector<double>> full_cache;
@@ -467,21 +482,26 @@ void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, std::
   std::vector<double> flat(plan.col.size(), 0.0);
   for (int ri = 0; ri < nrows; ri++)
     if (keep[ri]) std::copy(rw[ri].begin(), rw[ri].end(), flat.begin() + plan.row_start[ri]);
-  kriging_assemble(plan, flat, keep, rowptr, col, val);
+  kriging_assemble(plan, flat.data(), keep, rowptr, col, val);
 }
 
-void kriging_assemble(const KrigingPlan& plan, const std::vector<double>& w, const std::vector<char>& keep,
-                      std::vector<int>* rowptr, std::vector<int>* col, std::vector<float>* val) {
+void kriging_assemble(const KrigingPlan& plan, const double* w, const std::vector<char>& keep,
+                      std::vector<int>* rowptr, fill_vector<int>* col, fill_vector<float>* val) {
   rowptr->assign(plan.nrows + 1, 0);
-  col->clear();
-  val->clear();
   for (int ri = 0; ri < plan.nrows; ri++) {
-    const int r0 = plan.row_start[ri], r1 = plan.row_start[ri + 1];
-    if (keep[ri] && r1 > r0) {
-      col->insert(col->end(), plan.col.begin() + r0, plan.col.begin() + r1);
-      for (int k = r0; k < r1; k++) val->push_back((float)w[k]);
+    const int n = plan.row_start[ri + 1] - plan.row_start[ri];
+    (*rowptr)[ri + 1] = (*rowptr)[ri] + (keep[ri] ? n : 0);
+  }
+  col->resize((size_t)(*rowptr)[plan.nrows]);
+  val->resize((size_t)(*rowptr)[plan.nrows]);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int ri = 0; ri < plan.nrows; ri++) {
+    if (!keep[ri]) continue;
+    const int r0 = plan.row_start[ri], r1 = plan.row_start[ri + 1], o = (*rowptr)[ri];
+    for (int k = r0; k < r1; k++) {
+      (*col)[o + k - r0] = plan.col[k];
+      (*val)[o + k - r0] = (float)w[k];
     }
-    (*rowptr)[ri + 1] = (int)col->size();
   }
 }
 
@@ -491,7 +511,11 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
   KrigingPlan plan;
   const int rc = kriging_plan(hr, nx, ny, nz, Qhr, sr, sx, sy, sz, Qsr, theta, radius, &plan, n_offsets, err);
   if (rc != DR_OK) return rc;
-  kriging_solve_host(plan, rowptr, col, val);
+  fill_vector<int> c;
+  fill_vector<float> v;
+  kriging_solve_host(plan, rowptr, &c, &v);
+  col->assign(c.begin(), c.end());
+  val->assign(v.begin(), v.end());
   return DR_OK;
 }
 
@@ -499,19 +523,52 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
 // ---------------------------------------------------------------- preparation
 void build_transpose(HostVolume* hv) {
   const int n_h = (int)hv->Yh.size(), n_s = (int)hv->Ys.size();
+  const size_t nnz = hv->w_col.size();
   hv->wt_rowptr.assign(n_h + 1, 0);
-  for (int c : hv->w_col) hv->wt_rowptr[c + 1]++;
-  for (int i = 0; i < n_h; i++) hv->wt_rowptr[i + 1] += hv->wt_rowptr[i];
-  hv->wt_col.resize(hv->w_col.size());
-  hv->wt_val.resize(hv->w_col.size());
-  std::vector<int> fill(hv->wt_rowptr.begin(), hv->wt_rowptr.end() - 1);
-  for (int r = 0; r < n_s; r++)
-    for (int k = hv->w_rowptr[r]; k < hv->w_rowptr[r + 1]; k++) {
-      const int c = hv->w_col[k];
-      hv->wt_col[fill[c]] = r;
-      hv->wt_val[fill[c]] = hv->w_val[k];
-      fill[c]++;
+  hv->wt_col.resize(nnz);
+  hv->wt_val.resize(nnz);
+  // Counting sort by column over T contiguous chunks of W's rows: chunk t's entries of column c land after those
+  // of chunks 0..t-1, so every row of W^T lists its std-res rows in ascending order, as a serial pass would.
+  int T = 1;
+#ifdef _OPENMP
+  T = std::max(1, std::min(omp_get_max_threads(), n_s / 256));
+#endif
+  std::vector<int> cnt((size_t)T * n_h, 0);
+  auto chunk = [&](int t, int* r0, int* r1) {
+    *r0 = (int)((long long)n_s * t / T);
+    *r1 = (int)((long long)n_s * (t + 1) / T);
+  };
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+  for (int t = 0; t < T; t++) {
+    int r0, r1;
+    chunk(t, &r0, &r1);
+    int* ct = cnt.data() + (size_t)t * n_h;
+    for (int k = hv->w_rowptr[r0]; k < hv->w_rowptr[r1]; k++) ct[hv->w_col[k]]++;
+  }
+  // column totals, then each chunk's start within each column
+  for (int c = 0; c < n_h; c++) {
+    int run = 0;
+    for (int t = 0; t < T; t++) {
+      const int v = cnt[(size_t)t * n_h + c];
+      cnt[(size_t)t * n_h + c] = run;
+      run += v;
     }
+    hv->wt_rowptr[c + 1] = run;
+  }
+  for (int i = 0; i < n_h; i++) hv->wt_rowptr[i + 1] += hv->wt_rowptr[i];
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+  for (int t = 0; t < T; t++) {
+    int r0, r1;
+    chunk(t, &r0, &r1);
+    int* ct = cnt.data() + (size_t)t * n_h;
+    for (int r = r0; r < r1; r++)
+      for (int k = hv->w_rowptr[r]; k < hv->w_rowptr[r + 1]; k++) {
+        const int c = hv->w_col[k];
+        const int at = hv->wt_rowptr[c] + ct[c]++;
+        hv->wt_col[at] = r;
+        hv->wt_val[at] = hv->w_val[k];
+      }
+  }
 }
 
 uint32_t zorder_key(int x, int y, int z) {
@@ -522,7 +579,7 @@ uint32_t zorder_key(int x, int y, int z) {
   return k;
 }
 
-bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const std::vector<uint32_t>& key, int g_max,
+bool tc_plan(const std::vector<int>& rowptr, const int* col, size_t nnz, const std::vector<uint32_t>& key, int g_max,
              TcPlanHost* P) {
   constexpr int M = 128, KC = 32, BLK = M * KC;
   const int R = (int)rowptr.size() - 1;
@@ -533,7 +590,7 @@ bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const 
   P->tile_rows.assign((size_t)P->T * M, -1);
   for (int i = 0; i < R; i++) P->tile_rows[i] = order[i];
   int n_cols = 0;
-  for (int c : col) n_cols = std::max(n_cols, c + 1);
+  for (size_t k = 0; k < nnz; k++) n_cols = std::max(n_cols, col[k] + 1);
   // per tile: the sorted union of its rows' columns (a per-thread stamp array marks columns already taken)
   std::vector<std::vector<int>> uni(P->T);
 #pragma omp parallel
@@ -559,7 +616,7 @@ bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const 
   P->chunks = chunk_ptr[P->T];
   if (P->chunks * BLK > 0x7fffffffLL) return false;
   P->chunk_cols.assign((size_t)P->chunks * KC, -1);
-  P->dest.assign(col.size(), -1);
+  P->dest.assign(nnz, -1);
 #pragma omp parallel
   {
     std::vector<int> pos(n_cols, 0);

@@ -1,12 +1,37 @@
 // One-time host set-up of a volume: masks, indices and the kriging matrix.
 #pragma once
 
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dualres_b200.h"
 
 namespace drb {
+
+// Allocator whose value-less construction leaves the elements uninitialised: large buffers that are written in
+// full right after allocation (in parallel) skip a serial zero-fill of hundreds of MB on scanner-sized volumes.
+template <class T>
+struct uninit_allocator : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = uninit_allocator<U>;
+  };
+  uninit_allocator() = default;
+  template <class U>
+  uninit_allocator(const uninit_allocator<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using fill_vector = std::vector<T, uninit_allocator<T>>;
 
 // The part of the kriging build that fixes the sparsity (kriging_matrix.h:148-299)
 // and the covariances the per-row solves need.
@@ -17,9 +42,9 @@ struct KrigingPlan {
   std::vector<double> S;       // K^-1, empty when K is not positive definite (or not computed yet)
   bool inverse_wanted = true;  // the Schur route is allowed (DRB_KRIGING_DIRECT unset)
   std::vector<int> row_start;  // nrows + 1, into pid / col / kp
-  std::vector<int> pid;        // offset id of each present neighbour
-  std::vector<int> col;        // its high-res data ordinal (the CSR column)
-  std::vector<double> kp;      // its covariance with the std-res voxel centre
+  fill_vector<int> pid;        // offset id of each present neighbour
+  fill_vector<int> col;        // its high-res data ordinal (the CSR column)
+  fill_vector<double> kp;      // its covariance with the std-res voxel centre
 };
 
 // A row with cnt of m neighbours present solves through the Schur complement of
@@ -37,10 +62,9 @@ struct HostVolume {
   std::vector<int> d_flat, o_flat;   // flat embedding indices
   std::vector<int> box_to_d, box_to_o;
   std::vector<float> Yh, Ys;
-  std::vector<int> w_rowptr, w_col;
-  std::vector<float> w_val;
-  std::vector<int> wt_rowptr, wt_col;
-  std::vector<float> wt_val;
+  std::vector<int> w_rowptr, wt_rowptr;
+  fill_vector<int> w_col, wt_col;
+  fill_vector<float> w_val, wt_val;
   float Q[16];
   double theta[3];
   int covfun = 0;
@@ -66,14 +90,14 @@ void build_transpose(HostVolume* hv);
 int kriging_plan(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
                  const float* Qsr, const float* theta, float radius, KrigingPlan* plan, int* n_offsets,
                  std::string* err, bool host_inverse = true);
-void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, std::vector<int>* col,
-                        std::vector<float>* val);
+void kriging_solve_host(const KrigingPlan& plan, std::vector<int>* rowptr, fill_vector<int>* col,
+                        fill_vector<float>* val);
 // One row by the host route (Schur or Cholesky, QR if not positive definite);
 // false when its weight sum is NaN.
 bool kriging_solve_row_host(const KrigingPlan& plan, int ri, std::vector<double>* x);
 // CSR from per-candidate weights; rows with keep = 0 are emptied (NaN weight sums).
-void kriging_assemble(const KrigingPlan& plan, const std::vector<double>& w, const std::vector<char>& keep,
-                      std::vector<int>* rowptr, std::vector<int>* col, std::vector<float>* val);
+void kriging_assemble(const KrigingPlan& plan, const double* w, const std::vector<char>& keep,
+                      std::vector<int>* rowptr, fill_vector<int>* col, fill_vector<float>* val);
 
 // Kriging CSR of kriging_matrix.h:148-343 (exposed for tests through the volume).
 int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, const float* sr, int sx, int sy, int sz,
@@ -93,7 +117,7 @@ struct TcPlanHost {
   std::vector<int> tile_rows, chunk_cols, segs, cta_seg_ptr, tile_seg_ptr, dest;
 };
 // false when the blob would not be addressable with 32-bit positions.
-bool tc_plan(const std::vector<int>& rowptr, const std::vector<int>& col, const std::vector<uint32_t>& key, int g_max,
+bool tc_plan(const std::vector<int>& rowptr, const int* col, size_t nnz, const std::vector<uint32_t>& key, int g_max,
              TcPlanHost* P);
 // Z-order key of integer voxel coordinates (10 bits each).
 uint32_t zorder_key(int x, int y, int z);

@@ -68,45 +68,46 @@ __device__ __forceinline__ double kr_block_sum(double v, double* red) {
   return s;
 }
 
-// Factor the kb x kb block in sm.D in place (lower) with warp 0 and write its
-// inverse to sm.Di.  Returns false (block-uniform) if a pivot is not positive.
-__device__ bool kr_factor_diag(KrigSmem& sm, int kb) {
+// Factor the kb x kb block D in place (lower) with warp 0 and write its
+// inverse to Di.  Returns false (block-uniform) if a pivot is not positive.
+__device__ bool kr_factor_diag(double (*D)[KR_LDT], double (*Di)[KR_LDT], int& flag, int kb) {
   const int lane = threadIdx.x & 31;
   if (threadIdx.x < 32) {
     int bad = 0;
     for (int j = 0; j < kb; j++) {
       if (lane == j) {
-        const double d = sm.D[j][j];
+        const double d = D[j][j];
         if (!(d > 0.0)) bad = 1;
-        sm.D[j][j] = sqrt(fmax(d, 1e-300));
+        D[j][j] = sqrt(fmax(d, 1e-300));
       }
       bad = __shfl_sync(0xffffffffu, bad, j);
       __syncwarp();
-      const double djj = sm.D[j][j];
-      if (lane > j && lane < kb) sm.D[lane][j] /= djj;
+      const double djj = D[j][j];
+      if (lane > j && lane < kb) D[lane][j] /= djj;
       __syncwarp();
       if (lane > j && lane < kb) {
-        const double lij = sm.D[lane][j];
-        for (int l = j + 1; l <= lane; l++) sm.D[lane][l] -= lij * sm.D[l][j];
+        const double lij = D[lane][j];
+        for (int l = j + 1; l <= lane; l++) D[lane][l] -= lij * D[l][j];
       }
       __syncwarp();
     }
-    if (lane == 0) sm.flag = bad;
+    if (lane == 0) flag = bad;
   }
   __syncthreads();
-  if (sm.flag) return false;
+  if (flag) return false;
   // inverse of the lower-triangular factor, one column per thread (forward substitution)
   if (threadIdx.x < kb) {
     const int j = threadIdx.x;
     for (int i = 0; i < kb; i++) {
       double s = i == j ? 1.0 : 0.0;
-      for (int l = j; l < i; l++) s -= sm.D[i][l] * sm.Di[l][j];
-      sm.Di[i][j] = i < j ? 0.0 : s / sm.D[i][i];
+      for (int l = j; l < i; l++) s -= D[i][l] * Di[l][j];
+      Di[i][j] = i < j ? 0.0 : s / D[i][i];
     }
   }
   __syncthreads();
   return true;
 }
+__device__ bool kr_factor_diag(KrigSmem& sm, int kb) { return kr_factor_diag(sm.D, sm.Di, sm.flag, kb); }
 
 // In-place Cholesky M = L L^T of the n x n matrix (row-major, lower triangle read and written).
 __device__ bool kr_cholesky(double* M, int n, KrigSmem& sm) {
@@ -267,38 +268,198 @@ __device__ void kr_rows_dot(const double* Mat, int m, const int* rows, int nrows
   }
 }
 
-// K = L L^T in place by one block (M holds K on entry); *ok = 1 when K is positive definite.
-__global__ void __launch_bounds__(KR_NT) k_spd_factor(double* M, int n, int* ok) {
-  extern __shared__ __align__(16) unsigned char kr_smraw[];
-  KrigSmem& sm = *reinterpret_cast<KrigSmem*>(kr_smraw);
-  const bool good = kr_cholesky(M, n, sm);
-  if (threadIdx.x == 0) *ok = good ? 1 : 0;
-}
+// ---------------------------------------------------------------- K^-1 over the whole GPU
+// S = K^-1 of the neighbourhood covariance (m up to 5000), once per volume:
+//   right-looking blocked Cholesky K = L L^T in panels of KR_NB columns: the diagonal block by one CTA
+//   (k_chol_diag, which also keeps the inverse of the block's factor), the panel below it by one CTA per 64 rows
+//   (k_chol_panel), the trailing update by one CTA per 64 x 64 tile of the lower triangle (k_chol_update);
+//   X = L^-1 one block row at a time, X_ij = -Dinv_i sum_{j <= k < i} L_ik X_kj, one CTA per block column
+//   (k_trinv_row);  S = X^T X, one CTA per 32 x 32 tile of the lower triangle, stored to both triangles so that S is
+//   exactly symmetric (k_trinv_gram).
+// A pivot that is not positive clears *ok and every later launch returns at once.
 
-// Rows of S = K^-1 from the factor: each block solves L L^T x = e_j for its
-// share of j (x in its scratch vector) and stores x as row j of S.
-__global__ void __launch_bounds__(KR_NT) k_spd_inverse(const double* L, int n, double* S, double* scratch) {
-  extern __shared__ __align__(16) unsigned char kr_smraw[];
-  KrigSmem& sm = *reinterpret_cast<KrigSmem*>(kr_smraw);
-  double* b = scratch + (size_t)blockIdx.x * n;
-  for (int j = blockIdx.x; j < n; j += gridDim.x) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += KR_NT) b[i] = i == j ? 1.0 : 0.0;
-    __syncthreads();
-    kr_solve(L, n, b, sm);
-    for (int i = threadIdx.x; i < n; i += KR_NT) S[(size_t)j * n + i] = b[i];
+// The kb x kb diagonal block at k0: factored in place, its factor's inverse to Dinv[k0 / KR_NB] (32 x 32, zero
+// outside kb x kb).
+__global__ void __launch_bounds__(KR_NT) k_chol_diag(double* M, int n, int k0, double* Dinv, int* ok) {
+  __shared__ double D[KR_NB][KR_LDT], Di[KR_NB][KR_LDT];
+  __shared__ int flag;
+  if (!*ok) return;
+  const int kb = min(KR_NB, n - k0), tid = threadIdx.x;
+  for (int e = tid; e < KR_NB * KR_NB; e += KR_NT) {
+    const int i = e / KR_NB, j = e % KR_NB;
+    D[i][j] = (i < kb && j <= i) ? M[(size_t)(k0 + i) * n + k0 + j] : 0.0;
+    Di[i][j] = 0.0;
+  }
+  __syncthreads();
+  const bool good = kr_factor_diag(D, Di, flag, kb);
+  if (!good) {
+    if (tid == 0) *ok = 0;
+    return;
+  }
+  double* Dg = Dinv + (size_t)(k0 / KR_NB) * KR_NB * KR_NB;
+  for (int e = tid; e < KR_NB * KR_NB; e += KR_NT) {
+    const int i = e / KR_NB, j = e % KR_NB;
+    if (i < kb && j <= i) M[(size_t)(k0 + i) * n + k0 + j] = D[i][j];
+    Dg[e] = (i < kb && j < kb) ? Di[i][j] : 0.0;
   }
 }
 
-// S = (S + S^T) / 2 (the two triangular solves leave O(eps) asymmetry).
-__global__ void k_symmetrize(double* S, int n) {
-  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)n * n) return;
-  const int i = (int)(e / n), j = (int)(e % n);
-  if (j >= i) return;
-  const double a = 0.5 * (S[(size_t)i * n + j] + S[(size_t)j * n + i]);
-  S[(size_t)i * n + j] = a;
-  S[(size_t)j * n + i] = a;
+// L[i, k0:k0+kb] = A[i, k0:k0+kb] Dinv^T for the 64 rows i of this CTA below the diagonal block.
+__global__ void __launch_bounds__(KR_NT) k_chol_panel(double* M, int n, int k0, const double* Dinv, const int* ok) {
+  __shared__ double Di[KR_NB][KR_LDT], PA[KR_TILE][KR_LDT];
+  if (!*ok) return;
+  const int kb = min(KR_NB, n - k0), tid = threadIdx.x;
+  const int c0 = k0 + kb + blockIdx.x * KR_TILE, ch = min(KR_TILE, n - c0);
+  const double* Dg = Dinv + (size_t)(k0 / KR_NB) * KR_NB * KR_NB;
+  for (int e = tid; e < KR_NB * KR_NB; e += KR_NT) Di[e / KR_NB][e % KR_NB] = Dg[e];
+  for (int e = tid; e < ch * kb; e += KR_NT) {
+    const int i = e / kb, l = e % kb;
+    PA[i][l] = M[(size_t)(c0 + i) * n + k0 + l];
+  }
+  __syncthreads();
+  for (int e = tid; e < ch * kb; e += KR_NT) {
+    const int i = e / kb, j = e % kb;
+    double s = 0.0;
+    for (int l = 0; l <= j; l++) s += PA[i][l] * Di[j][l];
+    M[(size_t)(c0 + i) * n + k0 + j] = s;
+  }
+}
+
+// Lower-triangle tile index b -> (tI, tJ), tJ <= tI.
+__device__ __forceinline__ void kr_tri_tile(int b, int* tI, int* tJ) {
+  int i = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+  while (i * (i + 1) / 2 > b) i--;
+  while ((i + 1) * (i + 2) / 2 <= b) i++;
+  *tI = i;
+  *tJ = b - i * (i + 1) / 2;
+}
+
+// A[i, j] -= L[i, panel] . L[j, panel] on one 64 x 64 tile of the trailing lower triangle.
+__global__ void __launch_bounds__(KR_NT) k_chol_update(double* M, int n, int k0, const int* ok) {
+  __shared__ double PA[KR_TILE][KR_LDT], PB[KR_TILE][KR_LDT];
+  if (!*ok) return;
+  const int kb = min(KR_NB, n - k0), r0 = k0 + kb, tid = threadIdx.x;
+  int tI, tJ;
+  kr_tri_tile(blockIdx.x, &tI, &tJ);
+  const int i0 = r0 + tI * KR_TILE, j0 = r0 + tJ * KR_TILE;
+  const int ni = min(KR_TILE, n - i0), nj = min(KR_TILE, n - j0);
+  for (int e = tid; e < KR_TILE * kb; e += KR_NT) {
+    const int i = e / kb, l = e % kb;
+    PA[i][l] = i < ni ? M[(size_t)(i0 + i) * n + k0 + l] : 0.0;
+    PB[i][l] = i < nj ? M[(size_t)(j0 + i) * n + k0 + l] : 0.0;
+  }
+  __syncthreads();
+  const int ty = tid / 16, tx = tid % 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+  for (int l = 0; l < kb; l++) {
+    double pa[4], pb[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) pa[a] = PA[ty * 4 + a][l];
+#pragma unroll
+    for (int b = 0; b < 4; b++) pb[b] = PB[tx * 4 + b][l];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = fma(pa[a], pb[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int i = ty * 4 + a;
+    if (i >= ni) continue;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int j = tx * 4 + b;
+      if (j >= nj || j0 + j > i0 + i) continue;
+      M[(size_t)(i0 + i) * n + j0 + j] -= acc[a][b];
+    }
+  }
+}
+
+// One 32 x 32 tile product acc += A^T? B over shared tiles: acc[p][q] += sum_r TA[p][r] TB[r][q] (TRANS = false) or
+// sum_r TA[r][p] TB[r][q] (TRANS = true); each of the 256 threads owns 4 entries (p = tid / 8, q = 4 (tid % 8) + b).
+template <bool TRANS>
+__device__ __forceinline__ void kr_tile_mac(const double (*TA)[KR_LDT], const double (*TB)[KR_LDT], double acc[4]) {
+  const int p = threadIdx.x / 8, q0 = 4 * (threadIdx.x % 8);
+  for (int r = 0; r < KR_NB; r++) {
+    const double a = TRANS ? TA[r][p] : TA[p][r];
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[b] = fma(a, TB[r][q0 + b], acc[b]);
+  }
+}
+
+// Loads the 32 x 32 tile of the n x n row-major matrix at block (bi, bj), zero outside n x n.
+__device__ __forceinline__ void kr_load_tile(double (*T)[KR_LDT], const double* A, int n, int bi, int bj) {
+  for (int e = threadIdx.x; e < KR_NB * KR_NB; e += KR_NT) {
+    const int i = e / KR_NB, j = e % KR_NB, gi = bi * KR_NB + i, gj = bj * KR_NB + j;
+    T[i][j] = (gi < n && gj < n) ? A[(size_t)gi * n + gj] : 0.0;
+  }
+}
+
+// Block row bi of X = L^-1: CTA bj < bi computes X[bi][bj] = -Dinv_bi sum_{bj <= k < bi} L[bi][k] X[k][bj];
+// CTA bj = bi writes X[bi][bi] = Dinv_bi.
+__global__ void __launch_bounds__(KR_NT) k_trinv_row(const double* L, int n, int bi, const double* Dinv, double* X,
+                                                     const int* ok) {
+  __shared__ double TA[KR_NB][KR_LDT], TB[KR_NB][KR_LDT];
+  if (!*ok) return;
+  const int bj = blockIdx.x, p = threadIdx.x / 8, q0 = 4 * (threadIdx.x % 8);
+  const double* Dg = Dinv + (size_t)bi * KR_NB * KR_NB;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (bj == bi) {
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[b] = Dg[p * KR_NB + q0 + b];
+  } else {
+    for (int k = bj; k < bi; k++) {
+      __syncthreads();
+      kr_load_tile(TA, L, n, bi, k);
+      kr_load_tile(TB, X, n, k, bj);
+      __syncthreads();
+      kr_tile_mac<false>(TA, TB, acc);
+    }
+    // X[bi][bj] = -Dinv_bi acc (acc through shared memory)
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < 4; b++) TB[p][q0 + b] = acc[b];
+    for (int e = threadIdx.x; e < KR_NB * KR_NB; e += KR_NT) TA[e / KR_NB][e % KR_NB] = Dg[e];
+    __syncthreads();
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    kr_tile_mac<false>(TA, TB, r);
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[b] = -r[b];
+  }
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int gi = bi * KR_NB + p, gj = bj * KR_NB + q0 + b;
+    if (gi < n && gj < n) X[(size_t)gi * n + gj] = acc[b];
+  }
+}
+
+// S[ba][bb] = sum_{k >= ba} X[k][ba]^T X[k][bb] for the tile (ba >= bb) of this CTA, stored with its transpose.
+__global__ void __launch_bounds__(KR_NT) k_trinv_gram(const double* X, int n, double* S, const int* ok) {
+  __shared__ double TA[KR_NB][KR_LDT], TB[KR_NB][KR_LDT];
+  if (!*ok) return;
+  int ba, bb;
+  kr_tri_tile(blockIdx.x, &ba, &bb);
+  const int nb = (n + KR_NB - 1) / KR_NB, p = threadIdx.x / 8, q0 = 4 * (threadIdx.x % 8);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k = ba; k < nb; k++) {
+    __syncthreads();
+    kr_load_tile(TA, X, n, k, ba);
+    kr_load_tile(TB, X, n, k, bb);
+    __syncthreads();
+    kr_tile_mac<true>(TA, TB, acc);
+  }
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int gi = ba * KR_NB + p, gj = bb * KR_NB + q0 + b;
+    if (gi < n && gj < n) {
+      S[(size_t)gi * n + gj] = acc[b];
+      S[(size_t)gj * n + gi] = acc[b];
+    }
+  }
 }
 
 __global__ void __launch_bounds__(KR_NT) k_kriging_rows(KrigArgs a) {

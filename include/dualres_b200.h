@@ -341,6 +341,10 @@ int dr_debug_bounded_wait(int device, double limit_ms, int* gave_up, double* wai
 int dr_debug_tc_layout(int n_rows, int n_cols, const int* rowptr, const int* col, const float* val,
                        const uint32_t* keys, int g_max, float* dense, int64_t* stats);
 int dr_debug_time_kernel(dr_chainset* cs, int which, int step, int reps, double* avg_ms, double* algo_bytes);
+/* Bytes in use and the high-water mark of the library's device memory pool (every stream-ordered allocation of
+ * the library comes from it; it keeps freed memory for reuse).  reset_high != 0 first resets the high-water mark
+ * to the bytes in use.  No reference counterpart (allocation accounting for tests). */
+int dr_debug_pool_usage(int device, int reset_high, uint64_t* used, uint64_t* high);
 /* Device kernel launches made by this thread since the last call (for launch accounting). */
 int64_t dr_kernel_launches(int reset);
 const char* dr_last_error(void);

@@ -3,8 +3,10 @@ memory, for callers that may not call cudaMalloc/cudaFree (device memory owned b
 another allocator, or a loop that has stopped allocating).  Its scratch is one
 library-owned device array, so two consecutive calls must both agree with the
 allocating entry point dr_log_posterior and with the FP64 oracle, and a call
-after the first must leave the device's free memory and the default memory
-pool's high-water mark where they were.  This file is collected last on purpose."""
+after the first must leave the device's free memory, the default memory pool's
+high-water mark and that of the library's own pool (from which every other
+library allocation comes) where they were.  This file is collected last on
+purpose."""
 import ctypes
 import os
 
@@ -115,13 +117,17 @@ def test_noalloc_allocates_nothing_on_the_32cubed_volume(oracle):
     torch.cuda.synchronize()
     mem.reset_high()
     before = mem.snapshot()
+    lib_before = d.api.pool_usage(0, reset_high=True)
     second = d.api.log_posterior_noalloc(data, dmu.data_ptr(), sh, ss)
     torch.cuda.synchronize()
     after = mem.snapshot()
+    lib_after = d.api.pool_usage(0)
     for lp, ll in (first, second):
         assert abs(lp / lp64 - 1) < TOL and abs(ll / ll64 - 1) < TOL, (lp, lp64, ll, ll64)
     assert after["free"] == before["free"], (before, after)
     assert after["used"] == before["used"] and after["high"] == before["used"], (before, after)
+    assert lib_before[0] > 0 and lib_after[0] == lib_before[0] and lib_after[1] == lib_before[0], (lib_before,
+                                                                                                  lib_after)
     assert torch.cuda.current_device() == 0
     data.close()
 
