@@ -484,7 +484,7 @@ static void kriging_solve_device(HostVolume& hv, int device, cudaStream_t st) {
       task_route[t] = route[order[t].second];
     }
     if (ntasks > 0) {
-      const size_t slot = (size_t)nmax * nmax + m + nmax + (m + 1) / 2 + 1;
+      const size_t slot = (size_t)nmax * (nmax + 1) / 2 + m + nmax + (m + 1) / 2 + 1;
       int grid = std::min(ntasks, 2 * dt.sms);
       const size_t budget = (size_t)2 << 30;  // scratch cap
       grid = std::max(1, std::min(grid, (int)(budget / (slot * sizeof(double)))));
@@ -1012,7 +1012,7 @@ static bool volume_tc(Volume* V) {
   const DeviceTables& dt = device_tables(V->device);
   if (!dt.tc || dv.n_s == 0 || hv.w_col.empty() || hv.wt_col.empty()) return false;
   const auto t0 = std::chrono::steady_clock::now();
-  TraceScope tr("tensor-core tiles: row keys + tile plans");
+  TraceScope tr("tensor-core tiles: row keys");
   CK(cudaSetDevice(V->device));
   auto coords = [&](int flat, int* x, int* y, int* z) {
     *x = flat % hv.E[0];
@@ -1021,6 +1021,7 @@ static bool volume_tc(Volume* V) {
   };
   // W's rows are ordered by the centroid of the data voxels each std-res voxel is kriged from, W^T's by voxel
   std::vector<uint32_t> kw(dv.n_s, 0), kt(dv.n_h, 0);
+#pragma omp parallel for schedule(static)
   for (int r = 0; r < dv.n_s; r++) {
     double sx = 0, sy = 0, sz = 0;
     const int n = hv.w_rowptr[r + 1] - hv.w_rowptr[r];
@@ -1033,11 +1034,13 @@ static bool volume_tc(Volume* V) {
     }
     if (n > 0) kw[r] = zorder_key((int)std::lround(sx / n), (int)std::lround(sy / n), (int)std::lround(sz / n));
   }
+#pragma omp parallel for schedule(static)
   for (int j = 0; j < dv.n_h; j++) {
     int x, y, z;
     coords(hv.d_flat[j], &x, &y, &z);
     kt[j] = zorder_key(x, y, z);
   }
+  tr.next("tensor-core tiles: tile plans");
   TcPlanHost pw, pt;
   if (!tc_plan(hv.w_rowptr, hv.w_col.data(), hv.w_col.size(), kw, dt.sms, &pw) ||
       !tc_plan(hv.wt_rowptr, hv.wt_col.data(), hv.wt_col.size(), kt, dt.sms, &pt))

@@ -616,7 +616,7 @@ bool tc_plan(const std::vector<int>& rowptr, const int* col, size_t nnz, const s
   P->chunks = chunk_ptr[P->T];
   if (P->chunks * BLK > 0x7fffffffLL) return false;
   P->chunk_cols.assign((size_t)P->chunks * KC, -1);
-  P->dest.assign(nnz, -1);
+  P->dest.resize(nnz);
 #pragma omp parallel
   {
     std::vector<int> pos(n_cols, 0);

@@ -114,7 +114,8 @@ int kriging_build(const float* hr, int nx, int ny, int nz, const float* Qhr, con
 struct TcPlanHost {
   int T = 0, G = 0;
   long long chunks = 0;
-  std::vector<int> tile_rows, chunk_cols, segs, cta_seg_ptr, tile_seg_ptr, dest;
+  std::vector<int> tile_rows, chunk_cols, segs, cta_seg_ptr, tile_seg_ptr;
+  fill_vector<int> dest;  // every entry is written by the plan
 };
 // false when the blob would not be addressable with 32-bit positions.
 bool tc_plan(const std::vector<int>& rowptr, const int* col, size_t nnz, const std::vector<uint32_t>& key, int g_max,

@@ -12,7 +12,7 @@
 // inverse, then a 64 x 64-tiled rank-32 update of the trailing matrix.  One
 // CTA solves one row at a time, taking rows from a shared counter in
 // descending order of cost; its matrix lives in a private slot of global
-// memory (L2-resident for the sizes that occur).  A row whose pivot is not
+// memory, the lower triangle packed by rows.  A row whose pivot is not
 // positive is reported, and the caller solves that row by QR as the host
 // builder does.
 #pragma once
@@ -40,7 +40,7 @@ struct KrigArgs {
   int* counter;               // next task
   double* w;                  // output weights, indexed like pid
   int* status;                // per row: KR_OK, KR_DROP (weight sum NaN), KR_NOT_SPD
-  double* scratch;            // per CTA: nmax^2 (matrix) + m (v) + nmax (t) doubles, then m ints
+  double* scratch;            // per CTA: nmax (nmax + 1) / 2 (packed matrix) + m (v) + nmax (t) doubles, then m ints
   size_t slot;                // doubles per CTA slot
   int nmax;
 };
@@ -109,20 +109,23 @@ __device__ bool kr_factor_diag(double (*D)[KR_LDT], double (*Di)[KR_LDT], int& f
 }
 __device__ bool kr_factor_diag(KrigSmem& sm, int kb) { return kr_factor_diag(sm.D, sm.Di, sm.flag, kb); }
 
-// In-place Cholesky M = L L^T of the n x n matrix (row-major, lower triangle read and written).
+// Position of (i, j), j <= i, in a lower triangle packed by rows: row i starts at i (i + 1) / 2.
+__device__ __forceinline__ size_t kr_at(int i, int j) { return (size_t)i * (i + 1) / 2 + j; }
+
+// In-place Cholesky M = L L^T of the n x n matrix (lower triangle, packed by rows: kr_at).
 __device__ bool kr_cholesky(double* M, int n, KrigSmem& sm) {
   const int tid = threadIdx.x;
   for (int k0 = 0; k0 < n; k0 += KR_NB) {
     const int kb = min(KR_NB, n - k0);
     for (int e = tid; e < kb * kb; e += KR_NT) {
       const int i = e / kb, j = e % kb;
-      sm.D[i][j] = j <= i ? M[(size_t)(k0 + i) * n + k0 + j] : 0.0;
+      sm.D[i][j] = j <= i ? M[kr_at(k0 + i, k0 + j)] : 0.0;
     }
     __syncthreads();
     if (!kr_factor_diag(sm, kb)) return false;
     for (int e = tid; e < kb * kb; e += KR_NT) {
       const int i = e / kb, j = e % kb;
-      if (j <= i) M[(size_t)(k0 + i) * n + k0 + j] = sm.D[i][j];
+      if (j <= i) M[kr_at(k0 + i, k0 + j)] = sm.D[i][j];
     }
     const int r0 = k0 + kb;
     // panel: L[i, k0:k0+kb] = A[i, k0:k0+kb] Di^T, in chunks of KR_TILE rows
@@ -131,14 +134,14 @@ __device__ bool kr_cholesky(double* M, int n, KrigSmem& sm) {
       __syncthreads();
       for (int e = tid; e < ch * kb; e += KR_NT) {
         const int i = e / kb, l = e % kb;
-        sm.PA[i][l] = M[(size_t)(c0 + i) * n + k0 + l];
+        sm.PA[i][l] = M[kr_at(c0 + i, k0 + l)];
       }
       __syncthreads();
       for (int e = tid; e < ch * kb; e += KR_NT) {
         const int i = e / kb, j = e % kb;
         double s = 0.0;
         for (int l = 0; l <= j; l++) s += sm.PA[i][l] * sm.Di[j][l];
-        M[(size_t)(c0 + i) * n + k0 + j] = s;
+        M[kr_at(c0 + i, k0 + j)] = s;
       }
     }
     __syncthreads();
@@ -148,14 +151,14 @@ __device__ bool kr_cholesky(double* M, int n, KrigSmem& sm) {
       const int i0 = r0 + tI * KR_TILE, ni = min(KR_TILE, n - i0);
       for (int e = tid; e < ni * kb; e += KR_NT) {
         const int i = e / kb, l = e % kb;
-        sm.PA[i][l] = M[(size_t)(i0 + i) * n + k0 + l];
+        sm.PA[i][l] = M[kr_at(i0 + i, k0 + l)];
       }
       for (int tJ = 0; tJ <= tI; tJ++) {
         const int j0 = r0 + tJ * KR_TILE, nj = min(KR_TILE, n - j0);
         __syncthreads();
         for (int e = tid; e < nj * kb; e += KR_NT) {
           const int j = e / kb, l = e % kb;
-          sm.PB[j][l] = M[(size_t)(j0 + j) * n + k0 + l];
+          sm.PB[j][l] = M[kr_at(j0 + j, k0 + l)];
         }
         __syncthreads();
         // each thread: a 4 x 4 micro-tile (rows ty*4.., cols tx*4..) of the 64 x 64 tile
@@ -184,7 +187,7 @@ __device__ bool kr_cholesky(double* M, int n, KrigSmem& sm) {
           for (int b = 0; b < 4; b++) {
             const int j = tx * 4 + b;
             if (j >= nj || j0 + j > i0 + i) continue;
-            M[(size_t)(i0 + i) * n + j0 + j] -= acc[a][b];
+            M[kr_at(i0 + i, j0 + j)] -= acc[a][b];
           }
         }
       }
@@ -203,7 +206,7 @@ __device__ void kr_solve(const double* L, int n, double* b, KrigSmem& sm) {
     __syncthreads();
     for (int e = tid; e < kb * kb; e += KR_NT) {
       const int i = e / kb, j = e % kb;
-      sm.D[i][j] = j <= i ? L[(size_t)(k0 + i) * n + k0 + j] : 0.0;
+      sm.D[i][j] = j <= i ? L[kr_at(k0 + i, k0 + j)] : 0.0;
     }
     __syncthreads();
     if (tid < kb) {
@@ -229,7 +232,7 @@ __device__ void kr_solve(const double* L, int n, double* b, KrigSmem& sm) {
     if (tid < kb) b[k0 + tid] = sm.PA[0][tid];
     __syncthreads();
     for (int i = k0 + kb + tid; i < n; i += KR_NT) {
-      const double* Li = L + (size_t)i * n + k0;
+      const double* Li = L + kr_at(i, k0);
       double s = 0.0;
       for (int l = 0; l < kb; l++) s += Li[l] * sm.PA[0][l];
       b[i] -= s;
@@ -249,7 +252,7 @@ __device__ void kr_solve(const double* L, int n, double* b, KrigSmem& sm) {
     __syncthreads();
     for (int i = tid; i < k0; i += KR_NT) {
       double s = 0.0;
-      for (int l = 0; l < kb; l++) s += L[(size_t)(k0 + l) * n + i] * sm.PA[0][l];
+      for (int l = 0; l < kb; l++) s += L[kr_at(k0 + l, i)] * sm.PA[0][l];
       b[i] -= s;
     }
   }
@@ -467,7 +470,7 @@ __global__ void __launch_bounds__(KR_NT) k_kriging_rows(KrigArgs a) {
   KrigSmem& sm = *reinterpret_cast<KrigSmem*>(kr_smraw);
   const int tid = threadIdx.x;
   double* M = a.scratch + (size_t)blockIdx.x * a.slot;
-  double* v = M + (size_t)a.nmax * a.nmax;
+  double* v = M + kr_at(a.nmax, 0);  // the packed lower triangle of an nmax x nmax matrix
   double* t = v + a.m;
   int* ids = reinterpret_cast<int*>(t + a.nmax);
   const int m = a.m;
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(KR_NT) k_kriging_rows(KrigArgs a) {
       const int n = cnt;
       for (size_t e = tid; e < (size_t)n * n; e += KR_NT) {
         const int i = (int)(e / n), j = (int)(e % n);
-        if (j <= i) M[e] = a.K[(size_t)pid[i] * m + pid[j]];
+        if (j <= i) M[kr_at(i, j)] = a.K[(size_t)pid[i] * m + pid[j]];
       }
       for (int i = tid; i < n; i += KR_NT) x[i] = k[i];
       __syncthreads();
@@ -517,7 +520,7 @@ __global__ void __launch_bounds__(KR_NT) k_kriging_rows(KrigArgs a) {
         kr_rows_dot(a.S, m, ids, nb, v, t);  // t = [S v0]_B
         for (size_t e = tid; e < (size_t)nb * nb; e += KR_NT) {
           const int i = (int)(e / nb), j = (int)(e % nb);
-          if (j <= i) M[e] = a.S[(size_t)ids[i] * m + ids[j]];
+          if (j <= i) M[kr_at(i, j)] = a.S[(size_t)ids[i] * m + ids[j]];
         }
         __syncthreads();
         ok = kr_cholesky(M, nb, sm);
