@@ -827,7 +827,17 @@ static void launch_spmv(Chainset* S, int step, int sel, int chain_only, bool w) 
   else launch_spmv_dc(S->vol->dv, S->dc, S->NR, step, sel, chain_only, w, S->stream);
 }
 
+// The update kernels' L2 prefetch of their state (XF_L2_PREFETCH); DRB_L2_PREFETCH=0 turns it off.
+static int l2_prefetch_flag() {
+  static const int f = [] {
+    const char* e = std::getenv("DRB_L2_PREFETCH");
+    return (e && std::string(e) == "0") ? 0 : (int)XF_L2_PREFETCH;
+  }();
+  return f;
+}
+
 static void launch_xline(Chainset* S, int step, int flags) {
+  flags |= l2_prefetch_flag();
   const DevVolume& v = S->vol->dv;
   if (cdiv_i((long long)v.E1 * v.E2, TILE_LINES) > S->dc.maxblk)
     throw Error(DR_ERR_STATE, "partial-sum buffer smaller than the x-line block count");
@@ -851,6 +861,7 @@ static void launch_xline(Chainset* S, int step, int flags) {
 
 template <int E, bool PF>
 static void launch_plane_t(Chainset* S, int step, int flags) {
+  flags |= l2_prefetch_flag();
   const DevVolume& v = S->vol->dv;
   const dim3 grid(v.E2, S->C);
   const size_t smem = (size_t)plane_layout(E, PlaneGeom<E>::SIZE, PF).total;

@@ -137,6 +137,8 @@ enum PassPro : int { PRO_LOAD = 0, PRO_DATAGRAD = 1 };
 enum PassEpi : int { EPI_STORE = 0, EPI_GATHER = 1 };
 
 // x-line kernel flags
-enum XFlags : int { XF_FIXED_MOMENTUM = 1, XF_WRITE_Q_LAST = 2 };
+// XF_L2_PREFETCH: the update kernels ask L2 for their blocks' state (u, q, 1/lambda) at entry, so that its DRAM
+// latency overlaps the inverse transforms.
+enum XFlags : int { XF_FIXED_MOMENTUM = 1, XF_WRITE_Q_LAST = 2, XF_L2_PREFETCH = 4 };
 
 }  // namespace drb

@@ -265,6 +265,12 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
   float2* Qc = ch.Q + (long long)c * N;
   float2* T1 = ch.T1 + (long long)c * ch.t1_stride;
   const int bx = v.bx;
+  if ((flags & XF_L2_PREFETCH) && threadIdx.x == 0 && E0 >= 4) {
+    const bool draw = first && !(flags & XF_FIXED_MOMENTUM);
+    bulk_prefetch_l2(Usrc + lam0 * E0, (uint32_t)nl * E0 * 8);
+    if (!draw) bulk_prefetch_l2(Qc + lam0 * E0, (uint32_t)nl * E0 * 8);
+    bulk_prefetch_l2(v.sinv + lam0 * E0, (uint32_t)nl * E0 * 4);
+  }
 
   for (int e = threadIdx.x; e < TL * E0; e += NT) {
     const int l = e / E0, x = e % E0;
@@ -607,6 +613,11 @@ __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETC
   const float2* srcU = Usrc;
   const float2* srcQ = Qc;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
+  if (!PREFETCH && (flags & XF_L2_PREFETCH) && tid == 0) {
+    bulk_prefetch_l2(Usrc, E * E * 8);
+    if (need_q) bulk_prefetch_l2(Qc, E * E * 8);
+    bulk_prefetch_l2(Sg, E * E * 4);
+  }
   if constexpr (PREFETCH) {
     // U and q only: 1/lambda is one array shared by every chain and stays in L2
     srcU = reinterpret_cast<const float2*>(smraw + Ly.u_off);

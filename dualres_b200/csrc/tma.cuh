@@ -82,6 +82,12 @@ __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// Asks L2 to fetch [src, src + bytes) from global memory ahead of its use; nothing to wait for (16-byte aligned
+// address, size a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // Shared memory of every committed store may be reused.
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
