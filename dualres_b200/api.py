@@ -139,6 +139,7 @@ def _declare(L):
     L.dr_chainset_create.argtypes = [vp, C.c_int, C.POINTER(HmcOpts), C.POINTER(vp)]
     L.dr_chainset_config_get.argtypes = [vp, _ip, _ip, _dp, _ip]
     L.dr_chainset_ztile_get.argtypes = [vp, _ip]
+    L.dr_chainset_fft_plan_get.argtypes = [vp, _ip]
     L.dr_chainset_destroy.argtypes = [vp]
     L.dr_chainset_destroy.restype = None
     L.dr_step.argtypes = [vp, C.c_int]
@@ -375,14 +376,17 @@ class MultiResParameters:
     PATHS = ("plane", "plane+prefetch", "lines")
 
     def config(self):
-        """The chain set's update path, kriging-product blocks per SM, tuned iteration time (ms, 0 if untuned) and
-        whether the kriging products run on the tensor cores."""
+        """The chain set's update path, kriging-product blocks per SM, tuned iteration time (ms, 0 if untuned),
+        whether the kriging products run on the tensor cores, the z passes' tile shape and the radix plan of the z
+        (and x-line) transforms."""
         p, g, ms, tc = C.c_int(0), C.c_int(0), C.c_double(0), C.c_int(0)
         check(lib().dr_chainset_config_get(self.h, C.byref(p), C.byref(g), C.byref(ms), C.byref(tc)))
-        zt = C.c_int(0)
+        zt, fp = C.c_int(0), C.c_int(0)
         check(lib().dr_chainset_ztile_get(self.h, C.byref(zt)))
+        check(lib().dr_chainset_fft_plan_get(self.h, C.byref(fp)))
         return dict(path=self.PATHS[p.value], blocks_per_sm=g.value, tuned_ms=ms.value,
-                    tensor_products=bool(tc.value), tma_row_gather=tc.value == 2, z_tile_chains=zt.value)
+                    tensor_products=bool(tc.value), tma_row_gather=tc.value == 2, z_tile_chains=zt.value,
+                    fft_plan=fp.value)
 
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))

@@ -129,6 +129,17 @@ static void set_pass_attrs() {
     CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_xline<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if constexpr (N == 64 || N == 128 || N == 256) {  // the alternative radix plan (fft_smem PLAN 1)
+      CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 1, 1>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 1, 1>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      CK(cudaFuncSetAttribute(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8, 1>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      CK(cudaFuncSetAttribute(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8, 1>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      CK(cudaFuncSetAttribute(k_xline<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    }
   }
 }
 
@@ -235,11 +246,18 @@ static void launch_pass_n(int dir, int pro, int epi, const PassArgs& a, const De
     // set's tuning chose tiles of 32 lines of one chain (ch.ztile)
     const bool grouped = a.chain_only < 0 && nch >= 8 && a.B > 1 && ch.ztile != 1;
     const dim3 ggrid(cdiv_i((long long)a.A * a.B, TILE_LINES / 8), cdiv_i(nch, 8));
+    // the radix plan the chain set's tuning chose (ch.fftplan) for the lengths that have two
+    constexpr bool two_plans = N == 64 || N == 128 || N == 256;
+    const bool alt = two_plans && (ch.fftplan & (dir > 0 ? FP_ZINV : FP_ZFWD)) != 0;
     if (dir > 0 && pro == PRO_DATAGRAD && epi == EPI_STORE) {
-      if (grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
+      if (alt && grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8, 1><<<ggrid, block, smem, s>>>(a, v, ch, tw);
+      else if (alt) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 1, 1><<<grid, block, smem, s>>>(a, v, ch, tw);
+      else if (grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
       else k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
     } else if (dir < 0 && pro == PRO_LOAD && epi == EPI_GATHER) {
-      if (grouped) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
+      if (alt && grouped) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8, 1><<<ggrid, block, smem, s>>>(a, v, ch, tw);
+      else if (alt) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 1, 1><<<grid, block, smem, s>>>(a, v, ch, tw);
+      else if (grouped) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
       else k_pass<N, -1, PRO_LOAD, EPI_GATHER, C><<<grid, block, smem, s>>>(a, v, ch, tw);
     } else {
       throw Error(DR_ERR_INVALID, "unsupported pass combination");
@@ -850,9 +868,18 @@ static void launch_xline(Chainset* S, int step, int flags) {
     case 8: k_xline<8><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
     case 16: k_xline<16><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
     case 32: k_xline<32><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 64: k_xline<64><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 128: k_xline<128><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 256: k_xline<256><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 64:
+      if (S->dc.fftplan & FP_XLINE) k_xline<64, 1><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      else k_xline<64><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      break;
+    case 128:
+      if (S->dc.fftplan & FP_XLINE) k_xline<128, 1><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      else k_xline<128><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      break;
+    case 256:
+      if (S->dc.fftplan & FP_XLINE) k_xline<256, 1><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      else k_xline<256><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      break;
     case 512: k_xline<512><<<grid, 512, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
     default: throw Error(DR_ERR_UNSUPPORTED, "E0 not supported");
   }
@@ -1131,6 +1158,7 @@ struct TuneChoice {
   int grid = 8;      // kriging-product blocks per SM (CSR products)
   double ms = 0.0;   // measured milliseconds per iteration
   int tc = 0;        // 1: kriging products on the tensor cores
+  int fftplan = 0;   // FP_* bits: transforms on the second radix plan (fft_smem PLAN 1) for 64, 128, 256 points
 };
 
 static bool autotune_enabled() {
@@ -1192,7 +1220,8 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
     // a candidate that cannot be built or run (for instance out of device memory beside the caller's other
     // allocations) is skipped; if none can, the default configuration is used untuned
     const TraceScope tr("tuning candidate path " + std::to_string(c.path) + " tc " + std::to_string(c.tc) +
-                        " grid " + std::to_string(c.grid) + " ztile " + std::to_string(c.ztile));
+                        " grid " + std::to_string(c.grid) + " ztile " + std::to_string(c.ztile) + " fft plan " +
+                        std::to_string(c.fftplan));
     try {
       auto T = std::make_unique<Chainset>();
       chainset_build(T.get(), V, C, &to, &c);
@@ -1236,6 +1265,15 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
     if (C >= 8) {
       TuneChoice t = best;
       t.ztile = 1;
+      try_candidate(t);
+    }
+    // the second radix plan, one transform at a time on the best configuration so far: the inverse and the forward
+    // z passes, and the x transforms of the x-line kernel, where their length has two plans
+    auto two_plans = [](int n) { return n == 64 || n == 128 || n == 256; };
+    for (int bit : {(int)FP_ZINV, (int)FP_ZFWD, (int)FP_XLINE}) {
+      if (bit == FP_XLINE ? !(best.path == 2 && two_plans(v.E0)) : !two_plans(v.E2)) continue;
+      TuneChoice t = best;
+      t.fftplan |= bit;
       try_candidate(t);
     }
   }
@@ -1290,11 +1328,14 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   if (const char* e = std::getenv("DRB_TC_PRODUCTS")) tc = std::atoi(e) != 0;
   int ztile = 8;
   if (const char* e = std::getenv("DRB_ZTILE")) ztile = std::atoi(e) == 1 ? 1 : 8;
+  int fftplan = 0;
+  if (const char* e = std::getenv("DRB_FFT_PLAN")) fftplan = std::atoi(e) & (FP_ZINV | FP_ZFWD | FP_XLINE);
   if (forced) {
     path = forced->path;
     grid = forced->grid;
     tc = forced->tc;
     ztile = forced->ztile;
+    fftplan = forced->fftplan;
   } else if (std::getenv("DRB_NO_PLANE")) {
     path = 2;
   } else if (std::getenv("DRB_PLANE_PREFETCH")) {
@@ -1304,6 +1345,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     path = t.path;
     grid = t.grid;
     if (!std::getenv("DRB_ZTILE")) ztile = t.ztile;
+    if (!std::getenv("DRB_FFT_PLAN")) fftplan = t.fftplan;
     if (!std::getenv("DRB_TC_PRODUCTS")) tc = t.tc;
     S->tuned_ms = t.ms;
   }
@@ -1353,6 +1395,7 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   ch.seed = o->seed;
   ch.chain0 = 0;
   ch.ztile = ztile;
+  ch.fftplan = fftplan;
   ch.err = S->alloc<int>(1);
   S->tmp = S->alloc<float2>(N);
   init_chain_states(S);
@@ -1717,6 +1760,13 @@ int dr_chainset_ztile_get(const dr_chainset* s, int* z_tile_chains) {
   API_BEGIN
   if (!s || !z_tile_chains) throw Error(DR_ERR_INVALID, "NULL argument");
   *z_tile_chains = s->C >= 8 && s->dc.ztile != 1 ? 8 : 1;
+  API_END
+}
+
+int dr_chainset_fft_plan_get(const dr_chainset* s, int* plan) {
+  API_BEGIN
+  if (!s || !plan) throw Error(DR_ERR_INVALID, "NULL argument");
+  *plan = s->dc.fftplan;
   API_END
 }
 

@@ -96,6 +96,7 @@ struct DevChains {
   int chain0;               // global id of chain 0 (RNG key component)
   int* err;                 // device error word: bounded waits that gave up
   int ztile;                // chains per z-pass tile with 8 or more chains: 8 (4 lines x 8 chains) or 1 (32 lines)
+  int fftplan;              // FP_* bits: the transforms that use the second radix plan of fft_smem (64, 128, 256 points)
 };
 
 // A kriging matrix (W or W^T) cut into dense tiles for the tensor-core
@@ -140,5 +141,7 @@ enum PassEpi : int { EPI_STORE = 0, EPI_GATHER = 1 };
 // XF_L2_PREFETCH: the update kernels ask L2 for their blocks' state (u, q, 1/lambda) at entry, so that its DRAM
 // latency overlaps the inverse transforms.
 enum XFlags : int { XF_FIXED_MOMENTUM = 1, XF_WRITE_Q_LAST = 2, XF_L2_PREFETCH = 4 };
+// Transforms that a chain set's tuning may switch to the second radix plan (fft_smem PLAN 1), one bit each.
+enum FftPlanBits : int { FP_ZINV = 1, FP_ZFWD = 2, FP_XLINE = 4 };
 
 }  // namespace drb

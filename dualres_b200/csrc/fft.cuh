@@ -212,7 +212,9 @@ __device__ __forceinline__ void fft_smem_warp(C* sm, int ls, int es, int nlines,
 // Full FFT of nlines lines of length N held in shared memory.  MAXLINES and
 // NTHR bound the per-thread butterfly count at compile time.  The caller must
 // have synchronised after filling the tile; on return the tile is complete.
-template <int N, int DIR, int MAXLINES, int NTHR, class C>
+// PLAN picks the radix plan for N = 64, 128 and 256: 0 (8 x 8, 16 x 8,
+// 16 x 16) or 1 (16 x 4, 8 x 16, 8 x 8 x 4); a chain set's tuner times both.
+template <int N, int DIR, int MAXLINES, int NTHR, class C, int PLAN = 0>
 __device__ __forceinline__ void fft_smem(C* sm, int ls, int es, int nlines, const C* __restrict__ tw) {
   const int tid = threadIdx.x;
   if constexpr (N == 1) {
@@ -222,12 +224,22 @@ __device__ __forceinline__ void fft_smem(C* sm, int ls, int es, int nlines, cons
   } else if constexpr (N == 32) {
     fft_stage<32, 8, 1, DIR, cdiv(4 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
     fft_stage<32, 4, 8, DIR, cdiv(8 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+  } else if constexpr (N == 64 && PLAN == 1) {
+    fft_stage<64, 16, 1, DIR, cdiv(4 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+    fft_stage<64, 4, 16, DIR, cdiv(16 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
   } else if constexpr (N == 64) {
     fft_stage<64, 8, 1, DIR, cdiv(8 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
     fft_stage<64, 8, 8, DIR, cdiv(8 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+  } else if constexpr (N == 128 && PLAN == 1) {
+    fft_stage<128, 8, 1, DIR, cdiv(16 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+    fft_stage<128, 16, 8, DIR, cdiv(8 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
   } else if constexpr (N == 128) {
     fft_stage<128, 16, 1, DIR, cdiv(8 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
     fft_stage<128, 8, 16, DIR, cdiv(16 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+  } else if constexpr (N == 256 && PLAN == 1) {
+    fft_stage<256, 8, 1, DIR, cdiv(32 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+    fft_stage<256, 8, 8, DIR, cdiv(32 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
+    fft_stage<256, 4, 64, DIR, cdiv(64 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
   } else if constexpr (N == 256) {
     fft_stage<256, 16, 1, DIR, cdiv(16 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);
     fft_stage<256, 16, 16, DIR, cdiv(16 * MAXLINES, NTHR), C>(sm, ls, es, nlines, tw, tid, NTHR);

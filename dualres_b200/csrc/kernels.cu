@@ -105,7 +105,7 @@ template <int N> struct PassCfg {
   static constexpr int NT = N >= 512 ? 512 : 256;
 };
 
-template <int N, int DIR, int PRO, int EPI, class C, int CPB = 1>
+template <int N, int DIR, int PRO, int EPI, class C, int CPB = 1, int PLAN = 0>
 __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v, DevChains ch, const C* __restrict__ tw) {
   constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = PassCfg<N>::NT, LPC = TILE_LINES / CPB;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
     }
   }
   __syncthreads();
-  fft_smem<N, DIR, TL, NT>(sm, 1, P, TL, tw + tw_offset(N));
+  fft_smem<N, DIR, TL, NT, C, PLAN>(sm, 1, P, TL, tw + tw_offset(N));
 
   const auto scale = (decltype(C().x))a.scale;
   auto store = [&](int l, int k) {
@@ -237,7 +237,7 @@ template <int E0> struct XCfg {
   static constexpr int MINB = E0 >= 512 ? 1 : (E0 == 256 ? 3 : 4);
 };
 
-template <int E0>
+template <int E0, int PLAN = 0>
 __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolume v, DevChains ch, int step, int flags,
                                                         const float2* __restrict__ tw) {
   constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = XCfg<E0>::NT;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
     sm[x * P + l] = val;
   }
   __syncthreads();
-  fft_smem<E0, +1, TL, NT>(sm, 1, P, TL, tw + tw_offset(E0));
+  fft_smem<E0, +1, TL, NT, float2, PLAN>(sm, 1, P, TL, tw + tw_offset(E0));
 
   const bool fixed = (flags & XF_FIXED_MOMENTUM) != 0;
   const bool write_q = !last || (flags & XF_WRITE_Q_LAST);
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
   }
   if (last) return;
   __syncthreads();
-  fft_smem<E0, -1, TL, NT>(sm, 1, P, TL, tw + tw_offset(E0));
+  fft_smem<E0, -1, TL, NT, float2, PLAN>(sm, 1, P, TL, tw + tw_offset(E0));
   for (int e = threadIdx.x; e < TL * bx; e += NT) {
     const int l = e / bx, x = e % bx;
     if (l < nl) T1[(lam0 + l) * bx + x] = sm[x * P + l];

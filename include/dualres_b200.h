@@ -176,6 +176,12 @@ int dr_chainset_config_get(const dr_chainset* cs, int* path, int* blocks_per_sm,
  * 8 for tiles of 4 lines x 8 chains, 1 for tiles of 32 lines of one chain (always 1 below 8 chains).  No reference
  * counterpart: the reference's FFTW plans have no tiles. */
 int dr_chainset_ztile_get(const dr_chainset* cs, int* z_tile_chains);
+/* The radix plans of the chain set's transforms of length 64, 128 and 256, chosen by the same tuning
+ * (DRB_FFT_PLAN=<bits> forces them): *plan has bit 1 set when the inverse z pass uses the second plan, bit 2 the
+ * forward z pass, bit 4 the x transforms of the x-line kernel (first plan: 8 x 8, 16 x 8, 16 x 16 radices; second:
+ * 16 x 4, 8 x 16, 8 x 8 x 4).  Replaces the per-size plans FFTW chooses when the reference plans its transforms
+ * (sized_fft.h:63-68). */
+int dr_chainset_fft_plan_get(const dr_chainset* cs, int* plan);
 
 /* ---- fixed-input evaluation (MultiResParameters public API) ------------- */
 /* Sets chain `chain` to mu (2N floats) and sigma^-2 = (s_hr, s_sr). */
