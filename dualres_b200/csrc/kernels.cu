@@ -164,21 +164,25 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
     }
     return val;
   };
-  // every load of a thread is issued before the first shared-memory store: PER independent loads in flight (tiles
-  // of a whole number of block-widths, up to 16 per thread)
+  // the loads of a thread are issued before its shared-memory stores, up to 16 at a time: PER independent loads in
+  // flight per round (tiles of a whole number of block-widths)
   constexpr int PER = TL * N / NT;
-  if constexpr (PER >= 1 && PER <= 16 && PER * NT == TL * N) {
-    C r[PER];
+  constexpr int CH = PER > 16 ? 16 : PER;
+  if constexpr (PER >= 1 && PER * NT == TL * N && PER % CH == 0) {
+#pragma unroll 1
+    for (int k0 = 0; k0 < PER; k0 += CH) {
+      C r[CH];
 #pragma unroll
-    for (int k = 0; k < PER; k++) {
-      const int e = threadIdx.x + k * NT;
-      r[k] = B == 1 ? load(e / N, e % N) : load(e % TL, e / TL);
-    }
+      for (int k = 0; k < CH; k++) {
+        const int e = threadIdx.x + (k0 + k) * NT;
+        r[k] = B == 1 ? load(e / N, e % N) : load(e % TL, e / TL);
+      }
 #pragma unroll
-    for (int k = 0; k < PER; k++) {
-      const int e = threadIdx.x + k * NT;
-      if (B == 1) sm[(e % N) * P + e / N] = r[k];
-      else sm[(e / TL) * P + e % TL] = r[k];
+      for (int k = 0; k < CH; k++) {
+        const int e = threadIdx.x + (k0 + k) * NT;
+        if (B == 1) sm[(e % N) * P + e / N] = r[k];
+        else sm[(e / TL) * P + e % TL] = r[k];
+      }
     }
   } else if (B == 1) {
     for (int e = threadIdx.x; e < TL * N; e += NT) {
