@@ -73,7 +73,7 @@ class HmcOpts(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_int64), ("max_active", C.c_int),
-                ("iterations_per_round", C.c_int), ("host_threads", C.c_int)]
+                ("iterations_per_round", C.c_int), ("host_threads", C.c_int), ("max_chains_in_flight", C.c_int)]
 
 
 class JobStatus(C.Structure):
@@ -568,13 +568,16 @@ class Server:
 
     ``submit`` copies the images and returns a job id at once; host set-up runs
     on worker threads, and a scheduler thread admits prepared jobs while their
-    device footprint fits ``hbm_budget_bytes``, advancing every resident job
-    ``iterations_per_round`` iterations per round on its own stream.  A job's
-    result does not depend on what else runs beside it."""
+    device footprint fits ``hbm_budget_bytes``, advancing resident jobs
+    ``iterations_per_round`` iterations per round on their own streams, the
+    earliest admitted first while their chains fit ``max_chains_in_flight``.
+    A job's result does not depend on what else runs beside it."""
 
-    def __init__(self, device=0, hbm_budget_bytes=0, max_active=64, iterations_per_round=8, host_threads=4):
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=64, iterations_per_round=8, host_threads=4,
+                 max_chains_in_flight=0):
         L = lib()
-        o = ServerOpts(device, int(hbm_budget_bytes), max_active, iterations_per_round, host_threads)
+        o = ServerOpts(device, int(hbm_budget_bytes), max_active, iterations_per_round, host_threads,
+                       int(max_chains_in_flight))
         h = C.c_void_p()
         check(L.dr_server_create(C.byref(o), C.byref(h)))
         self.h = h

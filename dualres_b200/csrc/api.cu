@@ -2442,26 +2442,39 @@ struct Server {
           device_q.push_back(j);
           cv_device.notify_one();
         }
-        while (!built_q.empty()) {
-          active.push_back(built_q.front());
-          built_q.pop_front();
+        if (!built_q.empty()) {
+          while (!built_q.empty()) {
+            active.push_back(built_q.front());
+            built_q.pop_front();
+          }
+          // submission order: the in-flight budget favours the earliest jobs
+          std::stable_sort(active.begin(), active.end(),
+                           [](const std::shared_ptr<Job>& a, const std::shared_ptr<Job>& b) { return a->id < b->id; });
         }
         peak_running = std::max(peak_running, (int)active.size());
       }
-      // advance every resident job by one round, finalise finished ones
+      // advance resident jobs by one round, earliest admitted first while their chains fit the in-flight budget (a
+      // job wider than the budget runs when nothing else is in flight); finalise finished ones
       bool launched = false, waiting = false;
+      int chains_in_flight = 0;
       for (auto& j : active) {
         try {
           if (j->in_flight) {
             const cudaError_t q = cudaEventQuery(j->cs->done_event);
             if (q == cudaErrorNotReady) {
               waiting = true;
+              chains_in_flight += j->C;
               continue;
             }
             if (q != cudaSuccess) throw Error(DR_ERR_CUDA, cudaGetErrorString(q));
             j->in_flight = false;
           }
           if (j->iters_launched < j->iters_total) {
+            if (chains_in_flight > 0 && chains_in_flight + j->C > o.max_chains_in_flight) {
+              waiting = true;
+              continue;
+            }
+            chains_in_flight += j->C;
             const int n = std::min(o.iterations_per_round, j->iters_total - j->iters_launched);
             launch_iterations(j->cs.get(), n);
             j->iters_launched += n;
@@ -2519,6 +2532,7 @@ int dr_server_create(const dr_server_opts* opts, dr_server** out) {
   sv->o = *opts;
   if (sv->o.max_active <= 0) sv->o.max_active = 64;
   if (sv->o.iterations_per_round <= 0) sv->o.iterations_per_round = 8;
+  if (sv->o.max_chains_in_flight <= 0) sv->o.max_chains_in_flight = 128;
   if (sv->o.host_threads <= 0) sv->o.host_threads = 4;
   if (sv->o.hbm_budget_bytes > 0) {
     sv->budget = sv->o.hbm_budget_bytes;

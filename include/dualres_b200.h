@@ -242,6 +242,8 @@ typedef struct {
   int max_active;              /* jobs resident on the device at once; <= 0: 64 */
   int iterations_per_round;    /* iterations each admitted job advances per round; <= 0: 8 */
   int host_threads;            /* set-up workers; <= 0: 4 */
+  int max_chains_in_flight;    /* chains of the resident jobs advanced at once, earliest admitted first (a job of
+                                  more chains runs when it is the only one); <= 0: 128 */
 } dr_server_opts;
 
 #define DR_JOB_QUEUED 0   /* waiting for host set-up */

@@ -50,6 +50,28 @@ def test_job_alone_equals_job_in_mix_and_direct_fit():
         assert r.latency_s >= r.queue_s >= 0
 
 
+def test_chain_budget_runs_the_earliest_jobs_first():
+    """With room for 3 chains in flight, the jobs of 2, 3 and 1 chains cannot all advance at once: the first and the
+    third run together, the second starts when the first has finished. Every result equals the one without a
+    budget (the order of the rounds does not enter a job's arithmetic)."""
+    jobs = _jobs()
+    with d.Server(iterations_per_round=2) as sv:
+        ids = [sv.submit_volume(v, h, c) for v, h, c in jobs]
+        sv.drain(600)
+        free = [sv.result(i) for i in ids]
+    with d.Server(iterations_per_round=2, max_chains_in_flight=3) as sv:
+        ids = [sv.submit_volume(v, h, c) for v, h, c in jobs]
+        sv.drain(600)
+        held = [sv.result(i) for i in ids]
+        st = [sv.status(i) for i in ids]
+    assert all(s.state == d.api.JOB_DONE for s in st)
+    assert st[1].finish_s > st[0].finish_s
+    for a, b in zip(free, held):
+        np.testing.assert_array_equal(a.mean, b.mean)
+        np.testing.assert_array_equal(a.var, b.var)
+        assert a.grad_evals == b.grad_evals
+
+
 def _submit_wait(sv, vol, hmc, C):
     j = sv.submit_volume(vol, hmc, C)
     sv.wait(j, 600)
