@@ -140,6 +140,9 @@ def _declare(L):
     L.dr_chainset_config_get.argtypes = [vp, _ip, _ip, _dp, _ip]
     L.dr_chainset_ztile_get.argtypes = [vp, _ip]
     L.dr_chainset_fft_plan_get.argtypes = [vp, _ip]
+    L.dr_chainset_checkpoint_size.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.dr_chainset_checkpoint_save.argtypes = [vp, vp, C.c_int64]
+    L.dr_chainset_checkpoint_restore.argtypes = [vp, vp, C.c_int64]
     L.dr_chainset_destroy.argtypes = [vp]
     L.dr_chainset_destroy.restype = None
     L.dr_step.argtypes = [vp, C.c_int]
@@ -390,6 +393,19 @@ class MultiResParameters:
 
     def update(self, iterations=1):
         check(lib().dr_step(self.h, iterations))
+
+    def checkpoint(self):
+        """The chain set's sampler state as bytes (dr_chainset_checkpoint_save)."""
+        n = C.c_int64(0)
+        check(lib().dr_chainset_checkpoint_size(self.h, C.byref(n)))
+        buf = np.zeros(n.value, np.uint8)
+        check(lib().dr_chainset_checkpoint_save(self.h, _ptr(buf), n.value))
+        return buf.tobytes()
+
+    def restore(self, state):
+        """Continue from a checkpoint of a chain set of the same volume, options and chain count."""
+        buf = np.frombuffer(state, np.uint8).copy()
+        check(lib().dr_chainset_checkpoint_restore(self.h, _ptr(buf), len(buf)))
 
     def update_timed(self, iterations=1):
         """Advance and return the device time (ms, CUDA events on the library's stream)."""

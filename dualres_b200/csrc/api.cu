@@ -1883,6 +1883,115 @@ int dr_set_state(dr_chainset* s, int chain, const float* mu, float s_hr, float s
   API_END
 }
 
+// Checkpoint layout: a header of eight int64 {magic, version, C, N, n_h, n_o, Cp, nsave_stored}, then per chain the
+// accepted spectral state (N float2), mu_D [2][n_h][Cp] and mu_O [2][n_o][Cp] floats, the ChainState array, the
+// summary sums s1, s2, sa [n_o][Cp] doubles, and with stored samples the samples [nsave][n_o][Cp] floats and the
+// sample records [nsave][C][3] doubles.
+struct CheckpointShape {
+  int64_t C, N, n_h, n_o, Cp, nsave;  // nsave: saved-sample capacity when samples are stored, else 0
+  int64_t bytes() const {
+    const int64_t no = std::max<int64_t>(n_o, 1);
+    int64_t b = 8 * (int64_t)sizeof(int64_t);
+    b += C * N * (int64_t)sizeof(float2);
+    b += 2 * n_h * Cp * (int64_t)sizeof(float) + 2 * no * Cp * (int64_t)sizeof(float);
+    b += C * (int64_t)sizeof(ChainState);
+    b += 3 * no * Cp * (int64_t)sizeof(double);
+    if (nsave > 0) b += nsave * no * Cp * (int64_t)sizeof(float) + nsave * C * 3 * (int64_t)sizeof(double);
+    return b;
+  }
+};
+static constexpr int64_t CKPT_MAGIC = 0x44524232434b5054LL, CKPT_VERSION = 1;
+
+static CheckpointShape checkpoint_shape(const Chainset* s) {
+  const DevVolume& v = s->vol->dv;
+  const int64_t nsave = s->opts.store_samples ? std::max(s->opts.nsave, 1) : 0;
+  return CheckpointShape{s->C, v.N, v.n_h, v.n_o, s->dc.Cp, nsave};
+}
+
+// Copies between the chain set's device state and the checkpoint buffer (to_host: save; else restore).
+static void checkpoint_copy(Chainset* s, unsigned char* buf, bool to_host) {
+  const CheckpointShape sh = checkpoint_shape(s);
+  const DevChains& ch = s->dc;
+  const int64_t no = std::max<int64_t>(sh.n_o, 1);
+  cudaStream_t st = s->stream;
+  const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice;
+  auto copy = [&](void* dev, size_t bytes, size_t& off) {
+    if (bytes == 0) return;
+    if (to_host) CK(cudaMemcpyAsync(buf + off, dev, bytes, kind, st));
+    else CK(cudaMemcpyAsync(dev, buf + off, bytes, kind, st));
+    off += bytes;
+  };
+  size_t off = 8 * sizeof(int64_t);
+  // the chain states first: on restore they say which half of U is each chain's accepted state
+  std::vector<ChainState> states(sh.C);
+  const size_t u_off = off;
+  off += (size_t)sh.C * sh.N * sizeof(float2);
+  const size_t mu_off = off;
+  off += (size_t)(2 * sh.n_h * sh.Cp + 2 * no * sh.Cp) * sizeof(float);
+  if (to_host) {
+    read_states(s, &states);
+    std::memcpy(buf + off, states.data(), sizeof(ChainState) * sh.C);
+  } else {
+    std::memcpy(states.data(), buf + off, sizeof(ChainState) * sh.C);
+    write_states(s, states);
+  }
+  const size_t st_end = off + sizeof(ChainState) * sh.C;
+  size_t o = u_off;
+  for (int c = 0; c < sh.C; c++)
+    copy(ch.U + ((int64_t)c * 2 + (states[c].acc & 1)) * sh.N, sizeof(float2) * sh.N, o);
+  o = mu_off;
+  copy(ch.muD, sizeof(float) * 2 * sh.n_h * sh.Cp, o);
+  copy(ch.muO, sizeof(float) * 2 * no * sh.Cp, o);
+  o = st_end;
+  copy(ch.s1, sizeof(double) * no * sh.Cp, o);
+  copy(ch.s2, sizeof(double) * no * sh.Cp, o);
+  copy(ch.sa, sizeof(double) * no * sh.Cp, o);
+  if (sh.nsave > 0) {
+    copy(ch.samples, sizeof(float) * sh.nsave * no * sh.Cp, o);
+    copy(ch.save_rec, sizeof(double) * sh.nsave * sh.C * 3, o);
+  }
+  CK(cudaStreamSynchronize(st));
+  if ((int64_t)o != sh.bytes()) throw Error(DR_ERR_STATE, "checkpoint layout mismatch");
+}
+
+int dr_chainset_checkpoint_size(const dr_chainset* s, int64_t* bytes) {
+  API_BEGIN
+  if (!s || !bytes) throw Error(DR_ERR_INVALID, "NULL argument");
+  *bytes = checkpoint_shape(s).bytes();
+  API_END
+}
+
+int dr_chainset_checkpoint_save(dr_chainset* s, void* buf, int64_t bytes) {
+  API_BEGIN
+  if (!s || !buf) throw Error(DR_ERR_INVALID, "NULL argument");
+  const CheckpointShape sh = checkpoint_shape(s);
+  if (bytes < sh.bytes()) throw Error(DR_ERR_INVALID, "checkpoint buffer too small");
+  CK(cudaSetDevice(s->vol->device));
+  auto* b = static_cast<unsigned char*>(buf);
+  const int64_t hdr[8] = {CKPT_MAGIC, CKPT_VERSION, sh.C, sh.N, sh.n_h, sh.n_o, sh.Cp, sh.nsave};
+  std::memcpy(b, hdr, sizeof(hdr));
+  checkpoint_copy(s, b, true);
+  API_END
+}
+
+int dr_chainset_checkpoint_restore(dr_chainset* s, const void* buf, int64_t bytes) {
+  API_BEGIN
+  if (!s || !buf) throw Error(DR_ERR_INVALID, "NULL argument");
+  const CheckpointShape sh = checkpoint_shape(s);
+  if (bytes < 8 * (int64_t)sizeof(int64_t)) throw Error(DR_ERR_INVALID, "checkpoint buffer too small");
+  int64_t hdr[8];
+  std::memcpy(hdr, buf, sizeof(hdr));
+  if (hdr[0] != CKPT_MAGIC || hdr[1] != CKPT_VERSION) throw Error(DR_ERR_INVALID, "not a chain-set checkpoint");
+  const int64_t want[6] = {sh.C, sh.N, sh.n_h, sh.n_o, sh.Cp, sh.nsave};
+  for (int i = 0; i < 6; i++)
+    if (hdr[2 + i] != want[i])
+      throw Error(DR_ERR_INVALID, "checkpoint of a chain set of another shape (chains, volume or stored samples)");
+  if (bytes < sh.bytes()) throw Error(DR_ERR_INVALID, "checkpoint buffer too small");
+  CK(cudaSetDevice(s->vol->device));
+  checkpoint_copy(s, const_cast<unsigned char*>(static_cast<const unsigned char*>(buf)), false);
+  API_END
+}
+
 int dr_get_state(dr_chainset* s, int chain, float* mu, float* s2inv) {
   API_BEGIN
   if (!s || chain < 0 || chain >= s->C) throw Error(DR_ERR_INVALID, "bad argument");

@@ -188,6 +188,15 @@ int dr_chainset_fft_plan_get(const dr_chainset* cs, int* plan);
 int dr_set_state(dr_chainset* cs, int chain, const float* mu, float s_hr, float s_sr);
 /* mu (2N floats) and sigma^-2 of a chain (MultiResParameters::mu_ / sigma). */
 int dr_get_state(dr_chainset* cs, int chain, float* mu, float* s2inv);
+/* Checkpoint of a chain set's sampler state into a host buffer: every chain's accepted spectral state, mu at the
+ * data and output voxels, the chain states (iteration, step size and dual averaging, sigma, accept bookkeeping; the
+ * counter-based RNG needs nothing else), the posterior-summary sums and any stored samples.  A chain set created on
+ * the same volume with the same options and chain count and restored from it continues bit for bit as the saved
+ * one would have (DR_ERR_INVALID when the shapes differ).  _size gives the bytes of the buffer.  No reference
+ * counterpart (the reference's fits run to completion in one process). */
+int dr_chainset_checkpoint_size(const dr_chainset* cs, int64_t* bytes);
+int dr_chainset_checkpoint_save(dr_chainset* cs, void* buf, int64_t bytes);
+int dr_chainset_checkpoint_restore(dr_chainset* cs, const void* buf, int64_t bytes);
 /* log prior (MultiResParameters.h:429-476) and log likelihood (:488-514) at mu
  * with the chain's sigma: out[0] = prior, out[1] = likelihood. */
 int dr_log_posterior(dr_chainset* cs, int chain, const float* mu, double* out);
