@@ -1187,8 +1187,8 @@ static void write_states(Chainset* S, const std::vector<ChainState>& st);
 static int tune_bucket(int n) { return n <= 0 ? -1 : (int)std::lround(4.0 * std::log2((double)n)); }
 
 // Tunes in two rounds on scratch chain sets of the same shape, each candidate
-// timed for 2 iterations forced past the step-size search (so that all of
-// their leapfrog steps run, at most 6 of them): first the update paths, with
+// timed for one iteration after one untimed, forced past the step-size search
+// (so that all of their leapfrog steps run, at most 6 of them): first the update paths, with
 // the tensor-core products where the volume and chain count allow them (else
 // CSR products at 8 blocks per SM); then, on the fastest path, the other
 // product choices (CSR at 8 blocks/SM, and at 4 and 2 for chain sets of fewer
@@ -1237,14 +1237,14 @@ static TuneChoice autotune(Volume* V, int C, const dr_hmc_opts* o) {
       CK(cudaEventCreate(&e0));
       CK(cudaEventCreate(&e1));
       CK(cudaEventRecord(e0, T->stream));
-      launch_iterations(T.get(), 2);
+      launch_iterations(T.get(), 1);
       CK(cudaEventRecord(e1, T->stream));
       CK(cudaEventSynchronize(e1));
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, e0, e1));
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      c.ms = ms / 2.0 * to_full;
+      c.ms = ms * to_full;
       if (trace_on()) std::fprintf(stderr, "[drb]   measured %.3f ms per iteration (scaled to L)\n", c.ms);
       if (c.ms < best.ms) best = c;
     } catch (const Error&) {
