@@ -88,7 +88,7 @@ class ServerStats(C.Structure):
                 ("busy_s", C.c_double), ("kernel_launches", C.c_int64)]
 
 
-JOB_QUEUED, JOB_READY, JOB_RUNNING, JOB_DONE, JOB_FAILED = range(5)
+JOB_QUEUED, JOB_READY, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_PREEMPTED = range(6)
 
 
 class ChainStats(C.Structure):
@@ -162,6 +162,8 @@ def _declare(L):
     L.dr_debug_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
     L.dr_debug_tc_layout.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp]
     L.dr_debug_bounded_wait.argtypes = [C.c_int, C.c_double, _ip, _dp]
+    L.dr_server_preempt.argtypes = [vp, C.c_uint64, C.c_double]
+    L.dr_server_resume.argtypes = [vp, C.c_uint64]
     L.dr_debug_pool_usage.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.dr_log_posterior_noalloc.argtypes = [vp, vp, C.c_float, C.c_float, vp]
     L.dr_free.argtypes = [vp]
@@ -614,6 +616,14 @@ class Server:
         """Submit a ``dualres_b200.synth.Volume``."""
         return self.submit(vol.highres, vol.qform_hr, vol.stdres, vol.qform_sr, vol.theta, vol.radius,
                            hmask=vol.hmask, omask=vol.omask, hmc=hmc, n_chains=n_chains)
+
+    def preempt(self, job, timeout_s=600.0):
+        """Checkpoint a resident job at its next round boundary and release its device memory (dr_server_preempt)."""
+        check(lib().dr_server_preempt(self.h, job, float(timeout_s)))
+
+    def resume(self, job):
+        """Re-admit a preempted job; it continues from its checkpoint (dr_server_resume)."""
+        check(lib().dr_server_resume(self.h, job))
 
     def status(self, job):
         st = JobStatus()

@@ -1954,16 +1954,7 @@ static void checkpoint_copy(Chainset* s, unsigned char* buf, bool to_host) {
   if ((int64_t)o != sh.bytes()) throw Error(DR_ERR_STATE, "checkpoint layout mismatch");
 }
 
-int dr_chainset_checkpoint_size(const dr_chainset* s, int64_t* bytes) {
-  API_BEGIN
-  if (!s || !bytes) throw Error(DR_ERR_INVALID, "NULL argument");
-  *bytes = checkpoint_shape(s).bytes();
-  API_END
-}
-
-int dr_chainset_checkpoint_save(dr_chainset* s, void* buf, int64_t bytes) {
-  API_BEGIN
-  if (!s || !buf) throw Error(DR_ERR_INVALID, "NULL argument");
+static void checkpoint_save(Chainset* s, void* buf, int64_t bytes) {
   const CheckpointShape sh = checkpoint_shape(s);
   if (bytes < sh.bytes()) throw Error(DR_ERR_INVALID, "checkpoint buffer too small");
   CK(cudaSetDevice(s->vol->device));
@@ -1971,12 +1962,9 @@ int dr_chainset_checkpoint_save(dr_chainset* s, void* buf, int64_t bytes) {
   const int64_t hdr[8] = {CKPT_MAGIC, CKPT_VERSION, sh.C, sh.N, sh.n_h, sh.n_o, sh.Cp, sh.nsave};
   std::memcpy(b, hdr, sizeof(hdr));
   checkpoint_copy(s, b, true);
-  API_END
 }
 
-int dr_chainset_checkpoint_restore(dr_chainset* s, const void* buf, int64_t bytes) {
-  API_BEGIN
-  if (!s || !buf) throw Error(DR_ERR_INVALID, "NULL argument");
+static void checkpoint_restore(Chainset* s, const void* buf, int64_t bytes) {
   const CheckpointShape sh = checkpoint_shape(s);
   if (bytes < 8 * (int64_t)sizeof(int64_t)) throw Error(DR_ERR_INVALID, "checkpoint buffer too small");
   int64_t hdr[8];
@@ -1989,6 +1977,26 @@ int dr_chainset_checkpoint_restore(dr_chainset* s, const void* buf, int64_t byte
   if (bytes < sh.bytes()) throw Error(DR_ERR_INVALID, "checkpoint buffer too small");
   CK(cudaSetDevice(s->vol->device));
   checkpoint_copy(s, const_cast<unsigned char*>(static_cast<const unsigned char*>(buf)), false);
+}
+
+int dr_chainset_checkpoint_size(const dr_chainset* s, int64_t* bytes) {
+  API_BEGIN
+  if (!s || !bytes) throw Error(DR_ERR_INVALID, "NULL argument");
+  *bytes = checkpoint_shape(s).bytes();
+  API_END
+}
+
+int dr_chainset_checkpoint_save(dr_chainset* s, void* buf, int64_t bytes) {
+  API_BEGIN
+  if (!s || !buf) throw Error(DR_ERR_INVALID, "NULL argument");
+  checkpoint_save(s, buf, bytes);
+  API_END
+}
+
+int dr_chainset_checkpoint_restore(dr_chainset* s, const void* buf, int64_t bytes) {
+  API_BEGIN
+  if (!s || !buf) throw Error(DR_ERR_INVALID, "NULL argument");
+  checkpoint_restore(s, buf, bytes);
   API_END
 }
 
@@ -2339,6 +2347,8 @@ struct Job {
   int64_t est_bytes = 0, bytes = 0;
   int iters_total = 0, iters_launched = 0;
   bool in_flight = false;
+  std::atomic<bool> preempt_req{false};  // checkpoint and release at the next round boundary
+  std::vector<unsigned char> ckpt;   // chain-set checkpoint of a preempted job, restored when it is rebuilt
   std::vector<float> mean, var, act;
   int64_t grads = 0;
   float mh = 0.f;
@@ -2384,6 +2394,7 @@ struct Server {
   int64_t budget = 0, in_use = 0, peak_bytes = 0;
   int peak_running = 0;
   int64_t n_submitted = 0, n_done = 0, n_failed = 0, grads_done = 0, launches = 0;
+  int64_t n_preempted = 0;  // jobs preempted and not resumed
   double last_finish = 0;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
@@ -2455,6 +2466,11 @@ struct Server {
         volume_build_device(j->vol.get(), j->desc.covariance, j->desc.covfun, o.device);
         auto cs = std::make_unique<Chainset>();
         chainset_build(cs.get(), j->vol.get(), j->C, &j->opts);
+        if (!j->ckpt.empty()) {  // a resumed job continues from its checkpoint
+          checkpoint_restore(cs.get(), j->ckpt.data(), (int64_t)j->ckpt.size());
+          j->ckpt.clear();
+          j->ckpt.shrink_to_fit();
+        }
         bytes = j->vol->bytes + cs->bytes;
         j->cs = std::move(cs);
         j->iters_total = j->opts.burnin + (j->opts.thin == 0 ? 1 : j->opts.thin) * j->opts.nsave;
@@ -2485,6 +2501,30 @@ struct Server {
       built_q.push_back(j);
       cv_work.notify_all();
     }
+  }
+
+  // Saves a resident job's checkpoint (its round has completed), frees its device objects but keeps its host
+  // set-up for the rebuild, and marks it preempted.
+  void preempt(const std::shared_ptr<Job>& j) {
+    Chainset* cs = j->cs.get();
+    const int64_t n = checkpoint_shape(cs).bytes();
+    std::vector<unsigned char> buf((size_t)n);
+    checkpoint_save(cs, buf.data(), n);
+    HostVolume hv = std::move(j->vol->hv);
+    j->cs.reset();
+    j->vol.reset();
+    auto vol = std::make_unique<Volume>();
+    vol->hv = std::move(hv);
+    std::lock_guard<std::mutex> lk(mtx);
+    j->ckpt = std::move(buf);
+    j->vol = std::move(vol);
+    j->preempt_req = false;
+    j->in_flight = false;
+    j->state = DR_JOB_PREEMPTED;
+    in_use -= j->bytes;
+    j->bytes = 0;
+    n_preempted++;
+    cv_done.notify_all();
   }
 
   // Reads a finished job's summary and frees its device objects; the fields that dr_server_status and
@@ -2578,6 +2618,10 @@ struct Server {
             if (q != cudaSuccess) throw Error(DR_ERR_CUDA, cudaGetErrorString(q));
             j->in_flight = false;
           }
+          if (j->preempt_req) {
+            preempt(j);
+            continue;
+          }
           if (j->iters_launched < j->iters_total) {
             if (chains_in_flight > 0 && chains_in_flight + j->C > o.max_chains_in_flight) {
               waiting = true;
@@ -2602,7 +2646,8 @@ struct Server {
       }
       active.erase(std::remove_if(active.begin(), active.end(),
                                   [](const std::shared_ptr<Job>& j) {
-                                    return j->state == DR_JOB_DONE || j->state == DR_JOB_FAILED;
+                                    return j->state == DR_JOB_DONE || j->state == DR_JOB_FAILED ||
+                                           j->state == DR_JOB_PREEMPTED;
                                   }),
                    active.end());
       std::unique_lock<std::mutex> lk(mtx);
@@ -2767,12 +2812,42 @@ int dr_server_wait(dr_server* sv, uint64_t job_id, double timeout_s) {
   API_END
 }
 
+int dr_server_preempt(dr_server* sv, uint64_t job_id, double timeout_s) {
+  API_BEGIN
+  if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(sv->mtx);
+  auto j = find_job(sv, job_id);
+  if (j->state != DR_JOB_RUNNING) throw Error(DR_ERR_STATE, "only an admitted, unfinished job can be preempted");
+  j->preempt_req = true;
+  sv->cv_work.notify_all();
+  const bool ok = sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    return j->state == DR_JOB_PREEMPTED || j->state == DR_JOB_DONE || j->state == DR_JOB_FAILED;
+  });
+  if (!ok) throw Error(DR_ERR_TIMEOUT, "job not preempted yet");
+  if (j->state == DR_JOB_FAILED) throw Error(j->error ? j->error : DR_ERR_STATE, "job failed: " + j->msg);
+  if (j->state == DR_JOB_DONE) throw Error(DR_ERR_STATE, "job finished before it could be preempted");
+  API_END
+}
+
+int dr_server_resume(dr_server* sv, uint64_t job_id) {
+  API_BEGIN
+  if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(sv->mtx);
+  auto j = find_job(sv, job_id);
+  if (j->state != DR_JOB_PREEMPTED) throw Error(DR_ERR_STATE, "job is not preempted");
+  j->state = DR_JOB_READY;
+  sv->n_preempted--;
+  sv->ready_q.push_back(j);
+  sv->cv_work.notify_all();
+  API_END
+}
+
 int dr_server_drain(dr_server* sv, double timeout_s) {
   API_BEGIN
   if (!sv) throw Error(DR_ERR_INVALID, "NULL server");
   std::unique_lock<std::mutex> lk(sv->mtx);
   const bool ok = sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
-                                       [&] { return sv->n_done + sv->n_failed >= sv->n_submitted; });
+                                       [&] { return sv->n_done + sv->n_failed + sv->n_preempted >= sv->n_submitted; });
   if (!ok) throw Error(DR_ERR_TIMEOUT, "jobs still running");
   API_END
 }
@@ -2784,7 +2859,7 @@ int dr_server_stats_get(dr_server* sv, dr_server_stats* out) {
   out->submitted = sv->n_submitted;
   out->done = sv->n_done;
   out->failed = sv->n_failed;
-  out->running = sv->n_submitted - sv->n_done - sv->n_failed;
+  out->running = sv->n_submitted - sv->n_done - sv->n_failed - sv->n_preempted;
   out->grad_evals = sv->grads_done;
   out->peak_device_bytes = sv->peak_bytes;
   out->peak_running = sv->peak_running;

@@ -260,6 +260,7 @@ typedef struct {
 #define DR_JOB_RUNNING 2  /* resident on the device */
 #define DR_JOB_DONE 3
 #define DR_JOB_FAILED 4
+#define DR_JOB_PREEMPTED 5 /* checkpointed and released from the device; dr_server_resume continues it */
 
 typedef struct {
   int state;                   /* DR_JOB_* */
@@ -291,6 +292,14 @@ int dr_server_status(dr_server* sv, uint64_t job_id, dr_job_status* out);
 int dr_server_result(dr_server* sv, uint64_t job_id, float* mean, float* var, float* activation);
 /* Waits (host side) until the job finished or failed, or timeout_s passed (DR_ERR_TIMEOUT). */
 int dr_server_wait(dr_server* sv, uint64_t job_id, double timeout_s);
+/* Preempts a resident job: at its next round boundary the scheduler saves its chain set's checkpoint
+ * (dr_chainset_checkpoint_save) in host memory, releases its device memory (the host set-up, kriging matrix
+ * included, is kept) and marks it DR_JOB_PREEMPTED; the call waits up to timeout_s for that.  DR_ERR_STATE when the
+ * job is not admitted yet or has ended.  No reference counterpart (SURVEY's optional preemption of served jobs). */
+int dr_server_preempt(dr_server* sv, uint64_t job_id, double timeout_s);
+/* Re-admits a preempted job like a new submission (same id); once rebuilt on the device it continues from its
+ * checkpoint, so its result equals that of an uninterrupted run bit for bit. */
+int dr_server_resume(dr_server* sv, uint64_t job_id);
 /* Waits until every submitted job finished or failed. */
 int dr_server_drain(dr_server* sv, double timeout_s);
 int dr_server_stats_get(dr_server* sv, dr_server_stats* out);

@@ -72,6 +72,34 @@ def test_chain_budget_runs_the_earliest_jobs_first():
         assert a.grad_evals == b.grad_evals
 
 
+def test_preempted_job_resumes_bit_for_bit():
+    """A job preempted while it runs (its checkpoint saved, its device memory released) and resumed later gives the
+    same result as an uninterrupted run of the same job, while another job keeps running beside it."""
+    import time
+    jobs = _jobs()
+    vol, hmc, C = jobs[1]
+    with d.Server(iterations_per_round=2) as sv:
+        ref = sv.result(_submit_wait(sv, vol, hmc, C))
+    with d.Server(iterations_per_round=2) as sv:
+        other = sv.submit_volume(*jobs[0])
+        j = sv.submit_volume(vol, hmc, C)
+        t0 = time.time()
+        while sv.status(j).state != d.api.JOB_RUNNING and time.time() - t0 < 120:
+            time.sleep(0.005)
+        sv.preempt(j)
+        st = sv.status(j)
+        assert st.state == d.api.JOB_PREEMPTED and st.device_bytes == 0
+        sv.wait(other, 600)
+        sv.resume(j)
+        sv.wait(j, 600)
+        got = sv.result(j)
+        with pytest.raises(d.DrError):
+            sv.resume(j)  # only a preempted job can be resumed
+    np.testing.assert_array_equal(ref.mean, got.mean)
+    np.testing.assert_array_equal(ref.var, got.var)
+    assert ref.grad_evals == got.grad_evals and ref.mh_rate == got.mh_rate
+
+
 def _submit_wait(sv, vol, hmc, C):
     j = sv.submit_volume(vol, hmc, C)
     sv.wait(j, 600)
