@@ -280,20 +280,28 @@ struct Plan2 {
 
 // Line elements at or beyond rlim are read as zero (they are never loaded), and elements at or beyond wlim are not
 // written (nothing reads them): the pruned input of the first stage and the pruned output of the last.
-template <int N, int R, int P, int DIR, int PER_LANE, class Idx>
-__device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)[PER_LANE], bool on,
+// at(pp) is the address of padded position pp = i + i / 8 of the line.  Where a butterfly's element offsets are
+// multiples of 8, or its first element is, the padded positions are the first one's plus constants
+// (pad(i0 + o) = pad(i0) + o + o / 8), so one position per butterfly is computed and the rest are immediates.
+__device__ __forceinline__ constexpr int plane_pad(int i) { return i + (i >> 3); }
+template <int N, int R, int P, int DIR, int PER_LANE, class At>
+__device__ __forceinline__ void plane_stage(float2* sm, At at, const int (&bl)[PER_LANE], bool on,
                                             const float2* __restrict__ tw, int rlim = N, int wlim = N) {
   constexpr int M = N / P, Mn = M / R, NB = N / R;
+  constexpr bool LIN_IN = (Mn % 8 == 0) || (Mn == 1 && M % 8 == 0);
+  constexpr bool LIN_OUT = ((P * Mn) % 8 == 0) || (Mn == 1 && P == 1);
   float2 x[PER_LANE][R];
 #pragma unroll
   for (int q = 0; q < PER_LANE; q++) {
     const int b = bl[q];
     if (on && b < NB) {
       const int p = b / Mn, t = b % Mn;
+      const int i0 = p * M + t, pp0 = plane_pad(i0);
 #pragma unroll
       for (int j = 0; j < R; j++) {
-        const int i = p * M + t + Mn * j;
-        x[q][j] = i < rlim ? sm[idx(i)] : make_float2(0.f, 0.f);
+        const int i = i0 + Mn * j;
+        const int pp = LIN_IN ? pp0 + Mn * j + ((Mn * j) >> 3) : plane_pad(i);
+        x[q][j] = i < rlim ? sm[at(pp)] : make_float2(0.f, 0.f);
       }
       reg_fft<R, DIR>(x[q]);
       if (Mn > 1) {
@@ -312,10 +320,12 @@ __device__ __forceinline__ void plane_stage(float2* sm, Idx idx, const int (&bl)
     const int b = bl[q];
     if (on && b < NB) {
       const int p = b / Mn, t = b % Mn;
+      const int o0 = p * Mn + t, po0 = plane_pad(o0);
 #pragma unroll
       for (int k = 0; k < R; k++) {
-        const int i = (p + P * k) * Mn + t;
-        if (i < wlim) sm[idx(i)] = x[q][k];
+        const int i = o0 + P * Mn * k;
+        const int pp = LIN_OUT ? po0 + P * Mn * k + ((P * Mn * k) >> 3) : plane_pad(i);
+        if (i < wlim) sm[at(pp)] = x[q][k];
       }
     }
   }
@@ -335,9 +345,9 @@ __device__ __forceinline__ void plane_rows(float2* sm, const float2* __restrict_
     const int y = base + li;
     const bool on = li < LPW && y < E;
     const int row = on ? (y + (y >> 3)) * PL::RP : 0;
-    auto idx = [row](int i) { return row + i + (i >> 3); };
-    plane_stage<E, R1, 1, DIR, 1>(sm, idx, bl, on, tw, rlim, E);
-    plane_stage<E, R2, R1, DIR, 1>(sm, idx, bl, on, tw, E, wlim);
+    auto at = [row](int pp) { return row + pp; };
+    plane_stage<E, R1, 1, DIR, 1>(sm, at, bl, on, tw, rlim, E);
+    plane_stage<E, R2, R1, DIR, 1>(sm, at, bl, on, tw, E, wlim);
   }
   __syncthreads();
 }
@@ -358,9 +368,9 @@ __device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* 
     const int x = base + li;
     const bool on = x < ncols;
     const int col = on ? x + (x >> 3) : 0;
-    auto idx = [col](int i) { return (i + (i >> 3)) * PL::RP + col; };
-    plane_stage<E, R1, 1, DIR, PL_LANE>(sm, idx, bl, on, tw, rlim, E);
-    plane_stage<E, R2, R1, DIR, PL_LANE>(sm, idx, bl, on, tw, E, wlim);
+    auto at = [col](int pp) { return pp * PL::RP + col; };
+    plane_stage<E, R1, 1, DIR, PL_LANE>(sm, at, bl, on, tw, rlim, E);
+    plane_stage<E, R2, R1, DIR, PL_LANE>(sm, at, bl, on, tw, E, wlim);
   }
   __syncthreads();
 }
