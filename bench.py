@@ -300,7 +300,7 @@ def run_ours(args, dist):
     value = grads_all / t_max
 
     extra = {}
-    # ---- BASELINE B2: the reference algorithm ported plainly to the GPU (four FFTs per step), one chain
+    # ---- the plain GPU form (B2): the reference algorithm ported plainly to the GPU (four FFTs per step), one chain
     try:
         r_plain, ms_plain = plain_gpu_rate(data, wl["leapfrog"], 10, device=dev)
         extra["plain_gpu_single_chain"] = {
@@ -417,7 +417,7 @@ def run_ours(args, dist):
 
 # ------------------------------------------------------------------ plain single-chain GPU baseline
 class PlainGPU:
-    """The reference's single-chain algorithm ported to the GPU the plain way (BASELINE B2): mu and p kept in real
+    """The reference's single-chain algorithm ported to the GPU the plain way (the B2 arm): mu and p kept in real
     space, four full 3D FFTs per leapfrog step (cuFFT through torch.fft), the kriging products as sparse CSR
     matrix-vector products, the accept decision read back every iteration.  It follows the restated algorithm of
     MultiResParameters::update (include/dualres/MultiResParameters.h:337-376, 674-727, 784-859) on the volume the

@@ -295,7 +295,7 @@ int dr_server_wait(dr_server* sv, uint64_t job_id, double timeout_s);
 /* Preempts a resident job: at its next round boundary the scheduler saves its chain set's checkpoint
  * (dr_chainset_checkpoint_save) in host memory, releases its device memory (the host set-up, kriging matrix
  * included, is kept) and marks it DR_JOB_PREEMPTED; the call waits up to timeout_s for that.  DR_ERR_STATE when the
- * job is not admitted yet or has ended.  No reference counterpart (SURVEY's optional preemption of served jobs). */
+ * job is not admitted yet or has ended.  No reference counterpart (the reference runs one fit per process). */
 int dr_server_preempt(dr_server* sv, uint64_t job_id, double timeout_s);
 /* Re-admits a preempted job like a new submission (same id); once rebuilt on the device it continues from its
  * checkpoint, so its result equals that of an uninterrupted run bit for bit. */
