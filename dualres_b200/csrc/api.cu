@@ -1318,8 +1318,6 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
   if (S->NR == 3) S->NR = 4;
   if (S->NR > 4 && S->NR < 8) S->NR = 8;
   const long long N = v.N;
-  ch.U = S->alloc<float2>((size_t)C * 2 * N);
-  ch.Q = S->alloc<float2>((size_t)C * N);
   const PathOptions po = path_options(v, V->device);
   int path = po.plane ? 0 : 2, grid = 8;
   // tensor-core products by default for 32 or more chains; the tuner, DRB_TC_PRODUCTS=0 / 1 and a forced choice
@@ -1353,6 +1351,10 @@ static void chainset_build(Chainset* S, Volume* V, int C, const dr_hmc_opts* o, 
     if (const char* g = std::getenv("DRB_PRODUCT_BLOCKS_PER_SM")) grid = std::max(1, std::min(16, std::atoi(g)));
   }
   if ((path == 0 && !po.plane) || (path == 1 && !po.prefetch)) path = po.plane ? 0 : 2;
+  // the state arrays are allocated after the tuning, whose candidate chain sets then reuse the pool's memory
+  // without this chain set's arrays held beside them
+  ch.U = S->alloc<float2>((size_t)C * 2 * N);
+  ch.Q = S->alloc<float2>((size_t)C * N);
   S->path = path;
   S->grid = grid;
   S->plane = path != 2;
