@@ -60,6 +60,31 @@ struct Error : std::runtime_error {
     g_launches++;                                                                                    \
   } while (0)
 
+// Launches of the leapfrog kernels allow programmatic dependent launch: the next kernel's grid is set up while the
+// previous one drains, and each of these kernels waits for its predecessor (grid_dep_wait) before touching memory.
+// DRB_PDL=0 turns it off.
+static bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("DRB_PDL");
+    return !(e && std::string(e) == "0");
+  }();
+  return on;
+}
+template <typename... P, typename... A>
+static void launch_k(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  CK(cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...));
+}
+
 static int cdiv_i(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // An NVTX range for the enclosing scope (shown by Nsight tools; no cost without one attached).
@@ -238,9 +263,9 @@ static void launch_pass_n(int dir, int pro, int epi, const PassArgs& a, const De
   const dim3 block(PassCfg<N>::NT);
   const size_t smem = (size_t)N * (TILE_LINES + 1) * sizeof(C);
   if (dir < 0 && pro == PRO_LOAD && epi == EPI_STORE)
-    k_pass<N, -1, PRO_LOAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+    launch_k(k_pass<N, -1, PRO_LOAD, EPI_STORE, C>, grid, block, smem, s, a, v, ch, tw);
   else if (dir > 0 && pro == PRO_LOAD && epi == EPI_STORE)
-    k_pass<N, +1, PRO_LOAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+    launch_k(k_pass<N, +1, PRO_LOAD, EPI_STORE, C>, grid, block, smem, s, a, v, ch, tw);
   else if constexpr (sizeof(C) == 8) {
     // the z passes touch the chain-minor arrays: with 8 or more chains, tiles of 4 lines x 8 chains unless the chain
     // set's tuning chose tiles of 32 lines of one chain (ch.ztile)
@@ -250,15 +275,15 @@ static void launch_pass_n(int dir, int pro, int epi, const PassArgs& a, const De
     constexpr bool two_plans = N == 64 || N == 128 || N == 256;
     const bool alt = two_plans && (ch.fftplan & (dir > 0 ? FP_ZINV : FP_ZFWD)) != 0;
     if (dir > 0 && pro == PRO_DATAGRAD && epi == EPI_STORE) {
-      if (alt && grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8, 1><<<ggrid, block, smem, s>>>(a, v, ch, tw);
-      else if (alt) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 1, 1><<<grid, block, smem, s>>>(a, v, ch, tw);
-      else if (grouped) k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
-      else k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+      if (alt && grouped) launch_k(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8, 1>, ggrid, block, smem, s, a, v, ch, tw);
+      else if (alt) launch_k(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 1, 1>, grid, block, smem, s, a, v, ch, tw);
+      else if (grouped) launch_k(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C, 8>, ggrid, block, smem, s, a, v, ch, tw);
+      else launch_k(k_pass<N, +1, PRO_DATAGRAD, EPI_STORE, C>, grid, block, smem, s, a, v, ch, tw);
     } else if (dir < 0 && pro == PRO_LOAD && epi == EPI_GATHER) {
-      if (alt && grouped) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8, 1><<<ggrid, block, smem, s>>>(a, v, ch, tw);
-      else if (alt) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 1, 1><<<grid, block, smem, s>>>(a, v, ch, tw);
-      else if (grouped) k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8><<<ggrid, block, smem, s>>>(a, v, ch, tw);
-      else k_pass<N, -1, PRO_LOAD, EPI_GATHER, C><<<grid, block, smem, s>>>(a, v, ch, tw);
+      if (alt && grouped) launch_k(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8, 1>, ggrid, block, smem, s, a, v, ch, tw);
+      else if (alt) launch_k(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 1, 1>, grid, block, smem, s, a, v, ch, tw);
+      else if (grouped) launch_k(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C, 8>, ggrid, block, smem, s, a, v, ch, tw);
+      else launch_k(k_pass<N, -1, PRO_LOAD, EPI_GATHER, C>, grid, block, smem, s, a, v, ch, tw);
     } else {
       throw Error(DR_ERR_INVALID, "unsupported pass combination");
     }
@@ -769,11 +794,11 @@ static void launch_spmv_t(const DevVolume& v, const DevChains& ch, int nb, int s
   bool rows = false;
   if constexpr (CG <= 8) rows = w && v.n_s >= 8 * nb;
   if (rows) {
-    if constexpr (CG <= 8) k_spmv_w_rows<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
+    if constexpr (CG <= 8) launch_k(k_spmv_w_rows<CG, NR>, nb, 256, 0, s, v, ch, step, sel, chain_only);
   } else if (w) {
-    k_spmv_w<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
+    launch_k(k_spmv_w<CG, NR>, nb, 256, 0, s, v, ch, step, sel, chain_only);
   } else
-    k_spmv_wt<CG, NR><<<nb, 256, 0, s>>>(v, ch, step, sel, chain_only);
+    launch_k(k_spmv_wt<CG, NR>, nb, 256, 0, s, v, ch, step, sel, chain_only);
   CK_LAUNCH();
 }
 
@@ -816,8 +841,8 @@ static void launch_tc(Chainset* S, int step, int sel, int chain_only, bool w) {
     // the gathered bytes in twice the operations, and measured faster with the threads' own loads
     const bool tg = S->tc_tg && !w;
 #define DRB_TC_LAUNCH(NN)                                                                                 \
-  if (tg) k_tc_product<NN, true><<<M.G, tc_threads(NN), sm, S->stream>>>(M, S->dc, n_h, sel, mode, P, xm); \
-  else k_tc_product<NN, false><<<M.G, tc_threads(NN), sm, S->stream>>>(M, S->dc, n_h, sel, mode, P, xm);
+  if (tg) launch_k(k_tc_product<NN, true>, M.G, tc_threads(NN), sm, S->stream, M, S->dc, n_h, sel, mode, P, xm); \
+  else launch_k(k_tc_product<NN, false>, M.G, tc_threads(NN), sm, S->stream, M, S->dc, n_h, sel, mode, P, xm);
     switch (N) {
       case 16: DRB_TC_LAUNCH(16) break;
       case 32: DRB_TC_LAUNCH(32) break;
@@ -831,11 +856,11 @@ static void launch_tc(Chainset* S, int step, int sel, int chain_only, bool w) {
   const size_t fs = tc_finish_smem_bytes(N);
   const int fm = w ? 0 : 1;
   switch (N) {
-    case 16: k_tc_finish<16><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
-    case 32: k_tc_finish<32><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
-    case 64: k_tc_finish<64><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
-    case 128: k_tc_finish<128><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
-    default: k_tc_finish<256><<<nfin, 256, fs, S->stream>>>(M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 16: launch_k(k_tc_finish<16>, nfin, 256, fs, S->stream, M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 32: launch_k(k_tc_finish<32>, nfin, 256, fs, S->stream, M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 64: launch_k(k_tc_finish<64>, nfin, 256, fs, S->stream, M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    case 128: launch_k(k_tc_finish<128>, nfin, 256, fs, S->stream, M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
+    default: launch_k(k_tc_finish<256>, nfin, 256, fs, S->stream, M, S->tc_partial, V->dv, S->dc, step, sel, chain_only, fm); break;
   }
   CK_LAUNCH();
 }
@@ -863,24 +888,24 @@ static void launch_xline(Chainset* S, int step, int flags) {
   const size_t smem = (size_t)v.E0 * (TILE_LINES + 1) * sizeof(float2);
   const float2* tw = S->vol->tw_f;
   switch (v.E0) {
-    case 2: k_xline<2><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 4: k_xline<4><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 8: k_xline<8><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 16: k_xline<16><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
-    case 32: k_xline<32><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 2: launch_k(k_xline<2>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw); break;
+    case 4: launch_k(k_xline<4>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw); break;
+    case 8: launch_k(k_xline<8>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw); break;
+    case 16: launch_k(k_xline<16>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw); break;
+    case 32: launch_k(k_xline<32>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw); break;
     case 64:
-      if (S->dc.fftplan & FP_XLINE) k_xline<64, 1><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
-      else k_xline<64><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      if (S->dc.fftplan & FP_XLINE) launch_k(k_xline<64, 1>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw);
+      else launch_k(k_xline<64>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw);
       break;
     case 128:
-      if (S->dc.fftplan & FP_XLINE) k_xline<128, 1><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
-      else k_xline<128><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      if (S->dc.fftplan & FP_XLINE) launch_k(k_xline<128, 1>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw);
+      else launch_k(k_xline<128>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw);
       break;
     case 256:
-      if (S->dc.fftplan & FP_XLINE) k_xline<256, 1><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
-      else k_xline<256><<<grid, 256, smem, S->stream>>>(v, S->dc, step, flags, tw);
+      if (S->dc.fftplan & FP_XLINE) launch_k(k_xline<256, 1>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw);
+      else launch_k(k_xline<256>, grid, 256, smem, S->stream, v, S->dc, step, flags, tw);
       break;
-    case 512: k_xline<512><<<grid, 512, smem, S->stream>>>(v, S->dc, step, flags, tw); break;
+    case 512: launch_k(k_xline<512>, grid, 512, smem, S->stream, v, S->dc, step, flags, tw); break;
     default: throw Error(DR_ERR_UNSUPPORTED, "E0 not supported");
   }
   CK_LAUNCH();
@@ -892,7 +917,7 @@ static void launch_plane_t(Chainset* S, int step, int flags) {
   const DevVolume& v = S->vol->dv;
   const dim3 grid(v.E2, S->C);
   const size_t smem = (size_t)plane_layout(E, PlaneGeom<E>::SIZE, PF).total;
-  k_xyplane<E, PF><<<grid, PlaneCfg<E, PF>::NT, smem, S->stream>>>(v, S->dc, step, flags, S->vol->tw_f);
+  launch_k(k_xyplane<E, PF>, grid, PlaneCfg<E, PF>::NT, smem, S->stream, v, S->dc, step, flags, S->vol->tw_f);
   CK_LAUNCH();
 }
 

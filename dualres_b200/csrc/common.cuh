@@ -122,4 +122,8 @@ __device__ __forceinline__ bool in_bounds(long long i, long long n, int* err) {
 #endif
 }
 
+// Waits until the grid this one depends on (programmatic dependent launch) has completed and its memory is
+// visible; returns at once when the kernel was launched without that dependency.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace drb

@@ -107,6 +107,7 @@ template <int N> struct PassCfg {
 
 template <int N, int DIR, int PRO, int EPI, class C, int CPB = 1, int PLAN = 0>
 __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v, DevChains ch, const C* __restrict__ tw) {
+  grid_dep_wait();
   constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = PassCfg<N>::NT, LPC = TILE_LINES / CPB;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
@@ -244,6 +245,7 @@ template <int E0> struct XCfg {
 template <int E0, int PLAN = 0>
 __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolume v, DevChains ch, int step, int flags,
                                                         const float2* __restrict__ tw) {
+  grid_dep_wait();
   constexpr int TL = TILE_LINES, P = TILE_LINES + 1, NT = XCfg<E0>::NT;
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = reinterpret_cast<float2*>(smraw);
@@ -587,6 +589,7 @@ __device__ __forceinline__ void plane_load_box(float2* sm, const float2* __restr
 template <int E, bool PREFETCH>
 __global__ void __launch_bounds__(PlaneCfg<E, PREFETCH>::NT, PlaneCfg<E, PREFETCH>::MINB) k_xyplane(DevVolume v, DevChains ch, int step, int flags,
                                                                        const float2* __restrict__ tw) {
+  grid_dep_wait();
   constexpr int NT = PlaneCfg<E, PREFETCH>::NT;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ double red[NT / 32];
@@ -734,6 +737,7 @@ __device__ __forceinline__ void csr_batches(const float* __restrict__ val, const
 // row's 32-nonzero batches and combine their sums in a fixed order.
 template <int CG, int NR>
 __global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  grid_dep_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int C = ch.C, Cp = ch.Cp;
   const int cc = lane % CG;
@@ -782,6 +786,7 @@ __global__ void __launch_bounds__(256, 4) k_spmv_w(DevVolume v, DevChains ch, in
 // row in flight.  The per-chain squared residuals are summed over the block's warps in a fixed order.
 template <int CG, int NR>
 __global__ void __launch_bounds__(256, 4) k_spmv_w_rows(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  grid_dep_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int C = ch.C, Cp = ch.Cp;
   const int cc = lane % CG;
@@ -836,6 +841,7 @@ __global__ void __launch_bounds__(256, 4) k_spmv_w_rows(DevVolume v, DevChains c
 // ||Yh - mu_D||^2 partials per block.
 template <int CG, int NR>
 __global__ void __launch_bounds__(256, 4) k_spmv_wt(DevVolume v, DevChains ch, int step, int sel, int chain_only) {
+  grid_dep_wait();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int C = ch.C, Cp = ch.Cp;
   const int cc = lane % CG;

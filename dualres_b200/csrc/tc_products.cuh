@@ -89,6 +89,7 @@ template <int N, bool TG>
 __global__ void __launch_bounds__(tc_threads(N), 1)
     k_tc_product(DevTcMatrix A, DevChains ch, int n_h, int sel, int mode, float* __restrict__ partial,
                  const __grid_constant__ CUtensorMap xmap) {
+  grid_dep_wait();
   extern __shared__ __align__(1024) unsigned char tsm[];
   uint64_t* fullA = reinterpret_cast<uint64_t*>(tsm);
   uint64_t* fullB = fullA + 4;
@@ -357,6 +358,7 @@ __host__ __device__ inline int tc_finish_smem_bytes(int N) { return N * (TC_FR +
 template <int N>
 __global__ void __launch_bounds__(256) k_tc_finish(DevTcMatrix A, const float* __restrict__ partial, DevVolume v,
                                                    DevChains ch, int step, int sel, int chain_only, int mode) {
+  grid_dep_wait();
   constexpr int EPT = N * TC_FR / 256;  // elements per thread (N >= 16)
   extern __shared__ __align__(16) unsigned char fsm[];
   float* S = reinterpret_cast<float*>(fsm);
