@@ -457,11 +457,12 @@ __device__ __forceinline__ void plane_update(float2* sm, const DevVolume& v, con
   const float Nf = (float)v.N;
   double pa = 0.0, pb = 0.0;
   // Pairs of x-adjacent points: element pair e sits at li = 2e of the plane (x = 2 (e mod E/2), y = e / (E/2)),
-  // so U, q and 1/lambda are read as float4 / float4 / float2 at index e.  Each thread first issues the loads
-  // of B pairs, then computes and stores them, so B loads per array are in flight at once.  A thread reads and
-  // writes only its own elements, which is why the in-place state buffers may be marked non-aliasing.
+  // so U, q and 1/lambda are read as float4 / float4 / float2 at index e.  Each thread issues the loads of B pairs
+  // before computing them; with the block's state prefetched into L2 at entry one pair suffices (two pairs were
+  // 154.7 against 151.8 us for a 64^2 plane x 64 chains).  A thread reads and writes only its own elements, which is
+  // why the in-place state buffers may be marked non-aliasing.
   constexpr int TOTAL = E * (E / 2);
-  constexpr int B = TOTAL >= 2 * NT ? 2 : 1;
+  constexpr int B = 1;
   const float4* __restrict__ gU = reinterpret_cast<const float4*>(srcU);
   const float4* __restrict__ gQ = reinterpret_cast<const float4*>(srcQ);
   const float2* __restrict__ gS = reinterpret_cast<const float2*>(srcS);
