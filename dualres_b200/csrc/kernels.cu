@@ -395,10 +395,12 @@ struct PlaneGeom {
 };
 
 // PREFETCH: the U and q planes are bulk-copied into shared memory at entry; 256 threads and 128 registers, two
-// blocks per SM (E <= 64).  Without it four blocks of 256 threads at 64 registers (E <= 64).
+// blocks per SM (E <= 64).  Without it a register budget for three blocks of 256 threads (E <= 64): 80 registers
+// and 80 B of spill against 64 registers and 200 B for four, which with the state prefetched into L2 is the faster
+// (64^2 plane x 64 chains 150.0 against 150.9 us, one chain 10.8 against 12.4 us).
 template <int E, bool PREFETCH> struct PlaneCfg {
   static constexpr int NT = E >= 128 ? 512 : 256;
-  static constexpr int MINB = PREFETCH ? 2 : (E <= 64 ? 4 : 1);  // blocks per SM the register budget targets
+  static constexpr int MINB = PREFETCH ? 2 : (E <= 64 ? 3 : 1);  // blocks per SM the register budget targets
 };
 
 // Shared-memory layout in bytes: [mbarrier | plane | U | q].
