@@ -441,6 +441,10 @@ __device__ __forceinline__ void plane_fft(float2* sm, int ncols, int nrows, int 
   }
 }
 
+// e / d as __umulhi(e, box_div_magic(d)) for the box positions of a plane (e < 2^15, 2 <= d <= 256): the multiplier
+// ceil(2^32 / d) gives the exact quotient there, without a division per element.
+__device__ __forceinline__ uint32_t box_div_magic(int d) { return 0xFFFFFFFFu / (uint32_t)d + 1u; }
+
 // One plane of one chain after its inverse transforms, in two parts.  plane_update: the kick (and at step 0 the
 // momentum draw) and the drift, with the state read from srcU / srcQ / srcS (global memory, or shared-memory copies
 // of this plane) and written to Udst / Qc in global memory; the energies' per-thread partials go to pa / pb.
@@ -564,8 +568,9 @@ __device__ __forceinline__ void plane_finish(float2* sm, const DevChains& ch, in
   if (last) return;
   __syncthreads();
   plane_fft<E>(sm, bx, by, -1, twE);
+  const uint32_t mb = box_div_magic(bx);
   for (int e = tid; e < by * bx; e += NT) {
-    const int y = e / bx, x = e % bx;
+    const int y = (int)__umulhi((uint32_t)e, mb), x = e - y * bx;
     T[y * bx + x] = sm[G::at(y, x)];
   }
 }
@@ -577,8 +582,9 @@ __device__ __forceinline__ void plane_load_box(float2* sm, const float2* __restr
   using G = PlaneGeom<E>;
   const int tid = threadIdx.x;
   if constexpr (G::PADDED) {
+    const uint32_t mb = box_div_magic(bx);
     for (int e = tid; e < by * bx; e += NT) {
-      const int y = e / bx, x = e % bx;
+      const int y = (int)__umulhi((uint32_t)e, mb), x = e - y * bx;
       sm[G::at(y, x)] = T[e];
     }
   } else {
