@@ -19,6 +19,10 @@
 
 namespace drb {
 
+// e / d as __umulhi(e, box_div_magic(d)) for box positions (e < 2^15, 2 <= d <= 1024): the multiplier
+// ceil(2^32 / d) gives the exact quotient there, without a division per element.
+__device__ __forceinline__ uint32_t box_div_magic(int d) { return 0xFFFFFFFFu / (uint32_t)d + 1u; }
+
 // ----------------------------------------------------------------- twiddles
 __device__ float2 g_tw_f[TW_TOTAL];
 __device__ double2 g_tw_d[TW_TOTAL];
@@ -364,8 +368,9 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
   if (last) return;
   __syncthreads();
   fft_smem<E0, -1, TL, NT, float2, PLAN>(sm, 1, P, TL, tw + tw_offset(E0));
+  const uint32_t mb = box_div_magic(bx);
   for (int e = threadIdx.x; e < TL * bx; e += NT) {
-    const int l = e / bx, x = e % bx;
+    const int l = (int)__umulhi((uint32_t)e, mb), x = e - l * bx;
     if (l < nl) T1[(lam0 + l) * bx + x] = sm[x * P + l];
   }
 }
@@ -440,10 +445,6 @@ __device__ __forceinline__ void plane_fft(float2* sm, int ncols, int nrows, int 
     }
   }
 }
-
-// e / d as __umulhi(e, box_div_magic(d)) for the box positions of a plane (e < 2^15, 2 <= d <= 256): the multiplier
-// ceil(2^32 / d) gives the exact quotient there, without a division per element.
-__device__ __forceinline__ uint32_t box_div_magic(int d) { return 0xFFFFFFFFu / (uint32_t)d + 1u; }
 
 // One plane of one chain after its inverse transforms, in two parts.  plane_update: the kick (and at step 0 the
 // momentum draw) and the drift, with the state read from srcU / srcQ / srcS (global memory, or shared-memory copies
