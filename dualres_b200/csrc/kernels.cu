@@ -504,7 +504,7 @@ __device__ __forceinline__ void plane_update(float2* sm, const DevVolume& v, con
         w1 = box_muller(u01f(r.z), u01f(r.w));
         pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
       }
-      const int pi0 = G::at(y, x), pi1 = G::at(y, x + 1);
+      const int pi0 = G::at(y, x), pi1 = pi0 + 1;  // x is even: x + 1 is the next slot in either layout
       float2 uo[2], qo[2];
 #pragma unroll
       for (int m = 0; m < 2; m++) {
