@@ -809,9 +809,9 @@ def posterior_mean_vs_fp64(vol, iters=12, L=25, eps=0.05, seed=1):
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
     return {"rel_mean": rel(m32, m64), "rel_var": rel(v32, v64), "iterations": iters, "leapfrog": L, "eps": eps,
             "accept_flips": flips, "accept_rate": acc / iters, "seconds": dt,
-            "what": "FP32 sampler kernels (dr_leapfrog_fixed) vs the FP64 oracle on identical draws, one chain on the "
-                    "benchmark volume, sigma fixed; norm-wise relative error of the running posterior mean and "
-                    "variance of Re mu over the output voxels"}
+            "what": "FP32 sampler kernels (dr_leapfrog_fixed) vs the FP64 oracle on identical draws, one chain on "
+                    "this volume, sigma fixed; norm-wise relative error of the running posterior mean and variance "
+                    "of Re mu over the output voxels"}
 
 
 def cpu_baseline_line(vol, W, L, target_s=12.0, pm_iters=12, pm_L=25):
