@@ -284,9 +284,15 @@ struct Plan2 {
 // multiples of 8, or its first element is, the padded positions are the first one's plus constants
 // (pad(i0 + o) = pad(i0) + o + o / 8), so one position per butterfly is computed and the rest are immediates.
 __device__ __forceinline__ constexpr int plane_pad(int i) { return i + (i >> 3); }
+// Between the read and write phases of a stage: __syncwarp when one warp owns its lines (bar = 0), else named barrier
+// `bar` over the two warps that share them.
+__device__ __forceinline__ void line_sync(int bar) {
+  if (bar == 0) __syncwarp();
+  else asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
+}
 template <int N, int R, int P, int DIR, int PER_LANE, class At>
 __device__ __forceinline__ void plane_stage(float2* sm, At at, const int (&bl)[PER_LANE], bool on,
-                                            const float2* __restrict__ tw, int rlim = N, int wlim = N) {
+                                            const float2* __restrict__ tw, int rlim = N, int wlim = N, int bar = 0) {
   constexpr int M = N / P, Mn = M / R, NB = N / R;
   constexpr bool LIN_IN = (Mn % 8 == 0) || (Mn == 1 && M % 8 == 0);
   constexpr bool LIN_OUT = ((P * Mn) % 8 == 0) || (Mn == 1 && P == 1);
@@ -314,7 +320,7 @@ __device__ __forceinline__ void plane_stage(float2* sm, At at, const int (&bl)[P
       }
     }
   }
-  __syncwarp();
+  line_sync(bar);
 #pragma unroll
   for (int q = 0; q < PER_LANE; q++) {
     const int b = bl[q];
@@ -329,7 +335,7 @@ __device__ __forceinline__ void plane_stage(float2* sm, At at, const int (&bl)[P
       }
     }
   }
-  __syncwarp();
+  line_sync(bar);
 }
 
 // Row FFTs (lines = y rows, elements along x) of a padded plane, all E rows; x >= rlim read as zero, x >= wlim not
@@ -361,6 +367,27 @@ __device__ __forceinline__ void plane_cols(float2* sm, int ncols, const float2* 
   constexpr int NBM = Plan2<E, R1, R2>::NBM, PL_LANE = NBM / 4;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int li = lane & 7, bb = lane >> 3;
+  if constexpr (PL_LANE % 2 == 0) {
+    // At most half as many 8-column groups as warps (a pruned box): the two warps of a pair split each column's
+    // butterflies instead of half the warps idling, and the pair synchronises its stages on named barrier 1 + pair.
+    if (2 * ((ncols + 7) / 8) <= nw && nw % 2 == 0 && nw <= 30) {
+      constexpr int H = PL_LANE / 2;
+      const int pair = warp >> 1, half = warp & 1;
+      int bh[H];
+#pragma unroll
+      for (int q = 0; q < H; q++) bh[q] = bb + 4 * (half * H + q);
+      for (int base = pair * 8; base < ncols; base += (nw / 2) * 8) {
+        const int x = base + li;
+        const bool on = x < ncols;
+        const int col = on ? x + (x >> 3) : 0;
+        auto at = [col](int pp) { return pp * PL::RP + col; };
+        plane_stage<E, R1, 1, DIR, H>(sm, at, bh, on, tw, rlim, E, 1 + pair);
+        plane_stage<E, R2, R1, DIR, H>(sm, at, bh, on, tw, E, wlim, 1 + pair);
+      }
+      __syncthreads();
+      return;
+    }
+  }
   int bl[PL_LANE];
 #pragma unroll
   for (int q = 0; q < PL_LANE; q++) bl[q] = bb + 4 * q;
