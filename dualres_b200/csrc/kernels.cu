@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
     const int l = e / (E0 / 2), x = 2 * (e % (E0 / 2));
     if (l >= nl) continue;
     const long long gi = (lam0 + l) * E0 + x;
-    const float4 u4 = *reinterpret_cast<const float4*>(Usrc + gi);
+    const float4 u4 = __ldcs(reinterpret_cast<const float4*>(Usrc + gi));
     const float2 s2 = *reinterpret_cast<const float2*>(v.sinv + gi);
     float4 q4;
     float2 w0 = make_float2(0.f, 0.f), w1 = w0;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
       w1 = box_muller(u01f(r.z), u01f(r.w));
       pa += (double)(w0.x * w0.x + w0.y * w0.y) + (double)(w1.x * w1.x + w1.y * w1.y);
     } else {
-      q4 = *reinterpret_cast<const float4*>(Qc + gi);
+      q4 = __ldcs(reinterpret_cast<const float4*>(Qc + gi));
     }
     float2 uo[2], qo[2];
 #pragma unroll
@@ -355,8 +355,9 @@ __global__ void __launch_bounds__(XCfg<E0>::NT, XCfg<E0>::MINB) k_xline(DevVolum
       qo[m] = q;
       sm[(x + m) * P + l] = un;
     }
-    if (write_q) *reinterpret_cast<float4*>(Qc + gi) = make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y);
-    if (!last) *reinterpret_cast<float4*>(Udst + gi) = make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y);
+    // streaming loads and stores of the state, as in the plane kernel: it is not read again before the next step
+    if (write_q) __stcs(reinterpret_cast<float4*>(Qc + gi), make_float4(qo[0].x, qo[0].y, qo[1].x, qo[1].y));
+    if (!last) __stcs(reinterpret_cast<float4*>(Udst + gi), make_float4(uo[0].x, uo[0].y, uo[1].x, uo[1].y));
   }
   // per-block partial sums -> accept step
   if (first || last) {
