@@ -161,7 +161,11 @@ __global__ void __launch_bounds__(PassCfg<N>::NT) k_pass(PassArgs a, DevVolume v
       const long long idx = in_index(l, i);
       const int c = chain(l);
       if (PRO == PRO_LOAD) {
-        if (in_bounds(idx, in_lim, ch.err)) val = reinterpret_cast<const C*>(a.in)[(long long)c * a.in_cs + idx];
+        // the forward z pass is the last reader of its input (T2): streaming loads, evicted first
+        if (in_bounds(idx, in_lim, ch.err)) {
+          if constexpr (EPI == EPI_GATHER) val = __ldcs(reinterpret_cast<const C*>(a.in) + (long long)c * a.in_cs + idx);
+          else val = reinterpret_cast<const C*>(a.in)[(long long)c * a.in_cs + idx];
+        }
       } else if (in_bounds(idx, box, ch.err)) {
         const int j = v.box_to_d[idx];
         if (j >= 0 && in_bounds(j, v.n_h, ch.err)) val.x = ch.gD[(long long)j * ch.Cp + c];
@@ -596,7 +600,7 @@ __device__ __forceinline__ void plane_load_box(float2* sm, const float2* __restr
     const uint32_t mb = box_div_magic(bx);
     for (int e = tid; e < by * bx; e += NT) {
       const int y = (int)__umulhi((uint32_t)e, mb), x = e - y * bx;
-      sm[G::at(y, x)] = T[e];
+      sm[G::at(y, x)] = __ldcs(T + e);  // the last read of this T2 plane before the next inverse z pass
     }
   } else {
     for (int e = tid; e < E * E; e += NT) {
